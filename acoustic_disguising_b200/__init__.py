@@ -1,0 +1,14 @@
+"""B200-native FDTD + Kirchhoff-Helmholtz hot path of AcousticDisguising.
+
+The compute lives in libadfdtd.so (CUDA for sm_100a, C-ABI in
+include/adfdtd.h); this package is its Python mirror of the reference API.
+"""
+from ._lib import AdfError, build, lib, last_error, LIB_PATH  # noqa: F401
+from .api import (  # noqa: F401
+    Context, default_context, Domain, coord, coords, t, fibonacci_sphere, impulsive_wavelet,
+    ricker_wavelet, fib_sphere_area, cpml_profiles, split_profiles, Cpml, shape_params,
+    build_update_mask, Transceiver, TransceiverGrid, transceivers_to_grid, p_src, p_rec, vn_src,
+    vn_rec, run_fdtd, injection_coefficients,
+)
+
+__all__ = [n for n in dir() if not n.startswith("_")]

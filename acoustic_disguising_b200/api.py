@@ -1,0 +1,358 @@
+"""Python mirror of the reference's FDTD/KH entry points over libadfdtd.so.
+
+Names, argument meaning and array layouts follow the reference Julia API
+(AcousticDisguising: src/simulation.jl, src/geometry.jl, src/illumination.jl,
+src/greens.jl, src/kh_kernels.jl) so that host code reads the same way:
+numpy arrays are Fortran-ordered with the reference's shapes, e.g. the field
+is (nx, ny, nz, 4) Float32 and trace buffers are (nt, ntx).
+
+Every compute call goes through the C-ABI; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import threading
+from dataclasses import dataclass, field as dc_field
+
+import numpy as np
+
+from . import _lib as L
+
+_ctx_lock = threading.Lock()
+_ctx = None
+
+
+class Context:
+    """One adf_ctx (device, stream, HBM budget)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = C.c_void_p()
+        L.check(L.lib().adf_ctx_create(device, hbm_budget, C.byref(h)), "adf_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            L.lib().adf_ctx_destroy(self.h)
+            self.h = None
+
+    def last_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        L.check(L.lib().adf_last_timing(self.h, C.byref(ms), C.byref(n)), "adf_last_timing")
+        return ms.value, n.value
+
+
+def default_context() -> Context:
+    global _ctx
+    with _ctx_lock:
+        if _ctx is None:
+            _ctx = Context(0)
+        return _ctx
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# Domain and coordinates (src/simulation.jl:25-115)
+# ---------------------------------------------------------------------------
+def Domain(tmax=10e-4, xmax=1.0, ymax=None, zmax=None, nx=201, ny=None, nz=None, c0=1500.0,
+           r0=1000.0, cf=0.25) -> L.Domain:
+    ymax = xmax if ymax is None else ymax
+    zmax = xmax if zmax is None else zmax
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    d = L.Domain()
+    L.check(L.lib().adf_domain_make(float(tmax), float(xmax), float(ymax), float(zmax), int(nx),
+                                    int(ny), int(nz), float(c0), float(r0), float(cf),
+                                    C.byref(d)), "Domain")
+    return d
+
+
+def coord(d: L.Domain, axis: int, chan: int) -> np.ndarray:
+    """coords(d)[axis][chan]; axis 0..2 = x,y,z, chan 0..3 = p,vx,vy,vz."""
+    n = [d.nx, d.ny, d.nz][axis]
+    out = np.empty(n, np.float64)
+    L.check(L.lib().adf_coords(C.byref(d), axis, chan, _p(out)), "coords")
+    return out
+
+
+def coords(d: L.Domain) -> dict:
+    keys = ("p", "vx", "vy", "vz")
+    return {ax: {k: coord(d, a, c) for c, k in enumerate(keys)}
+            for a, ax in enumerate(("x", "y", "z"))}
+
+
+def t(d: L.Domain) -> np.ndarray:
+    """t(d) = range(0; stop=tmax, length=nt) (simulation.jl:86), the Julia
+    range values.  The step is tmax/(nt-1), not dt, as in the reference."""
+    out = np.empty(int(d.nt), np.float64)
+    L.check(L.lib().adf_time_axis(C.byref(d), _p(out)), "t")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Illumination helpers (src/illumination.jl)
+# ---------------------------------------------------------------------------
+def fibonacci_sphere(n: int, radius: float = 1.0):
+    """fibonacci_sphere (illumination.jl:19-46): (points, normals), (n,3)."""
+    i = np.arange(n, dtype=np.float64)
+    z = 1.0 - (2.0 * i + 1.0) / n
+    rxy = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    th = (math.pi * (3.0 - math.sqrt(5.0))) * i
+    nrm = np.stack([rxy * np.cos(th), rxy * np.sin(th), z], axis=1)
+    return radius * nrm, nrm
+
+
+def impulsive_wavelet(d: L.Domain, f_3db_hz: float):
+    """impulsive_wavelet (illumination.jl:167-184): (tf, timeshift)."""
+    sig = math.sqrt(math.log(2.0)) / (2 * math.pi * float(f_3db_hz))
+    plen = int(round(10 * sig / d.dt))
+    pl = min(plen, int(d.nt))
+    pc, pw = pl / 2, pl / 10
+    tf = np.zeros(int(d.nt), np.float64)
+    u = np.arange(1, pl + 1, dtype=np.float64) - pc
+    tf[:pl] = np.exp(-(u * u) / (2 * (pw * pw)))
+    tf /= tf.sum() * d.dt
+    return tf, pc * d.dt
+
+
+def ricker_wavelet(d: L.Domain, fc: float = 18_000.0, injection: bool = True):
+    """ricker_wavelet (illumination.jl:199-207)."""
+    wn = math.pi * fc * (t(d) - 1.0 / fc)
+    tf = (1.0 - 2.0 * wn * wn) * np.exp(-(wn * wn))
+    if injection:
+        tf = np.cumsum(tf) * (d.dt / d.dx)
+    return tf
+
+
+def fib_sphere_area(radius: float, n_points: int) -> float:
+    """fib_sphere_area (src/io.jl:131)."""
+    return 4 * math.pi * radius ** 2 / n_points
+
+
+# ---------------------------------------------------------------------------
+# CPML (src/simulation.jl:200-241, src/kernels/cpmlcoeffs.jl)
+# ---------------------------------------------------------------------------
+def cpml_profiles(npml: int, vel_max: float, dt: float, rcoef: float, thickness: float, fc: float,
+                  ctx: Context | None = None):
+    """compute_CPML_coefficients! on the GPU in FP64; returns (float32[8n+4],
+    float64[8n+4]) in the order a_l a_r a_hl a_hr b_l b_r b_hl b_hr."""
+    ctx = ctx or default_context()
+    o32 = np.zeros(8 * npml + 4, np.float32)
+    o64 = np.zeros(8 * npml + 4, np.float64)
+    L.check(L.lib().adf_cpml_profiles(ctx.h, npml, vel_max, dt, rcoef, thickness, fc, _p(o32),
+                                      _p(o64)), "cpml_profiles")
+    return o32, o64
+
+
+def split_profiles(flat: np.ndarray, npml: int) -> dict:
+    n = npml
+    sizes = [("a_l", n), ("a_r", n), ("a_hl", n + 1), ("a_hr", n + 1), ("b_l", n), ("b_r", n),
+             ("b_hl", n + 1), ("b_hr", n + 1)]
+    out, o = {}, 0
+    for k, s in sizes:
+        out[k] = flat[o:o + s]
+        o += s
+    return out
+
+
+class Cpml:
+    """`Cpml(d; npml, rcoef, fc)`: memory variables (Julia layout) + Float32
+    coefficients.  `mv[a]`/`mp[a]` are the reference's `cpml.v[a]`/`cpml.p[a]`."""
+
+    def __init__(self, d: L.Domain, npml: int, rcoef: float = 1e-4, fc: float = 3e3,
+                 ctx: Context | None = None):
+        self.n = npml
+        dims = [d.nx, d.ny, d.nz]
+        self.mv, self.mp = [], []
+        for a in range(3):
+            sv = list(dims); sv[a] = npml
+            sp = list(dims); sp[a] = npml + 1
+            self.mv.append(np.zeros(sv + [2], np.float32, order="F"))
+            self.mp.append(np.zeros(sp + [2], np.float32, order="F"))
+        self.coef, self.coef64 = cpml_profiles(npml, d.c0, d.dt, rcoef, d.dx * npml, fc, ctx)
+
+    def reset(self):
+        """resetCPMLmemory! (simulation.jl:235-241)."""
+        for a in self.mv + self.mp:
+            a[...] = 0
+
+    def _c(self):
+        s = L.CpmlC()
+        s.npml = self.n
+        for a in range(3):
+            s.mv[a] = self.mv[a].ctypes.data
+            s.mp[a] = self.mp[a].ctypes.data
+        s.coef = self.coef.ctypes.data
+        return s
+
+
+# ---------------------------------------------------------------------------
+# Geometry (src/geometry.jl)
+# ---------------------------------------------------------------------------
+def shape_params(scatterer: str, radius=None, length=None, semi_axes=None,
+                 center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    p = np.zeros(6, np.float64)
+    if scatterer == "sphere":
+        p[0] = radius
+        p[1:4] = center
+    elif scatterer == "cube":
+        p[0] = length
+        p[1:4] = center
+    elif scatterer == "cross":
+        p[0] = length
+    elif scatterer == "ellipsoid":
+        p[0:3] = semi_axes
+        p[3:6] = center
+    return p
+
+
+def build_update_mask(d: L.Domain, scatterer: str, ctx: Context | None = None, **kw):
+    """build_update_mask (geometry.jl:250-280) -> (nx,ny,nz,4) bool or None."""
+    if scatterer == "none":
+        return None
+    ctx = ctx or default_context()
+    out = np.zeros((d.nx, d.ny, d.nz, 4), np.uint8, order="F")
+    L.check(L.lib().adf_build_mask(ctx.h, C.byref(d), L.SHAPES[scatterer],
+                                   _p(shape_params(scatterer, **kw)), _p(out)), "build_update_mask")
+    return out.astype(bool)
+
+
+# ---------------------------------------------------------------------------
+# Transceivers (src/simulation.jl:168-187, 347-452)
+# ---------------------------------------------------------------------------
+@dataclass
+class Transceiver:
+    """Transceiver(d; point, direction, tf); direction = [q, fx, fy, fz]."""
+
+    point: np.ndarray
+    direction: np.ndarray
+    tf: np.ndarray
+
+
+@dataclass
+class TransceiverGrid:
+    """Packed per-channel buffers, Julia layout (channel order p, vx, vy, vz)."""
+
+    idx: list
+    w: list
+    src: list
+    rec: list
+    direction: np.ndarray
+    vn_src: np.ndarray
+    vn_rec: np.ndarray
+
+    @property
+    def ntx(self):
+        return self.direction.shape[1]
+
+    @property
+    def nt(self):
+        return self.vn_src.shape[0]
+
+    def _c(self):
+        g = L.TxGridC()
+        g.ntx, g.nt = self.ntx, self.nt
+        for c in range(4):
+            g.idx[c] = self.idx[c].ctypes.data
+            g.w[c] = self.w[c].ctypes.data
+            g.src[c] = self.src[c].ctypes.data
+            g.rec[c] = self.rec[c].ctypes.data
+        g.dir = self.direction.ctypes.data
+        g.vn_src = self.vn_src.ctypes.data
+        g.vn_rec = self.vn_rec.ctypes.data
+        return g
+
+    def copy(self):
+        cp = lambda a: a.copy(order="F")
+        return TransceiverGrid([cp(a) for a in self.idx], [cp(a) for a in self.w],
+                               [cp(a) for a in self.src], [cp(a) for a in self.rec],
+                               cp(self.direction), cp(self.vn_src), cp(self.vn_rec))
+
+
+def transceivers_to_grid(d: L.Domain, txs) -> TransceiverGrid:
+    """transceiversToGrid (simulation.jl:387-431)."""
+    ntx, nt = len(txs), int(d.nt)
+    pts = np.ascontiguousarray([np.asarray(x.point, np.float64) for x in txs]).reshape(ntx, 3)
+    dirs = np.ascontiguousarray([np.asarray(x.direction, np.float64) for x in txs]).reshape(ntx, 4)
+    tf = np.asfortranarray(np.stack([np.asarray(x.tf, np.float64) for x in txs], axis=1))
+    g = TransceiverGrid([np.zeros((3, ntx), np.float32, order="F") for _ in range(4)],
+                        [np.zeros((2, 2, 2, ntx), np.float32, order="F") for _ in range(4)],
+                        [np.zeros((nt, ntx), np.float32, order="F") for _ in range(4)],
+                        [np.zeros((nt, ntx), np.float32, order="F") for _ in range(4)],
+                        np.zeros((4, ntx), np.float32, order="F"),
+                        np.zeros((nt, ntx), np.float32, order="F"),
+                        np.zeros((nt, ntx), np.float32, order="F"))
+    cg = g._c()
+    L.check(L.lib().adf_pack_transceivers(C.byref(d), _p(pts), _p(dirs), _p(tf), C.byref(cg)),
+            "transceiversToGrid")
+    return g
+
+
+def p_src(g: TransceiverGrid):
+    return g.src[0]
+
+
+def p_rec(g: TransceiverGrid):
+    return g.rec[0]
+
+
+def vn_src(g: TransceiverGrid):
+    return g.vn_src
+
+
+def vn_rec(g: TransceiverGrid):
+    return g.vn_rec
+
+
+# ---------------------------------------------------------------------------
+# Time stepping (src/simulation.jl:542-557)
+# ---------------------------------------------------------------------------
+def run_fdtd(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | None, va=None,
+             start_step: int = 1, on_step=None, stop_step: int | None = None,
+             arith: str = "promote", ctx: Context | None = None) -> np.ndarray:
+    """run_fdtd!(dom, field, txs, cpml, va; start_step, on_step): advances
+    `field` (and the trace buffers and CPML memory) in place on the GPU.
+    on_step(it, read) is called after each step; read(c) returns channel c."""
+    ctx = ctx or default_context()
+    stop_step = int(d.nt) if stop_step is None else int(stop_step)
+    if field.dtype != np.float32 or not field.flags.f_contiguous:
+        raise ValueError("field must be a Fortran-ordered float32 array")
+    if field.shape != (d.nx, d.ny, d.nz, 4):
+        raise ValueError("field shape must be (nx, ny, nz, 4)")
+    mask = None
+    if va is not None:
+        mask = np.asfortranarray(va, dtype=np.uint8)
+    cg = txs._c()
+    cc = cpml._c() if cpml is not None else None
+    cb = L.STEP_CB()
+    if on_step is not None:
+        def _cb(it, _user):
+            def read(c):
+                out = np.zeros((d.nx, d.ny, d.nz), np.float32, order="F")
+                L.check(L.lib().adf_read_field(ctx.h, c, _p(out)), "adf_read_field")
+                return out
+            try:
+                r = on_step(int(it), read)
+            except Exception:  # a failing callback cancels the run
+                return 1
+            return 1 if r is False else 0
+        cb = L.STEP_CB(_cb)
+    L.check(L.lib().adf_run_fdtd(ctx.h, C.byref(d), _p(field), C.byref(cg),
+                                 C.byref(cc) if cc is not None else None, _p(mask),
+                                 int(start_step), stop_step, L.ARITH[arith], cb, None),
+            "run_fdtd")
+    return field
+
+
+def injection_coefficients(d: L.Domain, radius: float, n_points: int,
+                           ctx: Context | None = None):
+    """C_for_N on the GPU in FP64 -> (C_f, C_q, dS)."""
+    ctx = ctx or default_context()
+    out = np.zeros(3, np.float64)
+    L.check(L.lib().adf_injection_coefficients(ctx.h, C.byref(d), float(radius), int(n_points),
+                                               _p(out)), "injection_coefficients")
+    return float(out[0]), float(out[1]), float(out[2])

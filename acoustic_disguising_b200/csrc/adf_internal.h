@@ -1,0 +1,99 @@
+// adf_internal.h -- structures shared by the host runtime and the kernels.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace adf {
+
+// ---- HBM layout of one solve ----------------------------------------------
+// field : [2 buffers][4 channels P,Vx,Vy,Vz][nz][ny][nxp] Float32, x fastest.
+//         nxp = row pitch (multiple of 4 floats so rows are 16-B aligned).
+//         Step `it` reads buffer (it - it_first) & 1 and writes the other.
+// mask  : [nz][ny][mw] uint32, one nibble per cell (bit0 P, bit1 Vx,
+//         bit2 Vy, bit3 Vz open), cell x in word x/8, nibble x%8.
+// psi_p[a]: p-side CPML memory of axis a, [2 buffers][2 sides][...]:
+//         a=0: [nz][ny][npml]   a=1: [nz][npml][nxp]   a=2: [npml][ny][nxp]
+// psi_v[a]: v-side, the same with npml+1.
+// traces: src/rec/vn_src/vn_rec [nt][ntx] (transceiver fastest).
+enum : int {
+  SF_MASK = 1,      // solve has a scatterer mask
+  SF_PCPML = 2,     // p-side CPML active (npml>1, or npml>=1 with a mask)
+  SF_VCPML = 4,     // v-side CPML active (npml>=1)
+  SF_FP32 = 8,      // Float32 arithmetic instead of Float64 intermediates
+};
+
+struct SolveDev {
+  int nx, ny, nz, nxp;
+  int ty, nty;       // tile rows, number of y tiles
+  int npml, flags;
+  int nt;            // dom.nt
+  int it_base;       // 1-based step executed by launch-step 0 of a chunk
+  int it_stop;       // last step (inclusive) to execute
+  int it_first;      // step whose input field sits in buffer 0
+  int ntx, mw;
+  double fq, fv, rdx, rdy, rdz;
+  float fqf, fvf, rdxf, rdyf, rdzf;
+  float* field;
+  long long buf_stride;   // floats per field buffer (4*nz*ny*nxp)
+  long long chan_stride;  // floats per channel (nz*ny*nxp)
+  float* psi_p[3];
+  float* psi_v[3];
+  long long psi_p_buf[3], psi_v_buf[3];  // floats per psi buffer
+  long long psi_p_side[3], psi_v_side[3];
+  const float* coef;      // a_l a_r a_hl a_hr b_l b_r b_hl b_hr (Float32)
+  // injection / recording entries, grouped by (y tile, plane, channel)
+  const int* tp_off;      // nty*nz*4 + 1 offsets into seg
+  const int4* seg;        // {cell (row*nxp + x), first entry, count, 0}
+  const float* ent_w;
+  const int* ent_tx;
+  const int* ent_slot;    // contribution slot (c*ntx+tx)*8+corner or -1
+  float* contrib;         // [4][ntx][8]
+  const unsigned char* inb;  // [4][ntx] stencil in bounds
+  float* src[4];
+  float* rec[4];
+  float* vn_src;
+  float* vn_rec;
+  const float* dir;       // [ntx][4]
+  int* err;               // per-solve error word
+  int pad_;
+};
+
+// work item: {solve index, y tile, z0, z1}
+struct StepParams {
+  SolveDev* solves;
+  const CUtensorMap* tmaps;  // 3 per solve: field depth-1, field depth-2, mask
+  const int4* items;
+  int n_items;
+  int step;          // launch-step index within the chunk
+  int stages;
+  int stage_floats;  // ring slot stride (floats)
+  int pn_floats;     // one Pn plane buffer (floats)
+  int* err;          // launch-wide error word
+};
+
+struct EpiParams {
+  SolveDev* solves;
+  int n_solves;
+  int step;
+};
+
+// sizes of one ring slot for a solve (floats, each region 128-B aligned)
+inline __host__ __device__ int round32(long long v) { return (int)((v + 31) / 32 * 32); }
+inline __host__ __device__ int slot_region(int ty, int nxp) { return round32((long long)(ty + 2) * nxp); }
+inline __host__ __device__ int slot_floats(int ty, int nxp, int mw) {
+  return 3 * slot_region(ty, nxp) + round32(2LL * (ty + 2) * nxp) + round32((long long)(ty + 2) * mw);
+}
+inline __host__ __device__ int pn_plane_floats(int ty, int nxp) { return round32((long long)(ty + 1) * nxp); }
+
+// error codes written by kernels
+enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_DRAIN_TIMEOUT = 3 };
+
+// launch helpers implemented in fdtd_kernels.cu
+cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
+                        bool fp32);
+cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
+cudaError_t step_kernel_attributes(size_t smem, bool fp32);
+int consumer_threads();
+
+}  // namespace adf

@@ -1,0 +1,881 @@
+// runtime.cu -- host runtime behind the C-ABI (include/adfdtd.h).
+//
+// Owns device memory, builds the per-solve descriptors, entry lists and TMA
+// tensor maps, and drives the fused step kernel.  Layout conversions between
+// the reference's Julia arrays and the HBM layout (see adf_internal.h) happen
+// here, once per call.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/adfdtd.h"
+#include "adf_internal.h"
+#include "host_math.h"
+#include "runtime.h"
+
+namespace adf {
+cudaError_t launch_cpml_profiles(int n, double vel_max, double dt, double rcoef, double thickness,
+                                 double f0, float* out32, double* out64, cudaStream_t s);
+cudaError_t launch_mask(int kind, const double* params, const double* xs, const double* ys,
+                        const double* zs, int nx, int ny, int nz, int mw, uint32_t* bits,
+                        uint8_t* jl, cudaStream_t s);
+cudaError_t launch_pack_mask(const uint8_t* jl, int nx, int ny, int nz, int mw, uint32_t* bits,
+                             cudaStream_t s);
+cudaError_t launch_injection_coef(double radius, long long n, double dt, double rho, double dx,
+                                  double z0, double* out, cudaStream_t s);
+
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+static hm::Dom to_dom(const adf_domain& d) {
+  hm::Dom o;
+  o.tmax = d.tmax; o.xmax = d.xmax; o.ymax = d.ymax; o.zmax = d.zmax;
+  o.nx = d.nx; o.ny = d.ny; o.nz = d.nz;
+  o.c0 = d.c0; o.r0 = d.r0; o.cf = d.cf;
+  o.dx = d.dx; o.dy = d.dy; o.dz = d.dz;
+  o.fact_m0 = d.fact_m0; o.fact_m1 = d.fact_m1; o.dt = d.dt; o.nt = d.nt; o.z0 = d.z0;
+  return o;
+}
+
+// ---------------------------------------------------------------------------
+// Solve: device resources of one FDTD solve
+// ---------------------------------------------------------------------------
+Solve::~Solve() { release(); }
+
+void Solve::release() {
+  for (void* p : allocs)
+    if (p) cudaFree(p);
+  allocs.clear();
+}
+
+template <typename T>
+static T* dalloc(Solve& s, size_t n, int& rc) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    rc = fail(ADF_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  s.allocs.push_back(p);
+  s.bytes += n * sizeof(T);
+  return static_cast<T*>(p);
+}
+
+void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, int& mw) {
+  xh = (nx + 255) / 256;
+  int q = 4 * xh;
+  nxp = (nx + q - 1) / q * q;
+  mw = ((nx + 7) / 8 + 3) / 4 * 4;
+  const Tune t = tune_lookup(nx, ny, nz);
+  ty = t.ty;
+  nzc = t.nzc;
+  if (ty < 2) ty = 2;
+  if (ty > ny) ty = ny;
+  if (nzc < 2) nzc = 2;
+  if (nzc > nz) nzc = nz;
+}
+
+size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, int64_t ntx,
+                            int64_t nt, bool mask) {
+  int nxp, xh, ty, nzc, mw;
+  choose_tiles((int)nx, (int)ny, (int)nz, nxp, xh, ty, nzc, mw);
+  size_t b = 2ull * 4 * nz * ny * nxp * 4;
+  if (mask) b += (size_t)mw * ny * nz * 4;
+  size_t n = npml;
+  b += 2ull * 2 * 4 * (nz * ny * n + nz * n * nxp + n * ny * nxp);
+  b += 2ull * 2 * 4 * (nz * ny * (n + 1) + nz * (n + 1) * nxp + (n + 1) * ny * nxp);
+  b += 10ull * nt * ntx * 4;
+  b += (size_t)ntx * 4 * 8 * 4 * 3;  // contributions + entries
+  b += (size_t)((ny + ty - 1) / ty) * nz * 4 * 4;
+  return b + (1 << 20);
+}
+
+static int encode_tmaps(adf_ctx* ctx, Solve& s, int xh) {
+  SolveDev& d = s.dev;
+  const int bx = d.nxp / xh;
+  cuuint64_t dims[5] = {(cuuint64_t)(xh == 1 ? d.nx : bx), (cuuint64_t)xh, (cuuint64_t)d.ny,
+                        (cuuint64_t)d.nz, 8};
+  cuuint64_t strides[4] = {(cuuint64_t)bx * 4, (cuuint64_t)d.nxp * 4,
+                           (cuuint64_t)d.nxp * d.ny * 4, (cuuint64_t)d.nxp * d.ny * d.nz * 4};
+  cuuint32_t box[5] = {(cuuint32_t)bx, (cuuint32_t)xh, (cuuint32_t)(d.ty + 2), 1, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = ctx->encode(&s.tm[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, d.field, dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(field) failed: " + std::to_string((int)r));
+  box[3] = 2;
+  r = ctx->encode(&s.tm[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, d.field, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(vz) failed: " + std::to_string((int)r));
+  std::memset(&s.tm[2], 0, sizeof(CUtensorMap));
+  if (d.flags & SF_MASK) {
+    cuuint64_t md[3] = {(cuuint64_t)d.mw, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
+    cuuint64_t ms[2] = {(cuuint64_t)d.mw * 4, (cuuint64_t)d.mw * d.ny * 4};
+    cuuint32_t mb[3] = {(cuuint32_t)d.mw, (cuuint32_t)(d.ty + 2), 1};
+    r = ctx->encode(&s.tm[2], CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, (void*)s.mask_bits, md, ms, mb,
+                    es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(mask) failed: " + std::to_string((int)r));
+  }
+  return ADF_OK;
+}
+
+// Entry lists for interp_trilinear! (derivatives.jl:30-60): every in-bounds
+// (channel, transceiver) contributes its 8 stencil corners; corners are
+// grouped by (y tile, plane, channel) and, inside a cell, kept in
+// transceiver order (the order of the sequential reference loop).  P
+// corners on the last row of a tile are duplicated (slot -1) into the next
+// tile's halo row so that tile's velocity update sees the injection.
+static int build_entries(Solve& s, const float* const idx[4], const float* const w[4]) {
+  SolveDev& d = s.dev;
+  const int ntx = d.ntx, nx = d.nx, ny = d.ny, nz = d.nz, ty = d.ty, nxp = d.nxp;
+  struct E {
+    long long key;  // bucket * 2^32 + cell
+    int tx;
+    int slot;
+    float w;
+  };
+  std::vector<E> es;
+  es.reserve((size_t)ntx * 36);
+  std::vector<unsigned char> inb((size_t)4 * ntx, 0);
+  for (int c = 0; c < 4; ++c)
+    for (int tx = 0; tx < ntx; ++tx) {
+      const int I = (int)idx[c][3 * tx], J = (int)idx[c][3 * tx + 1], K = (int)idx[c][3 * tx + 2];
+      const bool ok = I >= 1 && I < nx && J >= 1 && J < ny && K >= 1 && K < nz;
+      inb[(size_t)c * ntx + tx] = ok;
+      if (!ok) continue;
+      for (int n = 0; n < 8; ++n) {
+        const int ii = n & 1, jj = (n >> 1) & 1, kk = n >> 2;
+        const int i = I - 1 + ii, j = J - 1 + jj, k = K - 1 + kk;
+        const float wv = w[c][8 * tx + n];
+        const int T = j / ty, r = j - T * ty + 1;
+        const long long bucket = ((long long)T * nz + k) * 4 + c;
+        es.push_back({(bucket << 32) | (long long)(r * nxp + i), tx, (c * ntx + tx) * 8 + n, wv});
+        if (c == 0 && (j + 1) % ty == 0 && j + 1 < ny) {
+          const long long b2 = ((long long)((j + 1) / ty) * nz + k) * 4;
+          es.push_back({(b2 << 32) | (long long)i, tx, -1, wv});
+        }
+      }
+    }
+  std::stable_sort(es.begin(), es.end(), [](const E& a, const E& b) {
+    return a.key < b.key || (a.key == b.key && a.tx < b.tx);
+  });
+  const long long nb = (long long)d.nty * nz * 4;
+  std::vector<int> off((size_t)nb + 1, 0);
+  std::vector<int4> seg;
+  std::vector<float> ew;
+  std::vector<int> etx, eslot;
+  ew.reserve(es.size());
+  etx.reserve(es.size());
+  eslot.reserve(es.size());
+  size_t i = 0;
+  long long cur_b = 0;
+  for (; i < es.size();) {
+    const long long b = es[i].key >> 32;
+    while (cur_b <= b) off[(size_t)cur_b++] = (int)seg.size();
+    size_t j = i;
+    while (j < es.size() && es[j].key == es[i].key) ++j;
+    int4 sg;
+    sg.x = (int)(es[i].key & 0xffffffffLL);
+    sg.y = (int)ew.size();
+    sg.z = (int)(j - i);
+    sg.w = 0;
+    for (size_t k = i; k < j; ++k) {
+      ew.push_back(es[k].w);
+      etx.push_back(es[k].tx);
+      eslot.push_back(es[k].slot);
+    }
+    seg.push_back(sg);
+    i = j;
+  }
+  while (cur_b <= nb) off[(size_t)cur_b++] = (int)seg.size();
+  int rc = ADF_OK;
+  int* d_off = dalloc<int>(s, off.size(), rc);
+  int4* d_seg = dalloc<int4>(s, seg.size(), rc);
+  float* d_w = dalloc<float>(s, ew.size(), rc);
+  int* d_tx = dalloc<int>(s, etx.size(), rc);
+  int* d_slot = dalloc<int>(s, eslot.size(), rc);
+  unsigned char* d_inb = dalloc<unsigned char>(s, inb.size(), rc);
+  float* d_contrib = dalloc<float>(s, (size_t)4 * ntx * 8, rc);
+  if (rc) return rc;
+  cudaStream_t st = s.stream;
+  cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st);
+  if (!seg.empty()) {
+    cudaMemcpyAsync(d_seg, seg.data(), seg.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_w, ew.data(), ew.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_tx, etx.data(), etx.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_slot, eslot.data(), eslot.size() * 4, cudaMemcpyHostToDevice, st);
+  }
+  cudaMemcpyAsync(d_inb, inb.data(), inb.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_contrib, 0, (size_t)4 * ntx * 8 * 4, st);
+  // the vectors must outlive the async copies
+  cudaStreamSynchronize(st);
+  d.tp_off = d_off;
+  d.seg = d_seg;
+  d.ent_w = d_w;
+  d.ent_tx = d_tx;
+  d.ent_slot = d_slot;
+  d.inb = d_inb;
+  d.contrib = d_contrib;
+  s.n_entries = (long long)ew.size();
+  return ADF_OK;
+}
+
+// Allocates everything except traces; field/psi zeroed.
+int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
+                int ntx) {
+  SolveDev& d = s.dev;
+  std::memset(&d, 0, sizeof(d));
+  s.stream = ctx->stream;
+  int xh;
+  choose_tiles((int)dom.nx, (int)dom.ny, (int)dom.nz, d.nxp, xh, d.ty, s.nzc, d.mw);
+  s.xh = xh;
+  d.nx = (int)dom.nx;
+  d.ny = (int)dom.ny;
+  d.nz = (int)dom.nz;
+  d.nty = (d.ny + d.ty - 1) / d.ty;
+  d.npml = npml;
+  d.nt = (int)dom.nt;
+  d.ntx = ntx;
+  d.flags = (has_mask ? SF_MASK : 0) | ((npml > 1 || (has_mask && npml >= 1)) ? SF_PCPML : 0) |
+            (npml >= 1 ? SF_VCPML : 0) | (arith == ADF_ARITH_FP32 ? SF_FP32 : 0);
+  d.fq = dom.fact_m0;
+  d.fv = dom.fact_m1;
+  d.rdx = 1.0 / dom.dx;
+  d.rdy = 1.0 / dom.dy;
+  d.rdz = 1.0 / dom.dz;
+  d.fqf = (float)dom.fact_m0;
+  d.fvf = (float)dom.fact_m1;
+  d.rdxf = 1.0f / (float)dom.dx;
+  d.rdyf = 1.0f / (float)dom.dy;
+  d.rdzf = 1.0f / (float)dom.dz;
+  d.chan_stride = (long long)d.nz * d.ny * d.nxp;
+  d.buf_stride = 4 * d.chan_stride;
+  int rc = ADF_OK;
+  d.field = dalloc<float>(s, (size_t)2 * d.buf_stride, rc);
+  if (rc) return rc;
+  cudaMemsetAsync(d.field, 0, (size_t)2 * d.buf_stride * 4, s.stream);
+  if (has_mask) {
+    s.mask_bits = dalloc<uint32_t>(s, (size_t)d.mw * d.ny * d.nz, rc);
+    if (rc) return rc;
+  }
+  const long long n = npml, nm = npml + 1, nxp = d.nxp, ny = d.ny, nz = d.nz;
+  const long long ps[3] = {nz * ny * n, nz * n * nxp, n * ny * nxp};
+  const long long vs[3] = {nz * ny * nm, nz * nm * nxp, nm * ny * nxp};
+  for (int a = 0; a < 3; ++a) {
+    d.psi_p_side[a] = ps[a];
+    d.psi_p_buf[a] = 2 * ps[a];
+    d.psi_v_side[a] = vs[a];
+    d.psi_v_buf[a] = 2 * vs[a];
+    if (npml > 0) {
+      d.psi_p[a] = dalloc<float>(s, (size_t)4 * ps[a], rc);
+      d.psi_v[a] = dalloc<float>(s, (size_t)4 * vs[a], rc);
+      if (rc) return rc;
+      cudaMemsetAsync(d.psi_p[a], 0, (size_t)4 * ps[a] * 4, s.stream);
+      cudaMemsetAsync(d.psi_v[a], 0, (size_t)4 * vs[a] * 4, s.stream);
+    }
+  }
+  float* coef = dalloc<float>(s, (size_t)8 * n + 4, rc);
+  if (rc) return rc;
+  cudaMemsetAsync(coef, 0, ((size_t)8 * n + 4) * 4, s.stream);
+  d.coef = coef;
+  s.coef_dev = coef;
+  int* e = dalloc<int>(s, 1, rc);
+  if (rc) return rc;
+  cudaMemsetAsync(e, 0, 4, s.stream);
+  d.err = e;
+  return ADF_OK;
+}
+
+int solve_alloc_traces(Solve& s, bool need_vsrc) {
+  SolveDev& d = s.dev;
+  const size_t n = (size_t)d.nt * d.ntx;
+  int rc = ADF_OK;
+  for (int c = 0; c < 4; ++c) {
+    d.rec[c] = dalloc<float>(s, n, rc);
+    if (rc) return rc;
+    cudaMemsetAsync(d.rec[c], 0, n * 4, s.stream);
+  }
+  for (int c = 0; c < 4; ++c) {
+    d.src[c] = dalloc<float>(s, n, rc);
+    if (rc) return rc;
+    cudaMemsetAsync(d.src[c], 0, n * 4, s.stream);
+  }
+  d.vn_src = dalloc<float>(s, n, rc);
+  d.vn_rec = dalloc<float>(s, n, rc);
+  float* dir = dalloc<float>(s, (size_t)4 * d.ntx, rc);
+  if (rc) return rc;
+  cudaMemsetAsync(d.vn_src, 0, n * 4, s.stream);
+  cudaMemsetAsync(d.vn_rec, 0, n * 4, s.stream);
+  d.dir = dir;
+  s.dir_dev = dir;
+  (void)need_vsrc;
+  return ADF_OK;
+}
+
+int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4]) {
+  int rc = build_entries(s, idx, w);
+  if (rc) return rc;
+  rc = encode_tmaps(ctx, s, s.xh);
+  if (rc) return rc;
+  // work items: z chunks outer, y tiles inner (neighbouring tiles run
+  // together so halo rows hit L2)
+  s.items.clear();
+  for (int z0 = 0; z0 < s.dev.nz; z0 += s.nzc)
+    for (int t = 0; t < s.dev.nty; ++t)
+      s.items.push_back(make_int4(0, t, z0, std::min(z0 + s.nzc, s.dev.nz)));
+  return ADF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batch: a set of solves advanced by one launch per step
+// ---------------------------------------------------------------------------
+Batch::~Batch() { release(); }
+void Batch::release() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  graph_exec = nullptr;
+  graph_steps = 0;
+  if (d_solves) cudaFree(d_solves);
+  if (d_tmaps) cudaFree(d_tmaps);
+  if (d_items) cudaFree(d_items);
+  if (d_err) cudaFree(d_err);
+  d_solves = nullptr;
+  d_tmaps = nullptr;
+  d_items = nullptr;
+  d_err = nullptr;
+  cap_solves = cap_items = 0;
+}
+
+int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
+  solves = list;
+  const int ns = (int)list.size();
+  std::vector<SolveDev> sd(ns);
+  std::vector<CUtensorMap> tm((size_t)3 * ns);
+  std::vector<int4> items;
+  int max_stage = 0, max_pn = 0;
+  max_ntx = 0;
+  for (int i = 0; i < ns; ++i) {
+    sd[i] = list[i]->dev;
+    for (int k = 0; k < 3; ++k) tm[(size_t)3 * i + k] = list[i]->tm[k];
+    const SolveDev& d = list[i]->dev;
+    max_stage = std::max(max_stage, slot_floats(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0));
+    max_pn = std::max(max_pn, pn_plane_floats(d.ty, d.nxp));
+    max_ntx = std::max(max_ntx, d.ntx);
+  }
+  // interleave items of different solves so the batch stays balanced
+  {
+    std::vector<size_t> pos(ns, 0);
+    bool any = true;
+    while (any) {
+      any = false;
+      for (int i = 0; i < ns; ++i) {
+        // a few consecutive items per solve keep neighbouring tiles together
+        for (int k = 0; k < 8 && pos[i] < list[i]->items.size(); ++k) {
+          int4 it = list[i]->items[pos[i]++];
+          it.x = i;
+          items.push_back(it);
+          any = true;
+        }
+      }
+    }
+  }
+  n_items = (int)items.size();
+  if (ns > cap_solves || n_items > cap_items) {
+    release();
+    cap_solves = std::max(ns, 1);
+    cap_items = std::max(n_items, 1);
+    if (cudaMalloc(&d_solves, sizeof(SolveDev) * cap_solves) != cudaSuccess ||
+        cudaMalloc(&d_tmaps, sizeof(CUtensorMap) * 3 * cap_solves) != cudaSuccess ||
+        cudaMalloc(&d_items, sizeof(int4) * cap_items) != cudaSuccess ||
+        cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADF_E_NOMEM, "batch descriptor allocation failed");
+    }
+  }
+  host_solves = sd;
+  cudaStream_t st = ctx->stream;
+  cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_tmaps, tm.data(), sizeof(CUtensorMap) * 3 * ns, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_err, 0, sizeof(int), st);
+  cudaStreamSynchronize(st);
+  stage_floats = max_stage;
+  pn_floats = max_pn;
+  // pipeline depth: as many slots as fit two CTAs per SM, else one CTA
+  const size_t fixed = 256 + (size_t)3 * pn_floats * 4;
+  const size_t per_cta2 = (size_t)ctx->smem_per_sm / 2 - 1024;
+  int stages = (int)((per_cta2 > fixed ? per_cta2 - fixed : 0) / ((size_t)stage_floats * 4));
+  if (stages < 3) {
+    const size_t per_cta1 = std::min((size_t)ctx->smem_optin, (size_t)ctx->smem_per_sm - 1024);
+    stages = (int)((per_cta1 - fixed) / ((size_t)stage_floats * 4));
+  }
+  stages = std::min(std::max(stages, 2), 6);
+  this->stages = stages;
+  smem = fixed + (size_t)stages * stage_floats * 4;
+  if (smem > (size_t)ctx->smem_optin) return fail(ADF_E_ARG, "grid too wide for shared memory");
+  if (step_kernel_attributes(smem, false) != cudaSuccess)
+    return fail(ADF_E_DEVICE, "cudaFuncSetAttribute failed");
+  int bps = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, step_kernel_ptr(), consumer_threads() + 32,
+                                                smem);
+  if (bps < 1) bps = 1;
+  grid = std::min(n_items, ctx->nsm * bps);
+  if (grid < 1) grid = 1;
+  if (graph_exec) {
+    cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    graph_steps = 0;
+  }
+  return ADF_OK;
+}
+
+int Batch::launch_step(adf_ctx* ctx, int step) {
+  StepParams p;
+  p.solves = d_solves;
+  p.tmaps = d_tmaps;
+  p.items = d_items;
+  p.n_items = n_items;
+  p.step = step;
+  p.stages = stages;
+  p.stage_floats = stage_floats;
+  p.pn_floats = pn_floats;
+  p.err = d_err;
+  if (adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, false) != cudaSuccess)
+    return fail(ADF_E_DEVICE, "step launch failed");
+  EpiParams e;
+  e.solves = d_solves;
+  e.n_solves = (int)solves.size();
+  e.step = step;
+  if (launch_epilogue(e, max_ntx, ctx->stream) != cudaSuccess)
+    return fail(ADF_E_DEVICE, "epilogue launch failed");
+  return ADF_OK;
+}
+
+// Runs `nsteps` launch-steps with step indices step0..step0+nsteps-1.  When
+// `use_graph`, chunks of `chunk` steps are captured once into a CUDA graph
+// whose last node advances it_base, and the graph is replayed.
+int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
+  if (!use_graph || nsteps < 2 * chunk) {
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = launch_step(ctx, s);
+      if (rc) return rc;
+      ctx->launches += 2;
+    }
+    return ADF_OK;
+  }
+  if (!graph_exec || graph_steps != chunk) {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return fail(ADF_E_DEVICE, "graph capture failed");
+    for (int s = 0; s < chunk; ++s) launch_step(ctx, s);
+    launch_advance(d_solves, (int)solves.size(), chunk, ctx->stream);
+    if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess)
+      return fail(ADF_E_DEVICE, "graph capture failed");
+    if (cudaGraphInstantiate(&graph_exec, g, 0) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(ADF_E_DEVICE, "graph instantiate failed");
+    }
+    cudaGraphDestroy(g);
+    graph_steps = chunk;
+  }
+  int done = 0;
+  while (nsteps - done >= chunk) {
+    if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
+      return fail(ADF_E_DEVICE, "graph launch failed");
+    ctx->launches += 2 * chunk + 1;
+    done += chunk;
+  }
+  for (int s = 0; s < nsteps - done; ++s) {
+    int rc = launch_step(ctx, s);
+    if (rc) return rc;
+    ctx->launches += 2;
+  }
+  // restore it_base on the host-side copy's semantics: the caller re-uploads
+  return ADF_OK;
+}
+
+int Batch::check_error(adf_ctx* ctx) {
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
+  if (h) return fail(ADF_E_TIMEOUT, "a bounded device-side wait gave up (code " + std::to_string(h) + ")");
+  return ADF_OK;
+}
+
+int Batch::upload_descriptors(adf_ctx* ctx) {
+  for (size_t i = 0; i < solves.size(); ++i) host_solves[i] = solves[i]->dev;
+  cudaMemcpyAsync(d_solves, host_solves.data(), sizeof(SolveDev) * solves.size(),
+                  cudaMemcpyHostToDevice, ctx->stream);
+  return ADF_OK;
+}
+
+}  // namespace adf
+
+using namespace adf;
+
+// ---------------------------------------------------------------------------
+// layout helpers
+// ---------------------------------------------------------------------------
+// Julia (nt, ntx) time-fastest  <->  device [nt][ntx] transceiver-fastest
+static void transpose_to_dev_layout(const float* jl, float* out, int64_t nt, int64_t ntx) {
+  const int64_t B = 64;
+  for (int64_t t0 = 0; t0 < nt; t0 += B)
+    for (int64_t x0 = 0; x0 < ntx; x0 += B)
+      for (int64_t x = x0; x < std::min(ntx, x0 + B); ++x)
+        for (int64_t t = t0; t < std::min(nt, t0 + B); ++t) out[t * ntx + x] = jl[t + nt * x];
+}
+static void transpose_to_julia(const float* dv, float* jl, int64_t nt, int64_t ntx) {
+  const int64_t B = 64;
+  for (int64_t x0 = 0; x0 < ntx; x0 += B)
+    for (int64_t t0 = 0; t0 < nt; t0 += B)
+      for (int64_t t = t0; t < std::min(nt, t0 + B); ++t)
+        for (int64_t x = x0; x < std::min(ntx, x0 + B); ++x) jl[t + nt * x] = dv[t * ntx + x];
+}
+
+static int upload_traces(Solve& s, const adf_txgrid* txs, cudaStream_t st) {
+  SolveDev& d = s.dev;
+  const int64_t nt = d.nt, ntx = d.ntx;
+  std::vector<float> tmp((size_t)(nt * ntx));
+  auto up = [&](const float* jl, float* dst) {
+    transpose_to_dev_layout(jl, tmp.data(), nt, ntx);
+    cudaMemcpy(dst, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice);
+  };
+  for (int c = 0; c < 4; ++c) {
+    up(txs->src[c], d.src[c]);
+    up(txs->rec[c], d.rec[c]);
+  }
+  up(txs->vn_src, d.vn_src);
+  up(txs->vn_rec, d.vn_rec);
+  cudaMemcpy(s.dir_dev, txs->dir, (size_t)4 * ntx * 4, cudaMemcpyHostToDevice);
+  (void)st;
+  return ADF_OK;
+}
+
+static int download_traces(Solve& s, adf_txgrid* txs) {
+  SolveDev& d = s.dev;
+  const int64_t nt = d.nt, ntx = d.ntx;
+  std::vector<float> tmp((size_t)(nt * ntx));
+  auto down = [&](const float* src, float* jl) {
+    cudaMemcpy(tmp.data(), src, tmp.size() * 4, cudaMemcpyDeviceToHost);
+    transpose_to_julia(tmp.data(), jl, nt, ntx);
+  };
+  for (int c = 0; c < 4; ++c) {
+    down(d.rec[c], txs->rec[c]);
+    if (c > 0) down(d.src[c], txs->src[c]);
+  }
+  down(d.vn_rec, txs->vn_rec);
+  return ADF_OK;
+}
+
+// psi: Julia (npml,ny,nz,2) / (nx,npml,nz,2) / (nx,ny,npml,2) <-> device
+static void psi_copy(Solve& s, int axis, bool vside, float* host, bool upload, int buffer) {
+  SolveDev& d = s.dev;
+  const long long n = vside ? d.npml + 1 : d.npml;
+  float* base = vside ? d.psi_v[axis] : d.psi_p[axis];
+  const long long side = vside ? d.psi_v_side[axis] : d.psi_p_side[axis];
+  float* dev = base + (long long)buffer * 2 * side;
+  if (axis == 0) {
+    size_t bytes = (size_t)2 * side * 4;
+    if (upload)
+      cudaMemcpy(dev, host, bytes, cudaMemcpyHostToDevice);
+    else
+      cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost);
+    return;
+  }
+  const size_t rows = axis == 1 ? (size_t)n * d.nz * 2 : (size_t)d.ny * n * 2;
+  if (upload)
+    cudaMemcpy2D(dev, (size_t)d.nxp * 4, host, (size_t)d.nx * 4, (size_t)d.nx * 4, rows,
+                 cudaMemcpyHostToDevice);
+  else
+    cudaMemcpy2D(host, (size_t)d.nx * 4, dev, (size_t)d.nxp * 4, (size_t)d.nx * 4, rows,
+                 cudaMemcpyDeviceToHost);
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int adf_version(void) { return 10000; }
+
+int adf_last_error(char* buf, size_t n) {
+  if (!buf || n == 0) return ADF_E_ARG;
+  std::snprintf(buf, n, "%s", g_err.c_str());
+  return ADF_OK;
+}
+
+int adf_ctx_create(int device, size_t hbm_budget, adf_ctx** out) {
+  if (!out) return fail(ADF_E_ARG, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, "no CUDA device available: this library has no CPU fallback");
+  }
+  if (device < 0 || device >= ndev) return fail(ADF_E_ARG, "bad device index");
+  if (cudaSetDevice(device) != cudaSuccess) return fail(ADF_E_DEVICE, "cudaSetDevice failed");
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major < 10) return fail(ADF_E_DEVICE, "this library is built for sm_100a (B200)");
+  auto* c = new adf_ctx();
+  c->device = device;
+  c->nsm = prop.multiProcessorCount;
+  c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
+  c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(ADF_E_DEVICE, "stream creation failed");
+  }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+  cudaDriverEntryPointQueryResult q;
+  void* fn = nullptr;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      !fn) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled unavailable");
+  }
+  c->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  *out = c;
+  return ADF_OK;
+}
+
+int adf_ctx_destroy(adf_ctx* c) {
+  if (!c) return ADF_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return ADF_OK;
+}
+
+int adf_domain_make(double tmax, double xmax, double ymax, double zmax, int64_t nx, int64_t ny,
+                    int64_t nz, double c0, double r0, double cf, adf_domain* o) {
+  if (!o || nx < 2 || ny < 2 || nz < 2 || !(c0 > 0) || !(cf > 0))
+    return fail(ADF_E_ARG, "bad domain arguments");
+  o->tmax = tmax; o->xmax = xmax; o->ymax = ymax; o->zmax = zmax;
+  o->nx = nx; o->ny = ny; o->nz = nz;
+  o->c0 = c0; o->r0 = r0; o->cf = cf;
+  o->dx = 2 * xmax / (double)(nx - 1);
+  o->dy = 2 * ymax / (double)(ny - 1);
+  o->dz = 2 * zmax / (double)(nz - 1);
+  o->dt = cf * std::min(o->dx, std::min(o->dy, o->dz)) / c0 / std::sqrt(3.0);
+  o->nt = (int64_t)std::ceil(tmax / o->dt);
+  o->fact_m0 = o->dt * r0 * (c0 * c0);
+  o->fact_m1 = o->dt / r0;
+  o->z0 = r0 * c0;
+  return ADF_OK;
+}
+
+int adf_coords(const adf_domain* d, int axis, int chan, double* out) {
+  if (!d || !out || axis < 0 || axis > 2 || chan < 0 || chan > 3)
+    return fail(ADF_E_ARG, "bad coords arguments");
+  hm::Range r = hm::axis_range(to_dom(*d), axis, chan);
+  for (int64_t i = 1; i <= r.len; ++i) out[i - 1] = r.at(i);
+  return ADF_OK;
+}
+
+int adf_time_axis(const adf_domain* d, double* out) {
+  if (!d || !out || d->nt < 1) return fail(ADF_E_ARG, "bad time axis arguments");
+  hm::Range r = hm::make_range(0.0, d->tmax, d->nt);
+  for (int64_t i = 1; i <= d->nt; ++i) out[i - 1] = r.at(i);
+  return ADF_OK;
+}
+
+int adf_cpml_profiles(adf_ctx* ctx, int64_t npml, double vel_max, double dt, double rcoef,
+                      double thickness, double fc, float* out32, double* out64) {
+  if (!ctx || npml < 0 || !out32) return fail(ADF_E_ARG, "bad cpml arguments");
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)(8 * npml + 4);
+  float* d32 = nullptr;
+  double* d64 = nullptr;
+  if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&d64, n * 8) != cudaSuccess)
+    return fail(ADF_E_NOMEM, "cudaMalloc failed");
+  launch_cpml_profiles((int)npml, vel_max, dt, rcoef, thickness, fc, d32, d64, ctx->stream);
+  cudaMemcpyAsync(out32, d32, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (out64) cudaMemcpyAsync(out64, d64, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d32);
+  cudaFree(d64);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+int adf_build_mask(adf_ctx* ctx, const adf_domain* d, int shape, const double* params,
+                   uint8_t* out_bool) {
+  if (!ctx || !d) return fail(ADF_E_ARG, "bad mask arguments");
+  if (shape == ADF_SHAPE_NONE) return 1;
+  if (shape < 0 || shape > 4) return fail(ADF_E_ARG, "unknown shape");
+  cudaSetDevice(ctx->device);
+  uint32_t* bits = nullptr;
+  uint8_t* jl = nullptr;
+  const int mw = (int)(((d->nx + 7) / 8 + 3) / 4 * 4);
+  int rc = build_mask_device(ctx, *d, shape, params, mw, &bits, out_bool ? &jl : nullptr);
+  if (rc) return rc;
+  if (out_bool)
+    cudaMemcpyAsync(out_bool, jl, (size_t)4 * d->nx * d->ny * d->nz, cudaMemcpyDeviceToHost,
+                    ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(bits);
+  if (jl) cudaFree(jl);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+int adf_pack_transceivers(const adf_domain* d, const double* points, const double* dirs,
+                          const double* tf, adf_txgrid* o) {
+  if (!d || !points || !dirs || !tf || !o) return fail(ADF_E_ARG, "NULL argument");
+  if (o->nt != d->nt) return fail(ADF_E_ARG, "txgrid nt must equal dom.nt");
+  return pack_transceivers_host(to_dom(*d), points, dirs, tf, o);
+}
+
+int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                 adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                 int flags, adf_step_cb cb, void* user) {
+  if (!ctx || !d || !field || !txs) return fail(ADF_E_ARG, "NULL argument");
+  if (txs->nt != d->nt) return fail(ADF_E_ARG, "txs.nt must equal dom.nt");
+  if (start_step < 1 || stop_step > d->nt) return fail(ADF_E_ARG, "step range outside 1..nt");
+  if (d->nx < 4 || d->ny < 4 || d->nz < 4) return fail(ADF_E_ARG, "grid must be at least 4^3");
+  if (d->nx > 512) return fail(ADF_E_ARG, "nx > 512 is not supported");
+  if (flags != ADF_ARITH_PROMOTE && flags != ADF_ARITH_FP32) return fail(ADF_E_ARG, "bad flags");
+  const int64_t npml = cpml ? cpml->npml : 0;
+  if (npml < 0 || (npml > 0 && !cpml->coef)) return fail(ADF_E_ARG, "bad cpml");
+  if (stop_step < start_step) return ADF_OK;
+  cudaSetDevice(ctx->device);
+  const size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
+  if (need > ctx->budget) return fail(ADF_E_BUDGET, "solve exceeds the context's HBM budget");
+  auto s = std::make_unique<Solve>();
+  const hm::Dom dom = to_dom(*d);
+  int rc = solve_alloc(ctx, *s, dom, (int)npml, mask != nullptr, flags, (int)txs->ntx);
+  if (!rc) rc = solve_alloc_traces(*s, true);
+  if (rc) return rc;
+  SolveDev& sd = s->dev;
+  // field -> buffer 0 (input of step start_step)
+  cudaMemcpy2D(sd.field, (size_t)sd.nxp * 4, field, (size_t)d->nx * 4, (size_t)d->nx * 4,
+               (size_t)d->ny * d->nz * 4, cudaMemcpyHostToDevice);
+  if (mask) {
+    uint8_t* jl = nullptr;
+    const size_t mb = (size_t)4 * d->nx * d->ny * d->nz;
+    if (cudaMalloc(&jl, mb) != cudaSuccess) return fail(ADF_E_NOMEM, "mask staging alloc failed");
+    cudaMemcpy(jl, mask, mb, cudaMemcpyHostToDevice);
+    launch_pack_mask(jl, sd.nx, sd.ny, sd.nz, sd.mw, s->mask_bits, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(jl);
+  }
+  if (npml > 0) {
+    cudaMemcpy(s->coef_dev, cpml->coef, (size_t)(8 * npml + 4) * 4, cudaMemcpyHostToDevice);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 2; ++b) {
+        if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], true, b);
+        if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], true, b);
+      }
+  }
+  upload_traces(*s, txs, ctx->stream);
+  const float* idx[4] = {txs->idx[0], txs->idx[1], txs->idx[2], txs->idx[3]};
+  const float* w[4] = {txs->w[0], txs->w[1], txs->w[2], txs->w[3]};
+  rc = solve_finalize(ctx, *s, idx, w);
+  if (rc) return rc;
+  sd.it_first = (int)start_step;
+  sd.it_base = (int)start_step;
+  sd.it_stop = (int)stop_step;
+  Batch b;
+  rc = b.setup(ctx, {s.get()});
+  if (rc) return rc;
+  const int nsteps = (int)(stop_step - start_step + 1);
+  ctx->launches = 0;
+  ctx->cur = s.get();
+  cudaEventRecord(ctx->ev0, ctx->stream);
+  if (!cb) {
+    rc = b.run(ctx, nsteps, true, kGraphChunk);
+  } else {
+    for (int k = 0; k < nsteps && !rc; ++k) {
+      rc = b.launch_step(ctx, k);
+      ctx->launches += 2;
+      if (rc) break;
+      ctx->cur_it = start_step + k;
+      cudaStreamSynchronize(ctx->stream);
+      if (cb(start_step + k, user)) rc = fail(ADF_E_CANCELLED, "cancelled by callback");
+    }
+  }
+  cudaEventRecord(ctx->ev1, ctx->stream);
+  int rc2 = b.check_error(ctx);
+  if (!rc) rc = rc2;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_ms = ms;
+  ctx->cur = nullptr;
+  if (rc) return rc;
+  // output buffer of the last executed step
+  const int fb = (int)((stop_step - start_step + 1) & 1);
+  cudaMemcpy2D(field, (size_t)d->nx * 4, sd.field + (size_t)fb * sd.buf_stride,
+               (size_t)sd.nxp * 4, (size_t)d->nx * 4, (size_t)d->ny * d->nz * 4,
+               cudaMemcpyDeviceToHost);
+  if (npml > 0)
+    for (int a = 0; a < 3; ++a) {
+      if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], false, fb);
+      if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], false, fb);
+    }
+  download_traces(*s, txs);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+int adf_read_field(adf_ctx* ctx, int chan, float* out) {
+  if (!ctx || !out || chan < 0 || chan > 3) return fail(ADF_E_ARG, "bad arguments");
+  if (!ctx->cur) return fail(ADF_E_STATE, "adf_read_field is only valid inside a step callback");
+  const SolveDev& sd = ctx->cur->dev;
+  const int fb = (int)((ctx->cur_it - sd.it_first + 1) & 1);
+  cudaMemcpy2D(out, (size_t)sd.nx * 4,
+               sd.field + (size_t)fb * sd.buf_stride + (size_t)chan * sd.chan_stride,
+               (size_t)sd.nxp * 4, (size_t)sd.nx * 4, (size_t)sd.ny * sd.nz,
+               cudaMemcpyDeviceToHost);
+  return ADF_OK;
+}
+
+int adf_last_timing(adf_ctx* ctx, double* ms, int64_t* launches) {
+  if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
+  if (ms) *ms = ctx->last_ms;
+  if (launches) *launches = ctx->launches;
+  return ADF_OK;
+}
+
+int adf_injection_coefficients(adf_ctx* ctx, const adf_domain* d, double radius, int64_t n,
+                               double* out) {
+  if (!ctx || !d || !out || n <= 0) return fail(ADF_E_ARG, "bad arguments");
+  cudaSetDevice(ctx->device);
+  double* dv = nullptr;
+  if (cudaMalloc(&dv, 3 * sizeof(double)) != cudaSuccess) return fail(ADF_E_NOMEM, "alloc");
+  launch_injection_coef(radius, n, d->dt, d->r0, d->dx, d->z0, dv, ctx->stream);
+  cudaMemcpyAsync(out, dv, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dv);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,102 @@
+// runtime.h -- host-side objects behind the C-ABI.
+#pragma once
+#include <cudaTypedefs.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/adfdtd.h"
+#include "adf_internal.h"
+#include "host_math.h"
+
+namespace adf {
+struct Solve;
+}
+
+struct adf_ctx {
+  int device = 0;
+  int nsm = 148;
+  int smem_per_sm = 233472;
+  int smem_optin = 232448;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  size_t budget = 0;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  struct adf::Solve* cur = nullptr;  // solve whose field adf_read_field reads
+  int64_t cur_it = 0;
+  double last_ms = 0.0;
+  int64_t launches = 0;
+};
+
+namespace adf {
+
+constexpr int kGraphChunk = 32;  // steps per captured CUDA graph
+
+int fail(int code, const std::string& msg);
+
+// Tile shape per grid size: rows per tile and z-chunk depth.  Chosen by the
+// autotuner (tune.cpp) and cached in a JSON table beside the library.
+struct Tune {
+  int ty;
+  int nzc;
+};
+Tune tune_lookup(int nx, int ny, int nz);
+int tune_store(int nx, int ny, int nz, Tune t);
+
+struct Solve {
+  SolveDev dev;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  CUtensorMap tm[3];
+  int nzc = 32;
+  int xh = 1;
+  uint32_t* mask_bits = nullptr;
+  float* coef_dev = nullptr;
+  float* dir_dev = nullptr;
+  long long n_entries = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<int4> items;  // {0, y tile, z0, z1}
+  ~Solve();
+  void release();
+};
+
+struct Batch {
+  std::vector<Solve*> solves;
+  std::vector<SolveDev> host_solves;
+  SolveDev* d_solves = nullptr;
+  CUtensorMap* d_tmaps = nullptr;
+  int4* d_items = nullptr;
+  int* d_err = nullptr;
+  int cap_solves = 0, cap_items = 0;
+  int n_items = 0, stages = 3, stage_floats = 0, pn_floats = 0, grid = 1, max_ntx = 0;
+  size_t smem = 0;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_steps = 0;
+  ~Batch();
+  void release();
+  int setup(adf_ctx* ctx, const std::vector<Solve*>& list);
+  int upload_descriptors(adf_ctx* ctx);
+  int launch_step(adf_ctx* ctx, int step);
+  int run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk);
+  int check_error(adf_ctx* ctx);
+};
+
+void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, int& mw);
+size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, int64_t ntx,
+                            int64_t nt, bool mask);
+int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
+                int ntx);
+int solve_alloc_traces(Solve& s, bool need_vsrc);
+int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4]);
+
+// set-up helpers (setup.cu)
+int build_mask_device(adf_ctx* ctx, const adf_domain& d, int shape, const double* params, int mw,
+                      uint32_t** bits, uint8_t** jl);
+int pack_transceivers_host(const hm::Dom& d, const double* points, const double* dirs,
+                           const double* tf, adf_txgrid* o);
+
+// kernels (fdtd_kernels.cu)
+cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s);
+const void* step_kernel_ptr();
+
+}  // namespace adf

@@ -1,0 +1,92 @@
+// tune.cpp -- tile-shape table for the step kernel.
+//
+// The fused step kernel's tile has `ty` rows (plus one recomputed halo row)
+// and streams `nzc` planes per work item.  bench/autotune runs sweep
+// candidate shapes per grid size and store the fastest in tune_table.json
+// next to the library; lookups fall back to a size-based default.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include <dlfcn.h>
+
+#include "runtime.h"
+
+namespace adf {
+
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, Tune> g_table;
+static bool g_loaded = false;
+
+static std::string table_path() {
+  const char* env = std::getenv("ADF_TUNE_TABLE");
+  if (env && *env) return env;
+  Dl_info info;
+  if (dladdr((void*)&table_path, &info) && info.dli_fname) {
+    std::string p = info.dli_fname;
+    size_t k = p.rfind('/');
+    if (k != std::string::npos) return p.substr(0, k + 1) + "tune_table.json";
+  }
+  return "tune_table.json";
+}
+
+// minimal parser for lines of the form  "nx,ny,nz": [ty, nzc],
+static void load_locked() {
+  g_loaded = true;
+  FILE* f = std::fopen(table_path().c_str(), "r");
+  if (!f) return;
+  char line[512];
+  while (std::fgets(line, sizeof line, f)) {
+    int nx, ny, nz, ty, nzc;
+    const char* q = std::strchr(line, '"');
+    if (!q) continue;
+    if (std::sscanf(q, "\"%d,%d,%d\": [%d, %d]", &nx, &ny, &nz, &ty, &nzc) == 5)
+      g_table[{nx, ny, nz}] = Tune{ty, nzc};
+  }
+  std::fclose(f);
+}
+
+static Tune default_tune(int nx, int ny, int nz) {
+  Tune t;
+  t.ty = nx > 256 ? 2 : 4;
+  t.nzc = nz >= 256 ? 32 : 16;
+  (void)ny;
+  return t;
+}
+
+Tune tune_lookup(int nx, int ny, int nz) {
+  const char* env = std::getenv("ADF_TILE");  // "ty,nzc" override for sweeps
+  if (env && *env) {
+    int ty = 0, nzc = 0;
+    if (std::sscanf(env, "%d,%d", &ty, &nzc) == 2 && ty > 0 && nzc > 0) return Tune{ty, nzc};
+  }
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  if (!g_loaded) load_locked();
+  auto it = g_table.find({nx, ny, nz});
+  if (it != g_table.end()) return it->second;
+  return default_tune(nx, ny, nz);
+}
+
+int tune_store(int nx, int ny, int nz, Tune t) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  if (!g_loaded) load_locked();
+  g_table[{nx, ny, nz}] = t;
+  FILE* f = std::fopen(table_path().c_str(), "w");
+  if (!f) return ADF_E_ARG;
+  std::fprintf(f, "{\n");
+  size_t k = 0;
+  for (auto& kv : g_table) {
+    std::fprintf(f, "  \"%d,%d,%d\": [%d, %d]%s\n", std::get<0>(kv.first), std::get<1>(kv.first),
+                 std::get<2>(kv.first), kv.second.ty, kv.second.nzc,
+                 ++k < g_table.size() ? "," : "");
+  }
+  std::fprintf(f, "}\n");
+  std::fclose(f);
+  return ADF_OK;
+}
+
+}  // namespace adf
