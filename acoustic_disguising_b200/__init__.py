@@ -8,7 +8,7 @@ from .api import (  # noqa: F401
     Context, default_context, Domain, coord, coords, t, fibonacci_sphere, impulsive_wavelet,
     ricker_wavelet, fib_sphere_area, cpml_profiles, split_profiles, Cpml, shape_params,
     build_update_mask, Transceiver, TransceiverGrid, transceivers_to_grid, p_src, p_rec, vn_src,
-    vn_rec, run_fdtd, injection_coefficients,
+    vn_rec, run_fdtd, injection_coefficients, GfRequest, gf_solve_batch, Server,
 )
 
 __all__ = [n for n in dir() if not n.startswith("_")]

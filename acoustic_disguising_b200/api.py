@@ -36,6 +36,22 @@ class Context:
             L.lib().adf_ctx_destroy(self.h)
             self.h = None
 
+    def set_kernel_timing(self, on: bool):
+        L.check(L.lib().adf_set_kernel_timing(self.h, int(bool(on))), "set_kernel_timing")
+
+    def kernel_timing(self, reset: bool = False):
+        ms = C.c_double()
+        n = C.c_int64()
+        L.check(L.lib().adf_kernel_timing(self.h, C.byref(ms), C.byref(n), int(reset)),
+                "kernel_timing")
+        return ms.value, n.value
+
+    def last_io_bytes(self):
+        h = C.c_int64()
+        d = C.c_int64()
+        L.check(L.lib().adf_last_io_bytes(self.h, C.byref(h), C.byref(d)), "last_io_bytes")
+        return h.value, d.value
+
     def last_timing(self):
         ms = C.c_double()
         n = C.c_int64()
@@ -356,3 +372,111 @@ def injection_coefficients(d: L.Domain, radius: float, n_points: int,
     L.check(L.lib().adf_injection_coefficients(ctx.h, C.byref(d), float(radius), int(n_points),
                                                _p(out)), "injection_coefficients")
     return float(out[0]), float(out[1]), float(out[2])
+
+
+# ---------------------------------------------------------------------------
+# Impulsive Green's-function solves (src/greens.jl:48-234)
+# ---------------------------------------------------------------------------
+@dataclass
+class GfRequest:
+    """One FDTD solve of impulsive_gfs: point source + receiver shell.
+
+    `src_direction` is [q, fx, fy, fz] ([1,0,0,0] is the :p source type,
+    [0, n] the :v type, greens.jl:154-155); receivers record p and v_n along
+    their outward normals.  Outputs p and vn are (nt, n_rec) Float32.
+    """
+
+    dom: L.Domain
+    src_point: np.ndarray
+    src_direction: np.ndarray
+    src_tf: np.ndarray
+    rec_points: np.ndarray
+    rec_normals: np.ndarray
+    npml: int = 10
+    pml_rcoef: float = 1e-4
+    pml_fc: float = 3e3
+    scatterer: str = "none"
+    scatterer_kw: dict = dc_field(default_factory=dict)
+    arith: str = "promote"
+    p: np.ndarray = None
+    vn: np.ndarray = None
+
+    def _c(self):
+        r = L.GfRequestC()
+        r.dom = self.dom
+        r.npml = int(self.npml)
+        r.pml_rcoef = float(self.pml_rcoef)
+        r.pml_fc = float(self.pml_fc)
+        r.shape = L.SHAPES[self.scatterer]
+        sp = shape_params(self.scatterer, **self.scatterer_kw)
+        for i in range(6):
+            r.shape_params[i] = sp[i]
+        for i in range(3):
+            r.src_point[i] = float(self.src_point[i])
+        for i in range(4):
+            r.src_dir[i] = float(self.src_direction[i])
+        self._tf = np.ascontiguousarray(self.src_tf, np.float64)
+        self._rp = np.ascontiguousarray(self.rec_points, np.float64).reshape(-1, 3)
+        self._rn = np.ascontiguousarray(self.rec_normals, np.float64).reshape(-1, 3)
+        n = self._rp.shape[0]
+        nt = int(self.dom.nt)
+        if self.p is None:
+            self.p = np.zeros((nt, n), np.float32, order="F")
+        if self.vn is None:
+            self.vn = np.zeros((nt, n), np.float32, order="F")
+        r.src_tf = self._tf.ctypes.data
+        r.n_rec = n
+        r.rec_points = self._rp.ctypes.data
+        r.rec_normals = self._rn.ctypes.data
+        r.flags = L.ARITH[self.arith]
+        r.out_p = self.p.ctypes.data
+        r.out_vn = self.vn.ctypes.data
+        return r
+
+
+def gf_solve_batch(reqs, batched: bool = True, ctx: Context | None = None):
+    """Run GF solves: batched (one launch per step for all resident solves,
+    graph-captured, HBM-budget admission) or the plain one-solve-per-launch
+    path.  Fills req.p / req.vn; returns (device_ms, kernel_launches)."""
+    ctx = ctx or default_context()
+    arr = (L.GfRequestC * len(reqs))(*[r._c() for r in reqs])
+    L.check(L.lib().adf_gf_solve_batch(ctx.h, len(reqs), arr, int(bool(batched))),
+            "gf_solve_batch")
+    return ctx.last_timing()
+
+
+class Server:
+    """Continuous-batching serving loop (adf_server_*)."""
+
+    def __init__(self, hbm_budget: int = 0, max_resident: int = 0, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        L.check(L.lib().adf_server_start(self.ctx.h, hbm_budget, max_resident, C.byref(h)),
+                "server_start")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, req: GfRequest) -> int:
+        rc = req._c()
+        i = C.c_int64()
+        L.check(L.lib().adf_server_submit(self.h, C.byref(rc), C.byref(i)), "server_submit")
+        self._keep[i.value] = (req, rc)
+        return i.value
+
+    def poll(self, rid: int):
+        st = C.c_int()
+        lat = C.c_double()
+        L.check(L.lib().adf_server_poll(self.h, rid, C.byref(st), C.byref(lat)), "server_poll")
+        return st.value, lat.value
+
+    def cancel(self, rid: int):
+        L.check(L.lib().adf_server_cancel(self.h, rid), "server_cancel")
+
+    def drain(self):
+        L.check(L.lib().adf_server_drain(self.h), "server_drain")
+
+    def stop(self):
+        if self.h:
+            rc = L.lib().adf_server_stop(self.h)
+            self.h = None
+            L.check(rc, "server_stop")

@@ -32,6 +32,7 @@ struct SolveDev {
   int it_stop;       // last step (inclusive) to execute
   int it_first;      // step whose input field sits in buffer 0
   int ntx, mw;
+  int src_ntx;            // columns of src[] (transceivers that inject)
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;
@@ -46,13 +47,13 @@ struct SolveDev {
   const int* tp_off;      // nty*nz*4 + 1 offsets into seg
   const int4* seg;        // {cell (row*nxp + x), first entry, count, 0}
   const float* ent_w;
-  const int* ent_tx;
+  const int* ent_tx;      // src column of the entry's transceiver, -1: no source
   const int* ent_slot;    // contribution slot (c*ntx+tx)*8+corner or -1
   float* contrib;         // [4][ntx][8]
   const unsigned char* inb;  // [4][ntx] stencil in bounds
-  float* src[4];
-  float* rec[4];
-  float* vn_src;
+  float* src[4];          // [nt][src_ntx]
+  float* rec[4];          // [nt][ntx]; rec[1..3] may be NULL (not kept)
+  float* vn_src;          // [nt][ntx] or NULL (no vn2v)
   float* vn_rec;
   const float* dir;       // [ntx][4]
   int* err;               // per-solve error word

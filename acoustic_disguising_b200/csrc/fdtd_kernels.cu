@@ -348,7 +348,7 @@ __device__ __forceinline__ void v_quad(const SolveDev& S, const PlaneCtx& c, int
 // corner order), then f += w*src[it].
 __device__ __forceinline__ void process_entries(const SolveDev& S, int b, int e, int chan,
                                                 float* cells, bool records, int it) {
-  const float* src = S.src[chan] + (long long)(it - 1) * S.ntx;
+  const float* src = S.src[chan] + (long long)(it - 1) * S.src_ntx;
   for (int si = b + (int)threadIdx.x; si < e; si += NCT) {
     const int4 sg = S.seg[si];
     float v = cells[sg.x];
@@ -356,7 +356,8 @@ __device__ __forceinline__ void process_entries(const SolveDev& S, int b, int e,
       const float w = S.ent_w[k];
       const int slot = S.ent_slot[k];
       if (records && slot >= 0) S.contrib[slot] = __fmul_rn(w, v);
-      v = __fadd_rn(v, __fmul_rn(w, src[S.ent_tx[k]]));
+      const int col = S.ent_tx[k];
+      if (col >= 0) v = __fadd_rn(v, __fmul_rn(w, src[col]));  // receivers: src == 0
     }
     cells[sg.x] = v;
   }
@@ -590,18 +591,20 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
     float r[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      r[c] = S.rec[c][row];
+      // a record buffer that is not kept starts every row at zero, as the
+      // reference's freshly packed rec (= src*0) does
+      r[c] = S.rec[c] ? S.rec[c][row] : 0.0f;
       if (S.inb[c * ntx + tx]) {
         const float* cb = S.contrib + ((long long)c * ntx + tx) * 8;
 #pragma unroll
         for (int k = 0; k < 8; ++k) r[c] = __fadd_rn(r[c], cb[k]);
-        S.rec[c][row] = r[c];
+        if (S.rec[c]) S.rec[c][row] = r[c];
       }
     }
     const float* d = S.dir + 4 * tx;
     S.vn_rec[row] =
         __fadd_rn(__fadd_rn(__fmul_rn(r[1], d[1]), __fmul_rn(r[2], d[2])), __fmul_rn(r[3], d[3]));
-    if (it < S.nt) {
+    if (S.vn_src && it < S.nt) {
       const long long nr = row + ntx;
       const float vs = S.vn_src[nr];
 #pragma unroll

@@ -38,15 +38,6 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-static hm::Dom to_dom(const adf_domain& d) {
-  hm::Dom o;
-  o.tmax = d.tmax; o.xmax = d.xmax; o.ymax = d.ymax; o.zmax = d.zmax;
-  o.nx = d.nx; o.ny = d.ny; o.nz = d.nz;
-  o.c0 = d.c0; o.r0 = d.r0; o.cf = d.cf;
-  o.dx = d.dx; o.dy = d.dy; o.dz = d.dz;
-  o.fact_m0 = d.fact_m0; o.fact_m1 = d.fact_m1; o.dt = d.dt; o.nt = d.nt; o.z0 = d.z0;
-  return o;
-}
 
 // ---------------------------------------------------------------------------
 // Solve: device resources of one FDTD solve
@@ -55,7 +46,12 @@ Solve::~Solve() { release(); }
 
 void Solve::release() {
   for (void* p : allocs)
-    if (p) cudaFree(p);
+    if (p) {
+      if (alloc_stream)
+        cudaFreeAsync(p, alloc_stream);
+      else
+        cudaFree(p);
+    }
   allocs.clear();
 }
 
@@ -63,7 +59,8 @@ template <typename T>
 static T* dalloc(Solve& s, size_t n, int& rc) {
   void* p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = s.alloc_stream ? cudaMallocAsync(&p, n * sizeof(T), s.alloc_stream)
+                                 : cudaMalloc(&p, n * sizeof(T));
   if (e != cudaSuccess) {
     cudaGetLastError();
     rc = fail(ADF_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
@@ -140,7 +137,8 @@ static int encode_tmaps(adf_ctx* ctx, Solve& s, int xh) {
 // transceiver order (the order of the sequential reference loop).  P
 // corners on the last row of a tile are duplicated (slot -1) into the next
 // tile's halo row so that tile's velocity update sees the injection.
-static int build_entries(Solve& s, const float* const idx[4], const float* const w[4]) {
+static int build_entries(Solve& s, const float* const idx[4], const float* const w[4],
+                         const int* src_col) {
   SolveDev& d = s.dev;
   const int ntx = d.ntx, nx = d.nx, ny = d.ny, nz = d.nz, ty = d.ty, nxp = d.nxp;
   struct E {
@@ -148,6 +146,7 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
     int tx;
     int slot;
     float w;
+    int col;        // src column, -1 when the transceiver never injects
   };
   std::vector<E> es;
   es.reserve((size_t)ntx * 36);
@@ -164,10 +163,12 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
         const float wv = w[c][8 * tx + n];
         const int T = j / ty, r = j - T * ty + 1;
         const long long bucket = ((long long)T * nz + k) * 4 + c;
-        es.push_back({(bucket << 32) | (long long)(r * nxp + i), tx, (c * ntx + tx) * 8 + n, wv});
+        const int col = src_col ? src_col[tx] : tx;
+        es.push_back({(bucket << 32) | (long long)(r * nxp + i), tx, (c * ntx + tx) * 8 + n, wv,
+                      col});
         if (c == 0 && (j + 1) % ty == 0 && j + 1 < ny) {
           const long long b2 = ((long long)((j + 1) / ty) * nz + k) * 4;
-          es.push_back({(b2 << 32) | (long long)i, tx, -1, wv});
+          es.push_back({(b2 << 32) | (long long)i, tx, -1, wv, col});
         }
       }
     }
@@ -196,7 +197,7 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
     sg.w = 0;
     for (size_t k = i; k < j; ++k) {
       ew.push_back(es[k].w);
-      etx.push_back(es[k].tx);
+      etx.push_back(es[k].col);
       eslot.push_back(es[k].slot);
     }
     seg.push_back(sg);
@@ -221,6 +222,7 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
     cudaMemcpyAsync(d_slot, eslot.data(), eslot.size() * 4, cudaMemcpyHostToDevice, st);
   }
   cudaMemcpyAsync(d_inb, inb.data(), inb.size(), cudaMemcpyHostToDevice, st);
+  s.h2d += (int64_t)(off.size() * 4 + seg.size() * sizeof(int4) + ew.size() * 12 + inb.size());
   cudaMemsetAsync(d_contrib, 0, (size_t)4 * ntx * 8 * 4, st);
   // the vectors must outlive the async copies
   cudaStreamSynchronize(st);
@@ -234,6 +236,13 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
   s.n_entries = (long long)ew.size();
   return ADF_OK;
 }
+
+template <typename T>
+T* solve_dalloc(Solve& s, size_t n, int& rc) {
+  return dalloc<T>(s, n, rc);
+}
+template float* solve_dalloc<float>(Solve&, size_t, int&);
+template int* solve_dalloc<int>(Solve&, size_t, int&);
 
 // Allocates everything except traces; field/psi zeroed.
 int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
@@ -304,6 +313,7 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
 int solve_alloc_traces(Solve& s, bool need_vsrc) {
   SolveDev& d = s.dev;
   const size_t n = (size_t)d.nt * d.ntx;
+  d.src_ntx = d.ntx;
   int rc = ADF_OK;
   for (int c = 0; c < 4; ++c) {
     d.rec[c] = dalloc<float>(s, n, rc);
@@ -327,8 +337,9 @@ int solve_alloc_traces(Solve& s, bool need_vsrc) {
   return ADF_OK;
 }
 
-int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4]) {
-  int rc = build_entries(s, idx, w);
+int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4],
+                   const int* src_col) {
+  int rc = build_entries(s, idx, w, src_col);
   if (rc) return rc;
   rc = encode_tmaps(ctx, s, s.xh);
   if (rc) return rc;
@@ -454,8 +465,11 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   p.stage_floats = stage_floats;
   p.pn_floats = pn_floats;
   p.err = d_err;
+  const bool timed = ctx->kernel_timing && 2 * step + 1 < (int)ctx->kev.size();
+  if (timed) cudaEventRecord(ctx->kev[2 * step], ctx->stream);
   if (adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, false) != cudaSuccess)
     return fail(ADF_E_DEVICE, "step launch failed");
+  if (timed) cudaEventRecord(ctx->kev[2 * step + 1], ctx->stream);
   EpiParams e;
   e.solves = d_solves;
   e.n_solves = (int)solves.size();
@@ -508,6 +522,59 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
   }
   // restore it_base on the host-side copy's semantics: the caller re-uploads
   return ADF_OK;
+}
+
+// One chunk of `n` launch-steps followed by the it_base advance: replayed from
+// a captured graph when n == chunk, launched directly otherwise.
+int Batch::run_chunk(adf_ctx* ctx, int n, int chunk) {
+  if (n == chunk) {
+    if (!graph_exec || graph_steps != chunk) {
+      if (graph_exec) cudaGraphExecDestroy(graph_exec);
+      graph_exec = nullptr;
+      cudaGraph_t g;
+      if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(ADF_E_DEVICE, "graph capture failed");
+      for (int s = 0; s < chunk; ++s) launch_step(ctx, s);
+      launch_advance(d_solves, (int)solves.size(), chunk, ctx->stream);
+      if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess)
+        return fail(ADF_E_DEVICE, "graph capture failed");
+      if (cudaGraphInstantiate(&graph_exec, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(ADF_E_DEVICE, "graph instantiate failed");
+      }
+      cudaGraphDestroy(g);
+      graph_steps = chunk;
+    }
+    if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
+      return fail(ADF_E_DEVICE, "graph launch failed");
+    ctx->launches += 2 * chunk + 1;
+    return ADF_OK;
+  }
+  for (int s = 0; s < n; ++s) {
+    int rc = launch_step(ctx, s);
+    if (rc) return rc;
+  }
+  launch_advance(d_solves, (int)solves.size(), n, ctx->stream);
+  ctx->launches += 2 * n + 1;
+  return ADF_OK;
+}
+
+int Batch::run_advance(adf_ctx* ctx, int n) {
+  if (launch_advance(d_solves, (int)solves.size(), n, ctx->stream) != cudaSuccess)
+    return fail(ADF_E_DEVICE, "advance launch failed");
+  ctx->launches += 1;
+  return ADF_OK;
+}
+
+void Batch::collect_kernel_times(adf_ctx* ctx, int n) {
+  if (!ctx->kernel_timing) return;
+  for (int s = 0; s < n && 2 * s + 1 < (int)ctx->kev.size(); ++s) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ctx->kev[2 * s], ctx->kev[2 * s + 1]) == cudaSuccess) {
+      ctx->kernel_ms += ms;
+      ++ctx->kernel_launches;
+    }
+  }
 }
 
 int Batch::check_error(adf_ctx* ctx) {
@@ -666,6 +733,7 @@ int adf_ctx_destroy(adf_ctx* c) {
   if (!c) return ADF_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  for (auto& e : c->kev) cudaEventDestroy(e);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaStreamDestroy(c->stream);
@@ -797,7 +865,7 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
   upload_traces(*s, txs, ctx->stream);
   const float* idx[4] = {txs->idx[0], txs->idx[1], txs->idx[2], txs->idx[3]};
   const float* w[4] = {txs->w[0], txs->w[1], txs->w[2], txs->w[3]};
-  rc = solve_finalize(ctx, *s, idx, w);
+  rc = solve_finalize(ctx, *s, idx, w, nullptr);
   if (rc) return rc;
   sd.it_first = (int)start_step;
   sd.it_base = (int)start_step;
@@ -807,6 +875,18 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
   if (rc) return rc;
   const int nsteps = (int)(stop_step - start_step + 1);
   ctx->launches = 0;
+  {
+    const int64_t ntr = (int64_t)d->nt * txs->ntx * 4;
+    ctx->h2d_bytes = (int64_t)d->nx * d->ny * d->nz * 16 + 10 * ntr + txs->ntx * 16 +
+                     (mask ? 4 * d->nx * d->ny * d->nz : 0) + s->h2d;
+    ctx->d2h_bytes = (int64_t)d->nx * d->ny * d->nz * 16 + 8 * ntr;
+    if (npml > 0) {
+      const int64_t psi = 2 * 2 * npml * (d->ny * d->nz + d->nx * d->nz + d->nx * d->ny) * 4 +
+                          2 * 2 * (npml + 1) * (d->ny * d->nz + d->nx * d->nz + d->nx * d->ny) * 4;
+      ctx->h2d_bytes += psi + (8 * npml + 4) * 4;
+      ctx->d2h_bytes += psi / 2;
+    }
+  }
   ctx->cur = s.get();
   cudaEventRecord(ctx->ev0, ctx->stream);
   if (!cb) {
@@ -861,6 +941,35 @@ int adf_last_timing(adf_ctx* ctx, double* ms, int64_t* launches) {
   if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
   if (ms) *ms = ctx->last_ms;
   if (launches) *launches = ctx->launches;
+  return ADF_OK;
+}
+
+int adf_set_kernel_timing(adf_ctx* ctx, int on) {
+  if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
+  ctx->kernel_timing = on != 0;
+  if (on && ctx->kev.empty()) {
+    ctx->kev.resize(2 * kGraphChunk);
+    for (auto& e : ctx->kev) cudaEventCreate(&e);
+  }
+  // graphs captured without (or with) event nodes are re-captured lazily
+  return ADF_OK;
+}
+
+int adf_last_io_bytes(adf_ctx* ctx, int64_t* h2d, int64_t* d2h) {
+  if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
+  if (h2d) *h2d = ctx->h2d_bytes;
+  if (d2h) *d2h = ctx->d2h_bytes;
+  return ADF_OK;
+}
+
+int adf_kernel_timing(adf_ctx* ctx, double* ms, int64_t* n, int reset) {
+  if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
+  if (ms) *ms = ctx->kernel_ms;
+  if (n) *n = ctx->kernel_launches;
+  if (reset) {
+    ctx->kernel_ms = 0.0;
+    ctx->kernel_launches = 0;
+  }
   return ADF_OK;
 }
 

@@ -26,6 +26,12 @@ struct adf_ctx {
   int64_t cur_it = 0;
   double last_ms = 0.0;
   int64_t launches = 0;
+  // per-launch timing of the step kernel
+  int64_t h2d_bytes = 0, d2h_bytes = 0;  // traffic of the last call
+  bool kernel_timing = false;
+  std::vector<cudaEvent_t> kev;  // 2 per launch-step of a chunk
+  double kernel_ms = 0.0;
+  int64_t kernel_launches = 0;
 };
 
 namespace adf {
@@ -33,6 +39,16 @@ namespace adf {
 constexpr int kGraphChunk = 32;  // steps per captured CUDA graph
 
 int fail(int code, const std::string& msg);
+
+inline hm::Dom to_dom(const adf_domain& d) {
+  hm::Dom o;
+  o.tmax = d.tmax; o.xmax = d.xmax; o.ymax = d.ymax; o.zmax = d.zmax;
+  o.nx = d.nx; o.ny = d.ny; o.nz = d.nz;
+  o.c0 = d.c0; o.r0 = d.r0; o.cf = d.cf;
+  o.dx = d.dx; o.dy = d.dy; o.dz = d.dz;
+  o.fact_m0 = d.fact_m0; o.fact_m1 = d.fact_m1; o.dt = d.dt; o.nt = d.nt; o.z0 = d.z0;
+  return o;
+}
 
 // Tile shape per grid size: rows per tile and z-chunk depth.  Chosen by the
 // autotuner (tune.cpp) and cached in a JSON table beside the library.
@@ -53,8 +69,11 @@ struct Solve {
   uint32_t* mask_bits = nullptr;
   float* coef_dev = nullptr;
   float* dir_dev = nullptr;
+  float* stage = nullptr;  // output staging of GF solves
+  int64_t h2d = 0;         // bytes uploaded while setting this solve up
   long long n_entries = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation when set
   std::vector<int4> items;  // {0, y tile, z0, z1}
   ~Solve();
   void release();
@@ -78,6 +97,9 @@ struct Batch {
   int upload_descriptors(adf_ctx* ctx);
   int launch_step(adf_ctx* ctx, int step);
   int run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk);
+  int run_chunk(adf_ctx* ctx, int n, int chunk);
+  void collect_kernel_times(adf_ctx* ctx, int n);
+  int run_advance(adf_ctx* ctx, int n);  // after the stream is synchronised
   int check_error(adf_ctx* ctx);
 };
 
@@ -87,7 +109,10 @@ size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, in
 int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
                 int ntx);
 int solve_alloc_traces(Solve& s, bool need_vsrc);
-int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4]);
+int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const float* const w[4],
+                   const int* src_col);
+template <typename T>
+T* solve_dalloc(Solve& s, size_t n, int& rc);
 
 // set-up helpers (setup.cu)
 int build_mask_device(adf_ctx* ctx, const adf_domain& d, int shape, const double* params, int mw,

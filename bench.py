@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark: impulsive Green's-function solves/s on the 256^3 GF-retrieval
+workload (rigid sphere scatterer, 10-cell CPML, 2048-point shell, 2000
+steps per solve), batched through the C-ABI on B200.
+
+One bench step = one call of adf_gf_solve_batch over `--batch` complete
+solves (B sources of the 512-point Fibonacci source sphere): set-up, 2000
+time steps for all B solves advanced together (one persistent launch per
+time step, graph-captured), and the p / v_n traces copied back.
+
+  value : GF solves/s from device time (CUDA events on the library's
+          stream around the stepping of each batch; inputs resident)
+  e2e   : GF solves/s from the wall clock around the C-ABI call with host
+          buffers (set-up uploads and trace downloads inside)
+  roofline : the fused step kernel's algorithmic HBM bytes per launch over
+          its mean launch time (per-launch CUDA events), against the
+          measured copy bandwidth
+
+`--impl reference` times the CPU restatement of the reference's Threads
+path (oracle/) on this host's cores on a bounded sample of the same solve.
+Multi-GPU (torchrun): each rank runs its own disjoint sources (weak
+scaling, no collective in the data path); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 256
+DX = 0.005
+C0, RHO = 343.0, 1.2
+NT = 2000
+NPML = 10
+N_SRC, R_SRC = 512, 60 * DX
+N_REC, R_REC = 2048, 45 * DX
+R_SPHERE = 24 * DX
+F3DB = 2000.0
+PML_FC = 2000.0
+METRIC = "GF solves/s"
+
+
+def dt_of():
+    return 0.5 * DX / C0 / math.sqrt(3.0)
+
+
+def tmax_of(nt):
+    return (nt - 0.5) * dt_of()
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=8, help="solves per bench step and rank")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--arith", default="promote", choices=["promote", "fp32"])
+    ap.add_argument("--cpu-steps", type=int, default=40,
+                    help="time steps of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nt", type=int, default=NT,
+                    help="steps per solve (profiling runs only; the metric uses 2000)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload_config(batch, n_gpus):
+    return {"workload": "impulsive GF retrieval, 256^3 grid (dx=5 mm, air c0=343 rho=1.2, "
+                        "CFL 0.5), rigid sphere r=24 cells, 10-cell CPML (fc 2 kHz, R=1e-4), "
+                        "q point sources on a 512-point Fibonacci sphere r=60 cells, p+vn "
+                        "recorded on a 2048-point shell r=45 cells, 2000 steps per solve",
+            "grid": [N, N, N], "steps_per_solve": NT, "solves_per_step": batch,
+            "solves_per_step_all_ranks": batch * n_gpus, "source_wavelet":
+                "impulsive_wavelet f_3db=2 kHz", "l2": "fields 268 MB/solve > 126 MB L2",
+            "parallelism": f"independent solves sharded over {n_gpus} GPU(s)"}
+
+
+def make_requests(A, first_source, batch, arith, nt=NT):
+    d = A.Domain(tmax=tmax_of(nt), xmax=(N - 1) * DX / 2, nx=N, c0=C0, r0=RHO, cf=0.5)
+    assert d.nt == nt
+    tf, _ = A.impulsive_wavelet(d, F3DB)
+    sp, _ = A.fibonacci_sphere(N_SRC, R_SRC)
+    rp, rn = A.fibonacci_sphere(N_REC, R_REC)
+    reqs = []
+    for b in range(batch):
+        k = (first_source + b) % N_SRC
+        reqs.append(A.GfRequest(d, sp[k], [1.0, 0.0, 0.0, 0.0], tf, rp, rn, npml=NPML,
+                                pml_rcoef=1e-4, pml_fc=PML_FC, scatterer="sphere",
+                                scatterer_kw=dict(radius=R_SPHERE), arith=arith))
+    return d, reqs
+
+
+def algorithmic_bytes_per_solve_step():
+    cells = N ** 3
+    field = 32.0 * cells + 0.5 * cells  # 4 fields read + written, 4-bit mask
+    psi = 8.0 * 6 * NPML * N * N + 8.0 * 6 * (NPML + 1) * N * N  # p- and v-side slabs, r+w
+    return field + psi
+
+
+def read_traffic():
+    """dram bytes per cell-step of the step kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "fdtd_step_256cube.md")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("traffic_bytes_per_cell_step:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement of the reference (oracle/) on this host
+# ---------------------------------------------------------------------------
+def cpu_sample(steps, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+
+    O.build()
+    d = O.domain(tmax=tmax_of(NT), xmax=(N - 1) * DX / 2, nx=N, c0=C0, r0=RHO, cf=0.5)
+    tf, _ = O.impulsive_wavelet(d, F3DB)
+    sp, _ = O.fibonacci_sphere(N_SRC, R_SRC)
+    rp, rn = O.fibonacci_sphere(N_REC, R_REC)
+    pts = np.vstack([sp[0], rp])
+    dirs = np.vstack([[1.0, 0, 0, 0], np.hstack([np.zeros((N_REC, 1)), rn])])
+    tfs = np.vstack([tf, np.zeros((N_REC, d.nt))])
+    g = O.transceivers_to_grid(d, pts, dirs, tfs)
+    cp = O.CpmlState(d, NPML, 1e-4, PML_FC)
+    m = O.build_update_mask(d, "sphere", radius=R_SPHERE)
+    f = np.zeros((N, N, N, 4), np.float32, order="F")
+    O.run_fdtd(d, f, g, cp, m, start_step=1, stop_step=1, nthreads=threads)  # warm
+    t0 = time.perf_counter()
+    O.run_fdtd(d, f, g, cp, m, start_step=2, stop_step=1 + steps, nthreads=threads)
+    sec = time.perf_counter() - t0
+    return sec / steps
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    per = []
+    t_all = time.perf_counter()
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(max(2, args.cpu_steps // 10), threads)
+        if i >= args.warmup:
+            per.append(s)
+    sec_per_step = statistics.mean(per)
+    sps = 1.0 / (NT * sec_per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec_per_step * 1e3 * NT, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 intermediates, f32 storage", "data": "synthetic",
+        "config": workload_config(1, 1),
+        "cpu_baseline": {"value": sps, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{max(2, args.cpu_steps // 10)} time steps of one solve per "
+                                   "bench step, extrapolated to 2000 steps"},
+        "e2e": {"value": sps, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "CPU restatement (oracle/) of the reference's Threads path; the reference is "
+                "Julia and no Julia runtime is available",
+        "wall_s": time.perf_counter() - t_all,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def b200_arm(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import acoustic_disguising_b200 as A
+
+    if not os.path.exists(A.LIB_PATH):
+        A.build()
+    ctx = A.Context(local)
+    ctx.set_kernel_timing(True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce_max(x):
+        if dist is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    B = args.batch
+    step_ix = 0
+
+    def one_step():
+        nonlocal step_ix
+        first = (step_ix * world + rank) * B
+        step_ix += 1
+        _, reqs = make_requests(A, first, B, args.arith, args.nt)
+        t0 = time.perf_counter()
+        A.gf_solve_batch(reqs, batched=True, ctx=ctx)
+        wall = time.perf_counter() - t0
+        dev_ms, launches = ctx.last_timing()
+        h2d, d2h = ctx.last_io_bytes()
+        return wall, dev_ms, launches, h2d, d2h
+
+    for _ in range(args.warmup):
+        one_step()
+    ctx.kernel_timing(reset=True)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    t_region = time.perf_counter()
+    walls, devs, launches, h2ds, d2hs = [], [], 0, [], []
+    for _ in range(args.steps):
+        w, dm, ln, h2d, d2h = one_step()
+        walls.append(w)
+        devs.append(dm)
+        launches += ln + 4 * B  # + per-solve set-up/extract kernels (cpml, mask, 2 extracts)
+        h2ds.append(h2d)
+        d2hs.append(d2h)
+    barrier()
+    region = time.perf_counter() - t_region
+    clk = clocks.stop()
+    k_ms, k_n = ctx.kernel_timing(reset=True)
+    dev_total = reduce_max(sum(devs))
+    wall_total = reduce_max(sum(walls))
+    k_avg_ms = reduce_max(k_ms / max(k_n, 1))
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    solves = world * B * args.steps * args.nt / NT  # solve-equivalents of 2000 steps
+    value = solves / (dev_total / 1e3)
+    e2e = solves / wall_total
+    bytes_launch = B * algorithmic_bytes_per_solve_step()
+    achieved = bytes_launch / (k_avg_ms / 1e3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_note = "measured (MEASURED_PEAKS.json hbm_gbs)" if peak else "fallback 6650"
+    peak = peak or 6650.0
+    tpc = read_traffic()
+    cells = N ** 3
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 intermediates, f32 storage" if args.arith == "promote" else "f32",
+        "data": "synthetic (seeded geometry, reference wavelets; no dataset)",
+        "config": workload_config(B, world),
+        "e2e": {"value": e2e, "unit": "solves/s",
+                "h2d_bytes_per_step": int(statistics.mean(h2ds)),
+                "d2h_bytes_per_step": int(statistics.mean(d2hs))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_note,
+                     "traffic": (tpc * cells * B) if tpc else None,
+                     "kernel": "adf_fdtd_step_kernel", "bytes_per_launch": bytes_launch,
+                     "mean_launch_ms": k_avg_ms, "launches_timed": k_n},
+        "gcell_upd_per_s": cells * NT * solves / (dev_total / 1e3) / 1e9,
+        "clocks": clk,
+        "region_wall_s": region,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sec = cpu_sample(args.cpu_steps, threads)
+        line["cpu_baseline"] = {
+            "value": 1.0 / (NT * sec), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{args.cpu_steps} time steps of one solve of this workload on the CPU "
+                      "restatement of the reference (oracle/), extrapolated to 2000 steps"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

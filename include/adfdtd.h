@@ -155,6 +155,16 @@ int adf_read_field(adf_ctx* ctx, int chan, float* out);
  * of kernels that call launched.                                           */
 int adf_last_timing(adf_ctx* ctx, double* device_ms, int64_t* kernel_launches);
 
+/* Per-launch CUDA-event timing of the fused step kernel (events recorded on
+ * the context stream around every step launch, inside captured graphs
+ * too).  Off by default.  adf_kernel_timing returns the summed device time
+ * and launch count since the last reset.                                   */
+int adf_set_kernel_timing(adf_ctx* ctx, int on);
+/* Host->device and device->host bytes copied by the most recent
+ * adf_run_fdtd / adf_gf_solve_batch call.                                  */
+int adf_last_io_bytes(adf_ctx* ctx, int64_t* h2d, int64_t* d2h);
+int adf_kernel_timing(adf_ctx* ctx, double* step_kernel_ms, int64_t* step_launches, int reset);
+
 /* ---- Impulsive Green's-function solves (impulsive_gfs, src/greens.jl:48-234) ----
  * One request = one FDTD solve: a point source at `src_point` with
  * direction {q,fx,fy,fz} driven by `src_tf` (nt Float64), recording p and
