@@ -438,8 +438,8 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   this->stages = stages;
   smem = fixed + (size_t)stages * stage_floats * 4;
   if (smem > (size_t)ctx->smem_optin) return fail(ADF_E_ARG, "grid too wide for shared memory");
-  if (step_kernel_attributes(smem, false) != cudaSuccess)
-    return fail(ADF_E_DEVICE, "cudaFuncSetAttribute failed");
+  if (cudaError_t ea = step_kernel_attributes(smem, false); ea != cudaSuccess)
+    return fail(ADF_E_DEVICE, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(ea));
   int bps = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, step_kernel_ptr(), consumer_threads() + 32,
                                                 smem);
@@ -466,16 +466,28 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   p.pn_floats = pn_floats;
   p.err = d_err;
   const bool timed = ctx->kernel_timing && 2 * step + 1 < (int)ctx->kev.size();
-  if (timed) cudaEventRecord(ctx->kev[2 * step], ctx->stream);
-  if (adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, false) != cudaSuccess)
-    return fail(ADF_E_DEVICE, "step launch failed");
-  if (timed) cudaEventRecord(ctx->kev[2 * step + 1], ctx->stream);
-  EpiParams e;
-  e.solves = d_solves;
-  e.n_solves = (int)solves.size();
-  e.step = step;
-  if (launch_epilogue(e, max_ntx, ctx->stream) != cudaSuccess)
-    return fail(ADF_E_DEVICE, "epilogue launch failed");
+  // inside stream capture an event record must be an external node to be
+  // a timing point on every replay
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (timed) cudaStreamIsCapturing(ctx->stream, &cap);
+  const unsigned evf =
+      cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if (timed && cudaEventRecordWithFlags(ctx->kev[2 * step], ctx->stream, evf) != cudaSuccess)
+    return fail(ADF_E_DEVICE, std::string("event record: ") + cudaGetErrorString(cudaGetLastError()));
+  cudaError_t e = adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, false);
+  if (e != cudaSuccess)
+    return fail(ADF_E_DEVICE, std::string("step launch failed: ") + cudaGetErrorString(e) +
+                                  " (grid " + std::to_string(grid) + ", smem " +
+                                  std::to_string(smem) + ")");
+  if (timed && cudaEventRecordWithFlags(ctx->kev[2 * step + 1], ctx->stream, evf) != cudaSuccess)
+    return fail(ADF_E_DEVICE, std::string("event record: ") + cudaGetErrorString(cudaGetLastError()));
+  EpiParams ep;
+  ep.solves = d_solves;
+  ep.n_solves = (int)solves.size();
+  ep.step = step;
+  cudaError_t e2;
+  if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
+    return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
   return ADF_OK;
 }
 

@@ -129,3 +129,14 @@ def test_server_cancel_and_bad_request(adf, ctx):
     assert srv.poll(i2)[0] < 0
     assert srv.poll(i3)[0] < 0
     srv.stop()
+
+
+def test_kernel_timing_in_graphs(adf, ctx):
+    """Per-launch step-kernel timing works inside captured graphs."""
+    ctx.set_kernel_timing(True)
+    ctx.kernel_timing(reset=True)
+    reqs = [make_req(adf, 40, 70, "none", s) for s in range(2)]
+    adf.gf_solve_batch(reqs, batched=True)
+    ms, n = ctx.kernel_timing(reset=True)
+    ctx.set_kernel_timing(False)
+    assert n == 70 and ms > 0
