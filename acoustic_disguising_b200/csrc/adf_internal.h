@@ -33,6 +33,7 @@ struct SolveDev {
   int it_first;      // step whose input field sits in buffer 0
   int ntx, mw;
   int src_ntx;            // columns of src[] (transceivers that inject)
+  int npp, nvp;           // x-slab psi row pitch (npml, npml+1 rounded up to 4)
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;
@@ -60,10 +61,13 @@ struct SolveDev {
   int pad_;
 };
 
+constexpr int kTmaps = 9;
+
 // work item: {solve index, y tile, z0, z1}
 struct StepParams {
   SolveDev* solves;
-  const CUtensorMap* tmaps;  // 3 per solve: field depth-1, field depth-2, mask
+  const CUtensorMap* tmaps;  // kTmaps per solve: field, field(2 planes), mask, x-psi p/v,
+                             // y-psi p/v, z-psi p/v
   const int4* items;
   int n_items;
   int step;          // launch-step index within the chunk
@@ -79,12 +83,56 @@ struct EpiParams {
   int step;
 };
 
-// sizes of one ring slot for a solve (floats, each region 128-B aligned)
+// One ring slot (floats; every region 128-B aligned so TMA can land in it):
+//   P, Vx, Vy : rows j0-1 .. j0+ty of plane k            (3 x reg)
+//   Vz        : the same rows of planes k and k+1        (reg2)
+//   mask      : nibble words of those rows               (regm, 0 without a mask)
+//   xp, xv    : x-slab CPML memory of those rows, both   (regxp / regxv, 0 when
+//               sides, p side and v side                  that side is inactive)
+//   py,vy,pz,vz: y- and z-slab CPML memory of those rows (reg each when that side
+//               (one slab side each)                      is active, else 0)
+//   header    : 32 floats, the plane's entry-list offsets
 inline __host__ __device__ int round32(long long v) { return (int)((v + 31) / 32 * 32); }
-inline __host__ __device__ int slot_region(int ty, int nxp) { return round32((long long)(ty + 2) * nxp); }
-inline __host__ __device__ int slot_floats(int ty, int nxp, int mw) {
-  return 3 * slot_region(ty, nxp) + round32(2LL * (ty + 2) * nxp) + round32((long long)(ty + 2) * mw);
+struct SlotLayout {
+  int reg, reg2, regm, regxp, regxv, regyz_p, regyz_v, total;
+  int off_vz, off_m, off_xp, off_xv, off_py, off_vy, off_pz, off_vz2;
+};
+inline __host__ __device__ SlotLayout slot_layout(int ty, int nxp, int mw, int npp, int nvp) {
+  SlotLayout L;
+  const long long R = ty + 2;
+  L.reg = round32(R * nxp);
+  L.reg2 = round32(2 * R * nxp);
+  L.regm = round32(R * mw);
+  L.regxp = round32(2 * R * npp);
+  L.regxv = round32(2 * R * nvp);
+  L.regyz_p = npp ? L.reg : 0;
+  L.regyz_v = nvp ? L.reg : 0;
+  L.off_vz = 3 * L.reg;
+  L.off_m = L.off_vz + L.reg2;
+  L.off_xp = L.off_m + L.regm;
+  L.off_xv = L.off_xp + L.regxp;
+  L.off_py = L.off_xv + L.regxv;
+  L.off_vy = L.off_py + L.regyz_p;
+  L.off_pz = L.off_vy + L.regyz_v;
+  L.off_vz2 = L.off_pz + L.regyz_p;
+  L.total = L.off_vz2 + L.regyz_v + 32;
+  return L;
 }
+// y-slab side whose rows a tile's box holds (-1: tile outside both slabs):
+// the left slab if any row j0-1..j0+ty lies in [0, w), else the right slab
+// if any lies in [n-w, n).  w = npml (p side) or npml+1 (v side).
+inline __host__ __device__ int tile_yside(int j0, int ty, int n, int w) {
+  if (j0 - 1 < w) return 0;
+  if (j0 + ty >= n - w) return 1;
+  return -1;
+}
+// z-slab side of a plane (left slab has priority, as getBoundaryIndex)
+inline __host__ __device__ int plane_zside(int k, int n, int w) {
+  if (k < w) return 0;
+  if (k >= n - w) return 1;
+  return -1;
+}
+
 inline __host__ __device__ int pn_plane_floats(int ty, int nxp) { return round32((long long)(ty + 1) * nxp); }
 
 // error codes written by kernels

@@ -39,7 +39,8 @@ constexpr int NCW = NCT / 32;     // consumer warps
 constexpr int NTHREADS = NCT + 32;
 constexpr int kMaxStages = 8;
 constexpr int kPnBufs = 3;
-constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kMaxCoef = 8 * 63 + 4;  // CPML coefficients for npml <= 63
+constexpr uint32_t kWaitLimit = 1u << 24;
 
 int consumer_threads() { return NCT; }
 
@@ -70,13 +71,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after kWaitLimit polls (about a second) so that a
-// logic error surfaces as an error code instead of a hung GPU.
+// Bounded wait: gives up after kWaitLimit polls so that a logic error
+// surfaces as an error code instead of a hung GPU.  try_wait itself suspends
+// the thread for a bounded, hardware-chosen interval, so the loop does not
+// spin hot and wakes as soon as the phase completes.
 __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
     if (mbar_try_wait(a, parity)) return true;
-    if (i >= 8) __nanosleep(64);
-  }
   return false;
 }
 __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
@@ -85,6 +86,14 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map
       "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
       "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
+                                            int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
       : "memory");
 }
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
@@ -137,25 +146,29 @@ struct Arith<float> {
 
 // CPML memory update m = b*m + a*d; d += m  (updates.jl:46-61): b*m is a
 // Float32 product, a*d is promoted, the sum is rounded to Float32 on store
-// and re-added.  Only the owning tile stores (halo/prologue cells read).
+// and re-added.  `m` is updated in place; the caller stores it.
 template <typename R>
-__device__ __forceinline__ void cpml_step(R& dv, const float* rd, float* wr, long long off,
-                                          float a, float b, bool owned) {
+__device__ __forceinline__ void cpml_apply(R& dv, float& m, float a, float b) {
   using A = Arith<R>;
-  float m = rd[off];
-  float bm = __fmul_rn(b, m);
-  R nm = A::add(A::cv(bm), A::mul(A::cv(a), dv));
-  float mf = A::rn(nm);
-  if (owned) wr[off] = mf;
-  dv = A::add(dv, A::cv(mf));
+  const float bm = __fmul_rn(b, m);
+  m = A::rn(A::add(A::cv(bm), A::mul(A::cv(a), dv)));
+  dv = A::add(dv, A::cv(m));
 }
 
 struct PlaneCtx {
   const float* sP;
   const float* sVx;
   const float* sVy;
-  const float* sVz;  // plane k rows, plane k+1 at + R*nxp
+  const float* sVz;   // plane k rows, plane k+1 at + R*nxp
   const uint32_t* sM;
+  const float* sXp;   // x-slab psi, p side: [side][R][npp]
+  const float* sXv;   // x-slab psi, v side: [side][R][nvp]
+  const float* yP;    // y-slab psi rows of side ysP (p) / ysV (v): [R][nxp]
+  const float* yV;
+  const float* zP;    // z-slab psi of this plane (p / v side): [R][nxp]
+  const float* zV;
+  int ysP, ysV;
+  const float* co;    // CPML coefficients staged in shared memory
   float* pn_cur;
   const float* pn_prev;
   int j0, R, pl, rb, wb;
@@ -164,20 +177,59 @@ struct PlaneCtx {
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ float f4get(const float4& v, int e) {
   return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w;
 }
+__device__ __forceinline__ void f4set(float4& v, int e, float x) {
+  if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
+}
 
-// Pressure update of one quad (4 cells along x) of row r (global row j0-1+r)
+// Per-item scalars held in registers for the fast paths (the descriptor
+// lives in shared memory; re-reading it per quad costs a load per field).
 template <typename R>
-__device__ __forceinline__ void p_quad(const SolveDev& S, const PlaneCtx& c, int r, int q,
-                                       bool owned) {
+struct Regs {
+  int nxp, R2;  // row pitch, rows per ring region (ty+2)
+  R fq, fv, rdx, rdy, rdz;
+};
+
+// ---------------------------------------------------------------------------
+// Boundary path, pressure: rigid planes, the i = nx plane, CPML slabs.  Row-
+// and plane-wide conditions are uniform branches; per-cell conditions (the x
+// slab, the last x cells) are selects, so the four cells' dependency chains
+// interleave.  CPML memory comes from the ring slot (x and staged y/z slabs).
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ float p_cell_slow(float P, float dx_in, float dy_in, float dz_in,
+                                             const Regs<R>& g, bool upd, bool open, bool xs,
+                                             float& mx, float ax, float bx, bool ys, float& my,
+                                             float ay, float by, bool zs, float& mz, float az,
+                                             float bz) {
   using A = Arith<R>;
-  const int nxp = S.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml;
+  R dvx = A::mul(A::cv(dx_in), g.rdx);
+  R dvy = A::mul(A::cv(dy_in), g.rdy);
+  R dvz = A::mul(A::cv(dz_in), g.rdz);
+  {  // x slab: computed for every cell, kept where the cell is in the slab
+    R d2 = dvx;
+    float m2 = mx;
+    cpml_apply<R>(d2, m2, ax, bx);
+    if (xs) { dvx = d2; mx = m2; }
+  }
+  if (ys) cpml_apply<R>(dvy, my, ay, by);
+  if (zs) cpml_apply<R>(dvz, mz, az, bz);
+  const float n = A::rn(A::sub(A::cv(P), A::mul(g.fq, A::add(A::add(dvx, dvy), dvz))));
+  return (upd && open) ? n : P;
+}
+
+template <typename R>
+__device__ __forceinline__ void p_quad(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
+                                       int r, int q, bool owned) {
+  const int nxp = g.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, npp = S.npp;
   const int x0 = 4 * q;
   const int j = c.j0 - 1 + r;
   const int pl = c.pl;
-  const float4 P4 = ld4(c.sP + r * nxp + x0);
+  const float* base = c.sP + r * nxp + x0;
+  const float4 P4 = ld4(base);
   const float4 X4 = ld4(c.sVx + r * nxp + x0);
   const float X5 = (x0 + 4 < nxp) ? c.sVx[r * nxp + x0 + 4] : 0.f;
   const float4 Y0 = ld4(c.sVy + r * nxp + x0);
@@ -185,81 +237,111 @@ __device__ __forceinline__ void p_quad(const SolveDev& S, const PlaneCtx& c, int
   const float4 Z0 = ld4(c.sVz + r * nxp + x0);
   const float4 Z1 = ld4(c.sVz + (c.R + r) * nxp + x0);
   uint32_t nib = 0xFFFFu;
-  if (c.has_mask) nib = (c.sM[r * S.mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-  const R fq = A::fq(S), rdx = A::rdx(S), rdy = A::rdy(S), rdz = A::rdz(S);
   const bool rigid_y = (j == ny - 1), rigid_z = (pl == nz - 1);
-  const bool pc = (S.flags & SF_PCPML) != 0;
-  float out[4];
+  // rigid planes use update_p! (updates.jl:122-136): -2V/d at the wall, no
+  // CPML, no mask; the (ny, nz) corner is not updated at all
+  const bool plain_rigid = rigid_y || rigid_z;
+  if (c.has_mask && !plain_rigid) nib = (c.sM[r * S.mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
+  const bool pc = (S.flags & SF_PCPML) != 0 && !plain_rigid;
+  const float* co = c.co;
+  int ysd = -1, yl = 0, zsd = -1, zl = 0;
+  if (pc) {
+    if (j < npml) { ysd = 0; yl = j; }
+    else if (j >= ny - npml) { ysd = 1; yl = j - (ny - npml); }
+    if (pl < npml) { zsd = 0; zl = pl; }
+    else if (pl >= nz - npml) { zsd = 1; zl = pl - (nz - npml); }
+  }
+  long long oy = 0, oz = 0;
+  float4 my = make_float4(0.f, 0.f, 0.f, 0.f), mz = my;
+  float ay = 0.f, by = 0.f, az = 0.f, bz = 0.f;
+  if (ysd >= 0) {  // staged with the plane unless the tile straddles both y slabs
+    oy = (long long)ysd * S.psi_p_side[1] + ((long long)pl * npml + yl) * nxp + x0;
+    my = ysd == c.ysP ? ld4(c.yP + r * nxp + x0) : ldg4(S.psi_p[1] + c.rb * S.psi_p_buf[1] + oy);
+    ay = co[ysd * npml + yl];
+    by = co[4 * npml + 2 + ysd * npml + yl];
+  }
+  if (zsd >= 0) {
+    oz = (long long)zsd * S.psi_p_side[2] + ((long long)zl * ny + j) * nxp + x0;
+    mz = ld4(c.zP + r * nxp + x0);
+    az = co[zsd * npml + zl];
+    bz = co[4 * npml + 2 + zsd * npml + zl];
+  }
+  // x slab: side and depth of each cell, memory from the slot
+  float mx[4], ax[4], bx[4];
+  bool xs[4];
+  int xside[4], xl[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int x = x0 + e;
-    const float P = f4get(P4, e);
-    const float xa = f4get(X4, e), xb = (e < 3) ? f4get(X4, e + 1) : X5;
-    if (x > nx - 2 || (rigid_y && rigid_z)) {  // i = nx plane / (ny,nz) corner: not updated
-      out[e] = P;
-      continue;
-    }
-    R dvx = A::mul(A::cv(__fsub_rn(xb, xa)), rdx);
-    R dvy, dvz;
-    if (rigid_y) {  // update_p! on the plane j = ny (updates.jl:122-136)
-      dvy = A::mul(A::cv(__fmul_rn(-2.0f, f4get(Y0, e))), rdy);
-      dvz = A::mul(A::cv(__fsub_rn(f4get(Z1, e), f4get(Z0, e))), rdz);
-      out[e] = A::rn(A::sub(A::cv(P), A::mul(fq, A::add(A::add(dvx, dvy), dvz))));
-      continue;
-    }
-    if (rigid_z) {  // update_p! on the plane k = nz
-      dvy = A::mul(A::cv(__fsub_rn(f4get(Y1, e), f4get(Y0, e))), rdy);
-      dvz = A::mul(A::cv(__fmul_rn(-2.0f, f4get(Z0, e))), rdz);
-      out[e] = A::rn(A::sub(A::cv(P), A::mul(fq, A::add(A::add(dvx, dvy), dvz))));
-      continue;
-    }
-    dvy = A::mul(A::cv(__fsub_rn(f4get(Y1, e), f4get(Y0, e))), rdy);
-    dvz = A::mul(A::cv(__fsub_rn(f4get(Z1, e), f4get(Z0, e))), rdz);
+    int side = -1, l = 0;
     if (pc) {
-      const float* co = S.coef;
-      // x slab (getBoundaryIndex(i, nx, npml), derivatives.jl:66-79)
-      int side = -1, l = 0;
-      if (x < npml) { side = 0; l = x; }
-      else if (x >= nx - npml) { side = 1; l = x - (nx - npml); }
-      if (side >= 0) {
-        long long off = (long long)side * S.psi_p_side[0] + ((long long)pl * ny + j) * npml + l;
-        cpml_step<R>(dvx, S.psi_p[0] + c.rb * S.psi_p_buf[0], S.psi_p[0] + c.wb * S.psi_p_buf[0],
-                     off, __ldg(co + side * npml + l), __ldg(co + 4 * npml + 2 + side * npml + l),
-                     owned);
-      }
-      side = -1;
-      if (j < npml) { side = 0; l = j; }
-      else if (j >= ny - npml) { side = 1; l = j - (ny - npml); }
-      if (side >= 0) {
-        long long off = (long long)side * S.psi_p_side[1] + ((long long)pl * npml + l) * nxp + x;
-        cpml_step<R>(dvy, S.psi_p[1] + c.rb * S.psi_p_buf[1], S.psi_p[1] + c.wb * S.psi_p_buf[1],
-                     off, __ldg(co + side * npml + l), __ldg(co + 4 * npml + 2 + side * npml + l),
-                     owned);
-      }
-      side = -1;
-      if (pl < npml) { side = 0; l = pl; }
-      else if (pl >= nz - npml) { side = 1; l = pl - (nz - npml); }
-      if (side >= 0) {
-        long long off = (long long)side * S.psi_p_side[2] + ((long long)l * ny + j) * nxp + x;
-        cpml_step<R>(dvz, S.psi_p[2] + c.rb * S.psi_p_buf[2], S.psi_p[2] + c.wb * S.psi_p_buf[2],
-                     off, __ldg(co + side * npml + l), __ldg(co + 4 * npml + 2 + side * npml + l),
-                     owned);
-      }
+      side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
+      l = side == 0 ? x : x - (nx - npml);
     }
-    if ((nib >> (4 * e)) & 1u)
-      out[e] = A::rn(A::sub(A::cv(P), A::mul(fq, A::add(A::add(dvx, dvy), dvz))));
-    else
-      out[e] = P;  // coeff = fq * false: the cell is frozen (updates.jl:314-316)
+    xs[e] = side >= 0;
+    const int sd = xs[e] ? side : 0, ll = xs[e] ? l : 0;
+    xside[e] = sd;
+    xl[e] = ll;
+    mx[e] = c.sXp[(sd * c.R + r) * npp + ll];
+    ax[e] = xs[e] ? co[sd * npml + ll] : 0.f;
+    bx[e] = xs[e] ? co[4 * npml + 2 + sd * npml + ll] : 0.f;
   }
-  st4(c.pn_cur + r * nxp + x0, make_float4(out[0], out[1], out[2], out[3]));
+  const float dyv[4] = {rigid_y ? __fmul_rn(-2.0f, Y0.x) : __fsub_rn(Y1.x, Y0.x),
+                        rigid_y ? __fmul_rn(-2.0f, Y0.y) : __fsub_rn(Y1.y, Y0.y),
+                        rigid_y ? __fmul_rn(-2.0f, Y0.z) : __fsub_rn(Y1.z, Y0.z),
+                        rigid_y ? __fmul_rn(-2.0f, Y0.w) : __fsub_rn(Y1.w, Y0.w)};
+  const float dzv[4] = {rigid_z ? __fmul_rn(-2.0f, Z0.x) : __fsub_rn(Z1.x, Z0.x),
+                        rigid_z ? __fmul_rn(-2.0f, Z0.y) : __fsub_rn(Z1.y, Z0.y),
+                        rigid_z ? __fmul_rn(-2.0f, Z0.z) : __fsub_rn(Z1.z, Z0.z),
+                        rigid_z ? __fmul_rn(-2.0f, Z0.w) : __fsub_rn(Z1.w, Z0.w)};
+  const float dxv[4] = {__fsub_rn(X4.y, X4.x), __fsub_rn(X4.z, X4.y), __fsub_rn(X4.w, X4.z),
+                        __fsub_rn(X5, X4.w)};
+  const bool corner = rigid_y && rigid_z;
+  const float Pv[4] = {P4.x, P4.y, P4.z, P4.w};
+  float myv[4] = {my.x, my.y, my.z, my.w}, mzv[4] = {mz.x, mz.y, mz.z, mz.w};
+  float o[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const bool upd = (x0 + e <= nx - 2) && !corner;
+    float myc = myv[e], mzc = mzv[e], mxc = mx[e];
+    o[e] = p_cell_slow<R>(Pv[e], dxv[e], dyv[e], dzv[e], g, upd, (nib >> (4 * e)) & 1u,
+                          xs[e] && upd, mxc, ax[e], bx[e], ysd >= 0, myc, ay, by, zsd >= 0, mzc,
+                          az, bz);
+    if (upd) { myv[e] = myc; mzv[e] = mzc; mx[e] = mxc; }
+  }
+  st4(c.pn_cur + r * nxp + x0, make_float4(o[0], o[1], o[2], o[3]));
+  if (owned) {  // cells of the quad that were not updated keep their loaded value
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (xs[e] && (x0 + e <= nx - 2) && !corner)
+        S.psi_p[0][c.wb * S.psi_p_buf[0] + xside[e] * S.psi_p_side[0] +
+                   ((long long)pl * ny + j) * npp + xl[e]] = mx[e];
+    if (ysd >= 0)
+      st4(S.psi_p[1] + c.wb * S.psi_p_buf[1] + oy, make_float4(myv[0], myv[1], myv[2], myv[3]));
+    if (zsd >= 0)
+      st4(S.psi_p[2] + c.wb * S.psi_p_buf[2] + oz, make_float4(mzv[0], mzv[1], mzv[2], mzv[3]));
+  }
 }
 
-// Velocity update of one quad of tile row r (global row j0-1+r)
+// Boundary path, velocities: grid edges (Vx at i=1, Vy at j=1, Vz at k=1 are
+// not updated) and CPML slabs with the half-grid coefficients (npml+1).
 template <typename R>
-__device__ __forceinline__ void v_quad(const SolveDev& S, const PlaneCtx& c, int r, int q,
-                                       float4& vxo, float4& vyo, float4& vzo) {
+__device__ __forceinline__ float v_cell_slow(float V, float dp_in, R fv, R rd, bool upd,
+                                             bool open, bool sl, float& m, float a, float b) {
   using A = Arith<R>;
-  const int nxp = S.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml;
+  R dp = A::mul(A::cv(dp_in), rd);
+  R d2 = dp;
+  float m2 = m;
+  cpml_apply<R>(d2, m2, a, b);
+  if (sl) { dp = d2; m = m2; }
+  const float n = A::rn(A::sub(A::cv(V), A::mul(fv, dp)));
+  return (upd && open) ? n : V;
+}
+
+template <typename R>
+__device__ __forceinline__ void v_quad(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
+                                       int r, int q, float4& vxo, float4& vyo, float4& vzo) {
+  const int nxp = g.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, nvp = S.nvp;
   const int nm = npml + 1;
   const int x0 = 4 * q;
   const int j = c.j0 - 1 + r;
@@ -273,93 +355,179 @@ __device__ __forceinline__ void v_quad(const SolveDev& S, const PlaneCtx& c, int
   const float4 VZ = ld4(c.sVz + r * nxp + x0);
   uint32_t nib = 0xFFFFu;
   if (c.has_mask) nib = (c.sM[r * S.mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-  const R fv = A::fv(S), rdx = A::rdx(S), rdy = A::rdy(S), rdz = A::rdz(S);
   const bool vc = (S.flags & SF_VCPML) != 0;
-  const float* co = S.coef;
-  float ox[4], oy[4], oz[4];
+  const float* co = c.co;
+  int ysd = -1, yl = 0, zsd = -1, zl = 0;
+  if (vc && j >= 1) {
+    if (j <= npml) { ysd = 0; yl = j; }
+    else if (j >= ny - npml - 1) { ysd = 1; yl = j - (ny - npml - 1); }
+  }
+  if (vc && pl >= 1) {
+    if (pl <= npml) { zsd = 0; zl = pl; }
+    else if (pl >= nz - npml - 1) { zsd = 1; zl = pl - (nz - npml - 1); }
+  }
+  long long oy = 0, oz = 0;
+  float4 my = make_float4(0.f, 0.f, 0.f, 0.f), mz = my;
+  float ay = 0.f, by = 0.f, az = 0.f, bz = 0.f;
+  if (ysd >= 0) {
+    oy = (long long)ysd * S.psi_v_side[1] + ((long long)pl * nm + yl) * nxp + x0;
+    my = ysd == c.ysV ? ld4(c.yV + r * nxp + x0) : ldg4(S.psi_v[1] + c.rb * S.psi_v_buf[1] + oy);
+    ay = co[2 * npml + ysd * nm + yl];
+    by = co[6 * npml + 2 + ysd * nm + yl];
+  }
+  if (zsd >= 0) {
+    oz = (long long)zsd * S.psi_v_side[2] + ((long long)zl * ny + j) * nxp + x0;
+    mz = ld4(c.zV + r * nxp + x0);
+    az = co[2 * npml + zsd * nm + zl];
+    bz = co[6 * npml + 2 + zsd * nm + zl];
+  }
+  const float Pv[4] = {Pc.x, Pc.y, Pc.z, Pc.w};
+  const float Pl[4] = {Pxm, Pc.x, Pc.y, Pc.z};
+  const float Py[4] = {Pym.x, Pym.y, Pym.z, Pym.w};
+  const float Pz[4] = {Pzm.x, Pzm.y, Pzm.z, Pzm.w};
+  const float Vx[4] = {VX.x, VX.y, VX.z, VX.w};
+  const float Vy[4] = {VY.x, VY.y, VY.z, VY.w};
+  const float Vz[4] = {VZ.x, VZ.y, VZ.z, VZ.w};
+  float myv[4] = {my.x, my.y, my.z, my.w}, mzv[4] = {mz.x, mz.y, mz.z, mz.w};
+  float ox[4], oy4[4], oz4[4], mx[4];
+  bool xs[4];
+  int xside[4], xl[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int x = x0 + e;
-    const float pc = f4get(Pc, e);
-    const float vx = f4get(VX, e), vy = f4get(VY, e), vz = f4get(VZ, e);
-    // Vx over i = 2..nx (update_vx!, updates.jl:192-218)
-    if (x == 0 || x >= nx) {
-      ox[e] = vx;
-    } else {
-      const float pm = e > 0 ? f4get(Pc, e - 1) : Pxm;
-      R dp = A::mul(A::cv(__fsub_rn(pc, pm)), rdx);
-      if (vc) {
-        int side = -1, l = 0;
-        if (x <= npml) { side = 0; l = x; }
-        else if (x >= nx - npml - 1) { side = 1; l = x - (nx - npml - 1); }
-        if (side >= 0) {
-          long long off = (long long)side * S.psi_v_side[0] + ((long long)pl * ny + j) * nm + l;
-          cpml_step<R>(dp, S.psi_v[0] + c.rb * S.psi_v_buf[0], S.psi_v[0] + c.wb * S.psi_v_buf[0],
-                       off, __ldg(co + 2 * npml + side * nm + l),
-                       __ldg(co + 6 * npml + 2 + side * nm + l), true);
-        }
-      }
-      ox[e] = ((nib >> (4 * e + 1)) & 1u) ? A::rn(A::sub(A::cv(vx), A::mul(fv, dp))) : vx;
+    const bool in = x < nx;
+    // Vx over i = 2..nx (update_vx!, updates.jl:192-218), x slab with npml+1
+    int side = -1, l = 0;
+    if (vc) {
+      side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
+      l = side == 0 ? x : x - (nx - npml - 1);
     }
+    const bool updx = in && x >= 1;
+    xs[e] = side >= 0 && updx;
+    const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
+    xside[e] = sd;
+    xl[e] = ll;
+    mx[e] = c.sXv[(sd * c.R + r) * nvp + ll];
+    const float axe = side >= 0 ? co[2 * npml + sd * nm + ll] : 0.f;
+    const float bxe = side >= 0 ? co[6 * npml + 2 + sd * nm + ll] : 0.f;
+    ox[e] = v_cell_slow<R>(Vx[e], __fsub_rn(Pv[e], Pl[e]), g.fv, g.rdx, updx,
+                           (nib >> (4 * e + 1)) & 1u, xs[e], mx[e], axe, bxe);
     // Vy over j = 2..ny
-    if (j == 0 || x >= nx) {
-      oy[e] = vy;
-    } else {
-      R dp = A::mul(A::cv(__fsub_rn(pc, f4get(Pym, e))), rdy);
-      if (vc) {
-        int side = -1, l = 0;
-        if (j <= npml) { side = 0; l = j; }
-        else if (j >= ny - npml - 1) { side = 1; l = j - (ny - npml - 1); }
-        if (side >= 0) {
-          long long off = (long long)side * S.psi_v_side[1] + ((long long)pl * nm + l) * nxp + x;
-          cpml_step<R>(dp, S.psi_v[1] + c.rb * S.psi_v_buf[1], S.psi_v[1] + c.wb * S.psi_v_buf[1],
-                       off, __ldg(co + 2 * npml + side * nm + l),
-                       __ldg(co + 6 * npml + 2 + side * nm + l), true);
-        }
-      }
-      oy[e] = ((nib >> (4 * e + 2)) & 1u) ? A::rn(A::sub(A::cv(vy), A::mul(fv, dp))) : vy;
-    }
+    float myc = myv[e];
+    oy4[e] = v_cell_slow<R>(Vy[e], __fsub_rn(Pv[e], Py[e]), g.fv, g.rdy, in && j >= 1,
+                            (nib >> (4 * e + 2)) & 1u, ysd >= 0 && in, myc, ay, by);
+    if (in) myv[e] = myc;
     // Vz over k = 2..nz
-    if (pl == 0 || x >= nx) {
-      oz[e] = vz;
-    } else {
-      R dp = A::mul(A::cv(__fsub_rn(pc, f4get(Pzm, e))), rdz);
-      if (vc) {
-        int side = -1, l = 0;
-        if (pl <= npml) { side = 0; l = pl; }
-        else if (pl >= nz - npml - 1) { side = 1; l = pl - (nz - npml - 1); }
-        if (side >= 0) {
-          long long off = (long long)side * S.psi_v_side[2] + ((long long)l * ny + j) * nxp + x;
-          cpml_step<R>(dp, S.psi_v[2] + c.rb * S.psi_v_buf[2], S.psi_v[2] + c.wb * S.psi_v_buf[2],
-                       off, __ldg(co + 2 * npml + side * nm + l),
-                       __ldg(co + 6 * npml + 2 + side * nm + l), true);
-        }
-      }
-      oz[e] = ((nib >> (4 * e + 3)) & 1u) ? A::rn(A::sub(A::cv(vz), A::mul(fv, dp))) : vz;
-    }
+    float mzc = mzv[e];
+    oz4[e] = v_cell_slow<R>(Vz[e], __fsub_rn(Pv[e], Pz[e]), g.fv, g.rdz, in && pl >= 1,
+                            (nib >> (4 * e + 3)) & 1u, zsd >= 0 && in, mzc, az, bz);
+    if (in) mzv[e] = mzc;
   }
   vxo = make_float4(ox[0], ox[1], ox[2], ox[3]);
-  vyo = make_float4(oy[0], oy[1], oy[2], oy[3]);
-  vzo = make_float4(oz[0], oz[1], oz[2], oz[3]);
+  vyo = make_float4(oy4[0], oy4[1], oy4[2], oy4[3]);
+  vzo = make_float4(oz4[0], oz4[1], oz4[2], oz4[3]);
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    if (xs[e])
+      S.psi_v[0][c.wb * S.psi_v_buf[0] + xside[e] * S.psi_v_side[0] +
+                 ((long long)pl * ny + j) * nvp + xl[e]] = mx[e];
+  if (ysd >= 0)
+    st4(S.psi_v[1] + c.wb * S.psi_v_buf[1] + oy, make_float4(myv[0], myv[1], myv[2], myv[3]));
+  if (zsd >= 0)
+    st4(S.psi_v[2] + c.wb * S.psi_v_buf[2] + oz, make_float4(mzv[0], mzv[1], mzv[2], mzv[3]));
+}
+
+// ---- fast paths: every cell of the quad is an interior cell of its update
+// (no rigid plane, no CPML slab, no grid edge); branch-free 4-wide code.
+template <typename R>
+__device__ __forceinline__ float p_cell(float P, float dvx, float dvy, float dvz, R fq, R rdx,
+                                        R rdy, R rdz, uint32_t open) {
+  using A = Arith<R>;
+  const R s = A::add(A::add(A::mul(A::cv(dvx), rdx), A::mul(A::cv(dvy), rdy)),
+                     A::mul(A::cv(dvz), rdz));
+  const float n = A::rn(A::sub(A::cv(P), A::mul(fq, s)));
+  return open ? n : P;
+}
+
+template <typename R>
+__device__ __forceinline__ float v_cell(float V, float dp, R fv, R rd, uint32_t open) {
+  using A = Arith<R>;
+  const float n = A::rn(A::sub(A::cv(V), A::mul(fv, A::mul(A::cv(dp), rd))));
+  return open ? n : V;
+}
+
+template <typename R>
+__device__ __forceinline__ void p_quad_fast(const Regs<R>& g, const float* __restrict__ sp,
+                                            const float* __restrict__ sx,
+                                            const float* __restrict__ sy,
+                                            const float* __restrict__ sz,
+                                            float* __restrict__ out, uint32_t nib) {
+  const int nxp = g.nxp;
+  const float4 P4 = ld4(sp), X4 = ld4(sx), Y0 = ld4(sy), Y1 = ld4(sy + nxp), Z0 = ld4(sz),
+               Z1 = ld4(sz + g.R2 * nxp);
+  const float X5 = sx[4];
+  float4 o;
+  o.x = p_cell<R>(P4.x, __fsub_rn(X4.y, X4.x), __fsub_rn(Y1.x, Y0.x), __fsub_rn(Z1.x, Z0.x),
+                  g.fq, g.rdx, g.rdy, g.rdz, nib & 1u);
+  o.y = p_cell<R>(P4.y, __fsub_rn(X4.z, X4.y), __fsub_rn(Y1.y, Y0.y), __fsub_rn(Z1.y, Z0.y),
+                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x10u);
+  o.z = p_cell<R>(P4.z, __fsub_rn(X4.w, X4.z), __fsub_rn(Y1.z, Y0.z), __fsub_rn(Z1.z, Z0.z),
+                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x100u);
+  o.w = p_cell<R>(P4.w, __fsub_rn(X5, X4.w), __fsub_rn(Y1.w, Y0.w), __fsub_rn(Z1.w, Z0.w),
+                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x1000u);
+  st4(out, o);
+}
+
+template <typename R>
+__device__ __forceinline__ void v_quad_fast(const Regs<R>& g, const float* __restrict__ pc,
+                                            const float* __restrict__ pz,
+                                            const float* __restrict__ sx,
+                                            const float* __restrict__ sy,
+                                            const float* __restrict__ sz, uint32_t nib,
+                                            float4& vx, float4& vy, float4& vz) {
+  const float4 Pc = ld4(pc), Pym = ld4(pc - g.nxp), Pzm = ld4(pz);
+  const float Pxm = pc[-1];
+  const float4 VX = ld4(sx), VY = ld4(sy), VZ = ld4(sz);
+  vx.x = v_cell<R>(VX.x, __fsub_rn(Pc.x, Pxm), g.fv, g.rdx, nib & 0x2u);
+  vx.y = v_cell<R>(VX.y, __fsub_rn(Pc.y, Pc.x), g.fv, g.rdx, nib & 0x20u);
+  vx.z = v_cell<R>(VX.z, __fsub_rn(Pc.z, Pc.y), g.fv, g.rdx, nib & 0x200u);
+  vx.w = v_cell<R>(VX.w, __fsub_rn(Pc.w, Pc.z), g.fv, g.rdx, nib & 0x2000u);
+  vy.x = v_cell<R>(VY.x, __fsub_rn(Pc.x, Pym.x), g.fv, g.rdy, nib & 0x4u);
+  vy.y = v_cell<R>(VY.y, __fsub_rn(Pc.y, Pym.y), g.fv, g.rdy, nib & 0x40u);
+  vy.z = v_cell<R>(VY.z, __fsub_rn(Pc.z, Pym.z), g.fv, g.rdy, nib & 0x400u);
+  vy.w = v_cell<R>(VY.w, __fsub_rn(Pc.w, Pym.w), g.fv, g.rdy, nib & 0x4000u);
+  vz.x = v_cell<R>(VZ.x, __fsub_rn(Pc.x, Pzm.x), g.fv, g.rdz, nib & 0x8u);
+  vz.y = v_cell<R>(VZ.y, __fsub_rn(Pc.y, Pzm.y), g.fv, g.rdz, nib & 0x80u);
+  vz.z = v_cell<R>(VZ.z, __fsub_rn(Pc.z, Pzm.z), g.fv, g.rdz, nib & 0x800u);
+  vz.w = v_cell<R>(VZ.w, __fsub_rn(Pc.w, Pzm.w), g.fv, g.rdz, nib & 0x8000u);
 }
 
 // interp_trilinear! entries of one (tile, plane, channel) in transceiver
 // order per cell: rec += w*f (stored per entry, summed by the epilogue in
-// corner order), then f += w*src[it].
+// corner order), then f += w*src[it].  A segment with one entry carries it
+// inline {cell | 1<<16, w, slot, src column}; longer ones point at the
+// entry arrays {cell | n<<16, first entry, 0, 0}.
 __device__ __forceinline__ void process_entries(const SolveDev& S, int b, int e, int chan,
                                                 float* cells, bool records, int it) {
   const float* src = S.src[chan] + (long long)(it - 1) * S.src_ntx;
   for (int si = b + (int)threadIdx.x; si < e; si += NCT) {
-    const int4 sg = S.seg[si];
-    float v = cells[sg.x];
-    for (int k = sg.y; k < sg.y + sg.z; ++k) {
-      const float w = S.ent_w[k];
-      const int slot = S.ent_slot[k];
-      if (records && slot >= 0) S.contrib[slot] = __fmul_rn(w, v);
-      const int col = S.ent_tx[k];
-      if (col >= 0) v = __fadd_rn(v, __fmul_rn(w, src[col]));  // receivers: src == 0
+    const int4 sg = __ldg(S.seg + si);
+    const int cell = sg.x & 0xFFFF, cnt = (int)((unsigned)sg.x >> 16);
+    float v = cells[cell];
+    if (cnt == 1) {
+      const float w = __int_as_float(sg.y);
+      if (records && sg.z >= 0) S.contrib[sg.z] = __fmul_rn(w, v);
+      if (sg.w >= 0) v = __fadd_rn(v, __fmul_rn(w, __ldg(src + sg.w)));
+    } else {
+      for (int k = sg.y; k < sg.y + cnt; ++k) {
+        const float w = __ldg(S.ent_w + k);
+        const int slot = __ldg(S.ent_slot + k);
+        if (records && slot >= 0) S.contrib[slot] = __fmul_rn(w, v);
+        const int col = __ldg(S.ent_tx + k);
+        if (col >= 0) v = __fadd_rn(v, __fmul_rn(w, __ldg(src + col)));  // receivers: src == 0
+      }
     }
-    cells[sg.x] = v;
+    cells[cell] = v;
   }
 }
 
@@ -381,19 +549,91 @@ __device__ __forceinline__ void store_outputs(const SolveDev& S, const PlaneCtx&
         make_float4(-vz.x, -vz.y, -vz.z, -vz.w));
 }
 
+// Work index -> (row, quad) for an ordinary tile-plane: u < na_pad are the
+// boundary quads of each row (the first nl and the last nr quads), padded to
+// whole warps; the interior quads follow.  Division by the per-row counts
+// uses a 32.32 reciprocal (exact for u, divisor < 2^16).
+struct XSplit {
+  int nl, ni, nb, na, na_pad, total;
+  unsigned long long mb, mi;
+  __device__ __forceinline__ bool map(int u, int& row, int& q) const {
+    if (u < na_pad) {
+      if (u >= na) { row = -1; return true; }
+      row = (int)(((unsigned long long)u * mb) >> 32);
+      const int k = u - row * nb;
+      q = k < nl ? k : k + ni;
+      return true;
+    }
+    const int v = u - na_pad;
+    row = (int)(((unsigned long long)v * mi) >> 32);
+    q = nl + v - row * ni;
+    return false;
+  }
+};
+__device__ __forceinline__ XSplit make_split(int xmin, int xmax, int nq, int nrows) {
+  XSplit s;
+  s.nl = (xmin + 3) / 4;                     // quads with x0 < xmin
+  const int qhi = xmax >= 3 ? (xmax - 3) / 4 : -1;  // last quad with x0+3 <= xmax
+  s.ni = max(0, min(qhi, nq - 1) - s.nl + 1);
+  s.nb = nq - s.ni;
+  s.na = nrows * s.nb;
+  s.na_pad = (s.na + 31) / 32 * 32;
+  s.total = s.na_pad + nrows * s.ni;
+  s.mb = s.nb ? ((1ull << 32) + s.nb - 1) / s.nb : 0;
+  s.mi = s.ni ? ((1ull << 32) + s.ni - 1) / s.ni : 0;
+  return s;
+}
+
 template <typename R>
 __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, int it,
                              uint64_t* full, uint64_t* empty, float* ring, float* pn, int& n,
-                             volatile int* s_fail) {
+                             volatile int* s_fail, const float* s_co) {
+  using A = Arith<R>;
   const int rb = (it - S.it_first) & 1;
   const int ty = S.ty, nxp = S.nxp, nq = nxp / 4;
   const int j0 = item.y * ty;
   const int Rr = ty + 2;
-  const int reg = slot_region(ty, nxp);
-  const int reg2 = round32(2LL * Rr * nxp);
+  const bool has_mask = (S.flags & SF_MASK) != 0;
+  const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
+  const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
+                                   vcpml ? S.nvp : 0);
   const int pz0 = item.z > 0 ? item.z - 1 : 0;
   const int tid = threadIdx.x;
-  const bool has_mask = (S.flags & SF_MASK) != 0;
+  Regs<R> g;
+  g.nxp = nxp;
+  g.R2 = Rr;
+  g.fq = A::fq(S);
+  g.fv = A::fv(S);
+  g.rdx = A::rdx(S);
+  g.rdy = A::rdy(S);
+  g.rdz = A::rdz(S);
+  const int nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, mw = S.mw;
+  // thread -> (row, quad) walk: stride NCT over rows of nq quads
+  const int dr = NCT / nq, dq = NCT - (NCT / nq) * nq;
+  const int r_first = tid / nq, q_first = tid - r_first * nq;
+  // x ranges where every cell of a quad takes the plain update
+  const int p_xmin = pcpml ? npml : 0;
+  const int p_xmax = pcpml ? min(nx - 2, nx - npml - 1) : nx - 2;
+  const int v_xmin = vcpml ? npml + 1 : 1;
+  const int v_xmax = vcpml ? nx - npml - 2 : nx - 1;
+  // Ordinary tile-planes: boundary quads (x slab / x edges) are packed into
+  // whole warps ahead of the interior quads, so interior warps never diverge
+  // into the boundary path.  Row range and x classes per phase:
+  const int rP0 = j0 == 0 ? 1 : 0, rP1 = min(ty, ny - j0);
+  const int rV1 = min(ty, ny - j0);
+  bool tileP = rP1 >= rP0, tileV = rV1 >= 1;
+  for (int r = rP0; r <= rP1; ++r) {
+    const int j = j0 - 1 + r;
+    tileP = tileP && (j != ny - 1) && (!pcpml || (j >= npml && j < ny - npml));
+  }
+  for (int r = 1; r <= rV1; ++r) {
+    const int j = j0 - 1 + r;
+    tileV = tileV && j >= 1 && (!vcpml || (j > npml && j < ny - npml - 1));
+  }
+  const XSplit sP = make_split(p_xmin, p_xmax, nq, rP1 - rP0 + 1);
+  const XSplit sV = make_split(v_xmin, v_xmax, nq, rV1);
+  tileP = tileP && sP.ni > 0;
+  tileV = tileV && sV.ni > 0;
   for (int pl = pz0; pl < item.w; ++pl, ++n) {
     const int slot = n % p.stages;
     const int round = n / p.stages;
@@ -406,10 +646,19 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
     float* base = ring + (long long)slot * p.stage_floats;
     PlaneCtx c;
     c.sP = base;
-    c.sVx = base + reg;
-    c.sVy = base + 2 * reg;
-    c.sVz = base + 3 * reg;
-    c.sM = reinterpret_cast<const uint32_t*>(base + 3 * reg + reg2);
+    c.sVx = base + L.reg;
+    c.sVy = base + 2 * L.reg;
+    c.sVz = base + L.off_vz;
+    c.sM = reinterpret_cast<const uint32_t*>(base + L.off_m);
+    c.sXp = base + L.off_xp;
+    c.sXv = base + L.off_xv;
+    c.yP = base + L.off_py;
+    c.yV = base + L.off_vy;
+    c.zP = base + L.off_pz;
+    c.zV = base + L.off_vz2;
+    c.co = s_co;
+    c.ysP = pcpml ? tile_yside(j0, ty, ny, npml) : -1;
+    c.ysV = vcpml ? tile_yside(j0, ty, ny, npml + 1) : -1;
     c.pn_cur = pn + (n % kPnBufs) * p.pn_floats;
     c.pn_prev = pn + ((n + kPnBufs - 1) % kPnBufs) * p.pn_floats;
     c.j0 = j0;
@@ -418,14 +667,34 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
     c.rb = rb;
     c.wb = rb ^ 1;
     c.has_mask = has_mask;
-    // ---- P phase ----
-    const int nP = (ty + 1) * nq;
+    // ---- P phase: rows j0-1 .. j0+ty-1 ----
     if (landed) {
-      for (int u = tid; u < nP; u += NCT) {
-        const int r = u / nq, q = u - r * nq;
-        const int j = j0 - 1 + r;
-        if (j < 0 || j >= S.ny) continue;
-        p_quad<R>(S, c, r, q, !prologue && r >= 1);
+      const bool pl_plain = !(pl == nz - 1) && (!pcpml || (pl >= npml && pl < nz - npml));
+      auto p_work = [&](int r, int q, bool fast) {
+        if (fast) {
+          uint32_t nib = 0xFFFFu;
+          if (has_mask) nib = (c.sM[r * mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
+          const int o = r * nxp + 4 * q;
+          p_quad_fast<R>(g, c.sP + o, c.sVx + o, c.sVy + o, c.sVz + o, c.pn_cur + o, nib);
+        } else {
+          p_quad<R>(S, g, c, r, q, !prologue && r >= 1);
+        }
+      };
+      if (pl_plain && tileP) {
+        for (int u = tid; u < sP.total; u += NCT) {
+          int row, q;
+          const bool bnd = sP.map(u, row, q);
+          if (row >= 0) p_work(rP0 + row, q, !bnd);
+        }
+      } else {
+        for (int r = r_first, q = q_first; r <= ty; q += dq, r += dr) {
+          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
+          const int j = j0 - 1 + r;
+          if (j < 0 || j >= ny) continue;
+          const int x0 = 4 * q;
+          const bool row_plain = (j != ny - 1) && (!pcpml || (j >= npml && j < ny - npml));
+          p_work(r, q, pl_plain && row_plain && x0 + 3 <= p_xmax && x0 >= p_xmin);
+        }
       }
     }
     consumer_bar();
@@ -434,47 +703,64 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
       return false;
     }
     // ---- Q phase: q-channel inject/record on P (forward.jl:92) ----
-    const int tb = (item.y * S.nz + pl) * 4;
-    {
-      const int b = S.tp_off[tb], e = S.tp_off[tb + 1];
-      if (b < e) {
-        process_entries(S, b, e, 0, c.pn_cur, !prologue, it);
-        consumer_bar();
-      }
+    const int* hdr = reinterpret_cast<const int*>(base + p.stage_floats - 32);
+    const int off0 = hdr[0], off1 = hdr[1], off2 = hdr[2], off3 = hdr[3], off4 = hdr[4];
+    if (off0 < off1) {
+      process_entries(S, off0, off1, 0, c.pn_cur, !prologue, it);
+      consumer_bar();
     }
     if (!prologue) {
-      const int fb = S.tp_off[tb + 1], fe = S.tp_off[tb + 4];
-      const bool has_f = fb < fe;
-      const int nV = ty * nq;
-      for (int u = tid; u < nV; u += NCT) {
-        const int r = 1 + u / nq, q = u - (r - 1) * nq;
-        const int j = j0 - 1 + r;
-        if (j >= S.ny) continue;
+      const bool has_f = off1 < off4;
+      const bool pl_vplain = pl >= 1 && (!vcpml || (pl > npml && pl < nz - npml - 1));
+      auto v_work = [&](int r, int q, bool fast) {
         float4 vx, vy, vz;
-        v_quad<R>(S, c, r, q, vx, vy, vz);
-        if (has_f) {  // stage into this slot's own rows (only this thread reads them)
-          st4(const_cast<float*>(c.sVx) + r * nxp + 4 * q, vx);
-          st4(const_cast<float*>(c.sVy) + r * nxp + 4 * q, vy);
-          st4(const_cast<float*>(c.sVz) + r * nxp + 4 * q, vz);
+        const int o = r * nxp + 4 * q;
+        if (fast) {
+          uint32_t nib = 0xFFFFu;
+          if (has_mask) nib = (c.sM[r * mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
+          v_quad_fast<R>(g, c.pn_cur + o, c.pn_prev + o, c.sVx + o, c.sVy + o, c.sVz + o, nib,
+                         vx, vy, vz);
         } else {
-          store_outputs(S, c, r, q, ld4(c.pn_cur + r * nxp + 4 * q), vx, vy, vz);
+          v_quad<R>(S, g, c, r, q, vx, vy, vz);
+        }
+        if (has_f) {  // stage into this slot's own rows (only this thread reads them)
+          st4(const_cast<float*>(c.sVx) + o, vx);
+          st4(const_cast<float*>(c.sVy) + o, vy);
+          st4(const_cast<float*>(c.sVz) + o, vz);
+        } else {
+          store_outputs(S, c, r, q, ld4(c.pn_cur + o), vx, vy, vz);
+        }
+      };
+      if (pl_vplain && tileV) {
+        for (int u = tid; u < sV.total; u += NCT) {
+          int row, q;
+          const bool bnd = sV.map(u, row, q);
+          if (row >= 0) v_work(1 + row, q, !bnd);
+        }
+      } else {
+        for (int r = 1 + r_first, q = q_first; r <= ty; q += dq, r += dr) {
+          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
+          const int j = j0 - 1 + r;
+          if (j >= ny) continue;
+          const int x0 = 4 * q;
+          const bool row_vplain = j >= 1 && (!vcpml || (j > npml && j < ny - npml - 1));
+          v_work(r, q, pl_vplain && row_vplain && x0 >= v_xmin && x0 + 3 <= v_xmax);
         }
       }
       if (has_f) {
         consumer_bar();
         // ---- F phase: f-channel inject/record (forward.jl:111-115) ----
-        for (int ch = 1; ch <= 3; ++ch) {
-          const int b = S.tp_off[tb + ch], e = S.tp_off[tb + ch + 1];
-          float* cells = const_cast<float*>(ch == 1 ? c.sVx : ch == 2 ? c.sVy : c.sVz);
-          if (b < e) process_entries(S, b, e, ch, cells, true, it);
-        }
+        if (off1 < off2) process_entries(S, off1, off2, 1, const_cast<float*>(c.sVx), true, it);
+        if (off2 < off3) process_entries(S, off2, off3, 2, const_cast<float*>(c.sVy), true, it);
+        if (off3 < off4) process_entries(S, off3, off4, 3, const_cast<float*>(c.sVz), true, it);
         consumer_bar();
-        for (int u = tid; u < nV; u += NCT) {
-          const int r = 1 + u / nq, q = u - (r - 1) * nq;
+        for (int r = 1 + r_first, q = q_first; r <= ty; q += dq, r += dr) {
+          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
           const int j = j0 - 1 + r;
-          if (j >= S.ny) continue;
-          store_outputs(S, c, r, q, ld4(c.pn_cur + r * nxp + 4 * q), ld4(c.sVx + r * nxp + 4 * q),
-                        ld4(c.sVy + r * nxp + 4 * q), ld4(c.sVz + r * nxp + 4 * q));
+          if (j >= ny) continue;
+          const int o = r * nxp + 4 * q;
+          store_outputs(S, c, r, q, ld4(c.pn_cur + o), ld4(c.sVx + o), ld4(c.sVy + o),
+                        ld4(c.sVz + o));
         }
         // generic-proxy writes to the slot must be ordered before the next
         // TMA write into it
@@ -520,19 +806,24 @@ __global__ void __launch_bounds__(NTHREADS, 2) adf_fdtd_step_kernel(const StepPa
       const int it = S.it_base + p.step;
       if (it > S.it_stop) continue;
       const int rb = (it - S.it_first) & 1;
-      const CUtensorMap* tm = p.tmaps + 3 * item.x;
+      const CUtensorMap* tm = p.tmaps + kTmaps * item.x;
       if (item.x != cur) {
-        tmap_acquire(tm);
-        tmap_acquire(tm + 1);
-        tmap_acquire(tm + 2);
+        for (int k = 0; k < kTmaps; ++k) tmap_acquire(tm + k);
         cur = item.x;
       }
       const int ty = S.ty, nxp = S.nxp, Rr = ty + 2;
       const int j0 = item.y * ty;
-      const int reg = slot_region(ty, nxp);
-      const int reg2 = round32(2LL * Rr * nxp);
       const bool has_mask = (S.flags & SF_MASK) != 0;
-      const uint32_t bytes = (uint32_t)(5 * Rr * nxp * 4 + (has_mask ? Rr * S.mw * 4 : 0));
+      const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
+      const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
+                                       vcpml ? S.nvp : 0);
+      const uint32_t bytes0 =
+          (uint32_t)(5 * Rr * nxp * 4 + (has_mask ? Rr * S.mw * 4 : 0) +
+                     (pcpml ? 2 * Rr * S.npp * 4 : 0) + (vcpml ? 2 * Rr * S.nvp * 4 : 0));
+      const uint32_t box_bytes = (uint32_t)(Rr * nxp * 4);
+      const int ny = S.ny, nz = S.nz, npml = S.npml;
+      const int ysP = pcpml ? tile_yside(j0, ty, ny, npml) : -1;
+      const int ysV = vcpml ? tile_yside(j0, ty, ny, npml + 1) : -1;
       const int pz0 = item.z > 0 ? item.z - 1 : 0;
       bool ok = true;
       for (int pl = pz0; pl < item.w; ++pl, ++n) {
@@ -543,13 +834,55 @@ __global__ void __launch_bounds__(NTHREADS, 2) adf_fdtd_step_kernel(const StepPa
           break;
         }
         const uint32_t mb = smem_u32(&full[slot]);
-        mbar_expect_tx(mb, bytes);
         float* base = ring + (long long)slot * p.stage_floats;
+        // bulk copies first (the transaction count may dip below zero until
+        // the arrive below adds the expected bytes; the phase cannot complete
+        // before that arrive)
         tma_load_5d(smem_u32(base), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 0);
-        tma_load_5d(smem_u32(base + reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 1);
-        tma_load_5d(smem_u32(base + 2 * reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 2);
-        tma_load_5d(smem_u32(base + 3 * reg), tm + 1, mb, 0, 0, j0 - 1, pl, 4 * rb + 3);
-        if (has_mask) tma_load_3d(smem_u32(base + 3 * reg + reg2), tm + 2, mb, 0, j0 - 1, pl);
+        tma_load_5d(smem_u32(base + L.reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 1);
+        tma_load_5d(smem_u32(base + 2 * L.reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 2);
+        tma_load_5d(smem_u32(base + L.off_vz), tm + 1, mb, 0, 0, j0 - 1, pl, 4 * rb + 3);
+        if (has_mask) tma_load_3d(smem_u32(base + L.off_m), tm + 2, mb, 0, j0 - 1, pl);
+        // x-slab CPML memory of both sides: box (np, R, 1, 2) at (0, j0-1, pl, 2*rb)
+        if (pcpml) tma_load_4d(smem_u32(base + L.off_xp), tm + 3, mb, 0, j0 - 1, pl, 2 * rb);
+        if (vcpml) tma_load_4d(smem_u32(base + L.off_xv), tm + 4, mb, 0, j0 - 1, pl, 2 * rb);
+        // y-slab rows of the tile (rows outside the slab arrive as zeros) and
+        // the z-slab plane, p and v sides
+        uint32_t bytes = bytes0;
+        if (ysP >= 0) {
+          const int l0 = ysP == 0 ? j0 - 1 : j0 - 1 - (ny - npml);
+          tma_load_5d(smem_u32(base + L.off_py), tm + 5, mb, 0, 0, l0, pl, 2 * rb + ysP);
+          bytes += box_bytes;
+        }
+        if (ysV >= 0) {
+          const int l0 = ysV == 0 ? j0 - 1 : j0 - 1 - (ny - npml - 1);
+          tma_load_5d(smem_u32(base + L.off_vy), tm + 6, mb, 0, 0, l0, pl, 2 * rb + ysV);
+          bytes += box_bytes;
+        }
+        if (pcpml) {
+          const int zs = plane_zside(pl, nz, npml);
+          if (zs >= 0) {
+            const int l = zs == 0 ? pl : pl - (nz - npml);
+            tma_load_5d(smem_u32(base + L.off_pz), tm + 7, mb, 0, 0, j0 - 1, l, 2 * rb + zs);
+            bytes += box_bytes;
+          }
+        }
+        if (vcpml) {
+          const int zs = plane_zside(pl, nz, npml + 1);
+          if (zs >= 0) {
+            const int l = zs == 0 ? pl : pl - (nz - npml - 1);
+            tma_load_5d(smem_u32(base + L.off_vz2), tm + 8, mb, 0, 0, j0 - 1, l, 2 * rb + zs);
+            bytes += box_bytes;
+          }
+        }
+        {  // entry-list offsets of this (tile, plane), staged for the consumers
+          int* hdr = reinterpret_cast<int*>(base + p.stage_floats - 32);
+          const int tb = (item.y * S.nz + pl) * 4;
+          const int4 o4 = *reinterpret_cast<const int4*>(S.tp_off + tb);
+          hdr[0] = o4.x; hdr[1] = o4.y; hdr[2] = o4.z; hdr[3] = o4.w;
+          hdr[4] = S.tp_off[tb + 4];
+        }
+        mbar_expect_tx(mb, bytes);  // release: the header is visible after the wait
         last_round[slot] = round;
       }
       if (!ok) break;
@@ -562,17 +895,31 @@ __global__ void __launch_bounds__(NTHREADS, 2) adf_fdtd_step_kernel(const StepPa
   }
 
   // ---------------- consumer warps ----------------
-  int n = 0;
+  // the solve descriptor is read from shared memory inside the hot loops
+  __shared__ __align__(16) SolveDev s_desc[2];
+  __shared__ float s_coef[2][kMaxCoef];
+  int n = 0, k_item = 0;
   for (int i = blockIdx.x; i < p.n_items; i += gridDim.x) {
     const int4 item = p.items[i];
-    const SolveDev& S = p.solves[item.x];
-    const int it = S.it_base + p.step;
-    if (it > S.it_stop) continue;
+    const SolveDev& G = p.solves[item.x];
+    const int it = G.it_base + p.step;
+    if (it > G.it_stop) continue;
+    SolveDev& S = s_desc[k_item & 1];
+    float* co = s_coef[k_item & 1];
+    ++k_item;
+    {
+      const int* src = reinterpret_cast<const int*>(&G);
+      int* dst = reinterpret_cast<int*>(&S);
+      for (int w = tid; w < (int)(sizeof(SolveDev) / 4); w += NCT) dst[w] = src[w];
+      const int ncoef = 8 * G.npml + 4;
+      for (int w = tid; w < ncoef; w += NCT) co[w] = G.coef[w];
+      consumer_bar();
+    }
     bool ok;
     if (S.flags & SF_FP32)
-      ok = consume_item<float>(p, S, item, it, full, empty, ring, pn, n, &s_fail);
+      ok = consume_item<float>(p, S, item, it, full, empty, ring, pn, n, &s_fail, co);
     else
-      ok = consume_item<double>(p, S, item, it, full, empty, ring, pn, n, &s_fail);
+      ok = consume_item<double>(p, S, item, it, full, empty, ring, pn, n, &s_fail, co);
     if (!ok) return;
     // items run in lock-step with the producer; if it stopped on an error
     // flag the next full-barrier wait times out and returns here

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -118,7 +119,46 @@ static int encode_tmaps(adf_ctx* ctx, Solve& s, int xh) {
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(vz) failed: " + std::to_string((int)r));
-  std::memset(&s.tm[2], 0, sizeof(CUtensorMap));
+  for (int k = 2; k < kTmaps; ++k) std::memset(&s.tm[k], 0, sizeof(CUtensorMap));
+  if (d.npml > 0) {  // x-slab CPML memory, [buf][side][nz][ny][np]: box (np, ty+2, 1, 2)
+    for (int v = 0; v < 2; ++v) {
+      const int np = v ? d.nvp : d.npp;
+      cuuint64_t xd[4] = {(cuuint64_t)np, (cuuint64_t)d.ny, (cuuint64_t)d.nz, 4};
+      cuuint64_t xs[3] = {(cuuint64_t)np * 4, (cuuint64_t)np * d.ny * 4,
+                          (cuuint64_t)np * d.ny * d.nz * 4};
+      cuuint32_t xb[4] = {(cuuint32_t)np, (cuuint32_t)(d.ty + 2), 1, 2};
+      r = ctx->encode(&s.tm[3 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                      v ? (void*)d.psi_v[0] : (void*)d.psi_p[0], xd, xs, xb, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(x psi) failed: " + std::to_string((int)r));
+    }
+    // y slab [buf][side][nz][n][nxp] and z slab [buf][side][n][ny][nxp], n = npml (p) or
+    // npml+1 (v): 5-D like the field, box (bx, xh, ty+2, 1, 1)
+    for (int v = 0; v < 2; ++v) {
+      const int n = v ? d.npml + 1 : d.npml;
+      float* base_y = v ? d.psi_v[1] : d.psi_p[1];
+      float* base_z = v ? d.psi_v[2] : d.psi_p[2];
+      cuuint64_t yd[5] = {dims[0], dims[1], (cuuint64_t)n, (cuuint64_t)d.nz, 4};
+      cuuint64_t ys[4] = {strides[0], (cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * n * 4,
+                          (cuuint64_t)d.nxp * n * d.nz * 4};
+      cuuint64_t zd[5] = {dims[0], dims[1], (cuuint64_t)d.ny, (cuuint64_t)n, 4};
+      cuuint64_t zs[4] = {strides[0], (cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * d.ny * 4,
+                          (cuuint64_t)d.nxp * d.ny * n * 4};
+      cuuint32_t b5[5] = {(cuuint32_t)bx, (cuuint32_t)xh, (cuuint32_t)(d.ty + 2), 1, 1};
+      r = ctx->encode(&s.tm[5 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base_y, yd, ys, b5, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(y psi) failed: " + std::to_string((int)r));
+      r = ctx->encode(&s.tm[7 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base_z, zd, zs, b5, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(z psi) failed: " + std::to_string((int)r));
+    }
+  }
   if (d.flags & SF_MASK) {
     cuuint64_t md[3] = {(cuuint64_t)d.mw, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
     cuuint64_t ms[2] = {(cuuint64_t)d.mw * 4, (cuuint64_t)d.mw * d.ny * 4};
@@ -190,15 +230,25 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
     while (cur_b <= b) off[(size_t)cur_b++] = (int)seg.size();
     size_t j = i;
     while (j < es.size() && es[j].key == es[i].key) ++j;
+    // {cell | count<<16, ...}: one entry inline {w, slot, src column},
+    // more than one {first entry, 0, 0} into the entry arrays
+    const int cell = (int)(es[i].key & 0xffffffffLL);
+    const int cnt = (int)(j - i);
     int4 sg;
-    sg.x = (int)(es[i].key & 0xffffffffLL);
-    sg.y = (int)ew.size();
-    sg.z = (int)(j - i);
-    sg.w = 0;
-    for (size_t k = i; k < j; ++k) {
-      ew.push_back(es[k].w);
-      etx.push_back(es[k].col);
-      eslot.push_back(es[k].slot);
+    sg.x = cell | (cnt << 16);
+    if (cnt == 1) {
+      std::memcpy(&sg.y, &es[i].w, 4);
+      sg.z = es[i].slot;
+      sg.w = es[i].col;
+    } else {
+      sg.y = (int)ew.size();
+      sg.z = 0;
+      sg.w = 0;
+      for (size_t k = i; k < j; ++k) {
+        ew.push_back(es[k].w);
+        etx.push_back(es[k].col);
+        eslot.push_back(es[k].slot);
+      }
     }
     seg.push_back(sg);
     i = j;
@@ -215,8 +265,9 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
   if (rc) return rc;
   cudaStream_t st = s.stream;
   cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st);
-  if (!seg.empty()) {
+  if (!seg.empty())
     cudaMemcpyAsync(d_seg, seg.data(), seg.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+  if (!ew.empty()) {
     cudaMemcpyAsync(d_w, ew.data(), ew.size() * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_tx, etx.data(), etx.size() * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_slot, eslot.data(), eslot.size() * 4, cudaMemcpyHostToDevice, st);
@@ -233,7 +284,7 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
   d.ent_slot = d_slot;
   d.inb = d_inb;
   d.contrib = d_contrib;
-  s.n_entries = (long long)ew.size();
+  s.n_entries = (long long)es.size();
   return ADF_OK;
 }
 
@@ -283,8 +334,10 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
     if (rc) return rc;
   }
   const long long n = npml, nm = npml + 1, nxp = d.nxp, ny = d.ny, nz = d.nz;
-  const long long ps[3] = {nz * ny * n, nz * n * nxp, n * ny * nxp};
-  const long long vs[3] = {nz * ny * nm, nz * nm * nxp, nm * ny * nxp};
+  d.npp = (npml + 3) / 4 * 4;
+  d.nvp = (npml + 1 + 3) / 4 * 4;
+  const long long ps[3] = {nz * ny * d.npp, nz * n * nxp, n * ny * nxp};
+  const long long vs[3] = {nz * ny * d.nvp, nz * nm * nxp, nm * ny * nxp};
   for (int a = 0; a < 3; ++a) {
     d.psi_p_side[a] = ps[a];
     d.psi_p_buf[a] = 2 * ps[a];
@@ -375,15 +428,18 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   solves = list;
   const int ns = (int)list.size();
   std::vector<SolveDev> sd(ns);
-  std::vector<CUtensorMap> tm((size_t)3 * ns);
+  std::vector<CUtensorMap> tm((size_t)kTmaps * ns);
   std::vector<int4> items;
   int max_stage = 0, max_pn = 0;
   max_ntx = 0;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
-    for (int k = 0; k < 3; ++k) tm[(size_t)3 * i + k] = list[i]->tm[k];
+    for (int k = 0; k < kTmaps; ++k) tm[(size_t)kTmaps * i + k] = list[i]->tm[k];
     const SolveDev& d = list[i]->dev;
-    max_stage = std::max(max_stage, slot_floats(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0));
+    const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
+                                     (d.flags & SF_PCPML) ? d.npp : 0,
+                                     (d.flags & SF_VCPML) ? d.nvp : 0);
+    max_stage = std::max(max_stage, L.total);
     max_pn = std::max(max_pn, pn_plane_floats(d.ty, d.nxp));
     max_ntx = std::max(max_ntx, d.ntx);
   }
@@ -410,7 +466,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
     cap_solves = std::max(ns, 1);
     cap_items = std::max(n_items, 1);
     if (cudaMalloc(&d_solves, sizeof(SolveDev) * cap_solves) != cudaSuccess ||
-        cudaMalloc(&d_tmaps, sizeof(CUtensorMap) * 3 * cap_solves) != cudaSuccess ||
+        cudaMalloc(&d_tmaps, sizeof(CUtensorMap) * kTmaps * cap_solves) != cudaSuccess ||
         cudaMalloc(&d_items, sizeof(int4) * cap_items) != cudaSuccess ||
         cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
@@ -420,7 +476,8 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   host_solves = sd;
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_tmaps, tm.data(), sizeof(CUtensorMap) * 3 * ns, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_tmaps, tm.data(), sizeof(CUtensorMap) * kTmaps * ns, cudaMemcpyHostToDevice,
+                  st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   cudaStreamSynchronize(st);
@@ -430,11 +487,15 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   const size_t fixed = 256 + (size_t)3 * pn_floats * 4;
   const size_t per_cta2 = (size_t)ctx->smem_per_sm / 2 - 1024;
   int stages = (int)((per_cta2 > fixed ? per_cta2 - fixed : 0) / ((size_t)stage_floats * 4));
-  if (stages < 3) {
+  if (stages < 2) {
     const size_t per_cta1 = std::min((size_t)ctx->smem_optin, (size_t)ctx->smem_per_sm - 1024);
     stages = (int)((per_cta1 - fixed) / ((size_t)stage_floats * 4));
   }
-  stages = std::min(std::max(stages, 2), 6);
+  stages = std::min(std::max(stages, 2), 8);
+  if (const char* env = std::getenv("ADF_STAGES")) {  // sweep override
+    const int v = std::atoi(env);
+    if (v >= 2 && v <= 8) stages = v;
+  }
   this->stages = stages;
   smem = fixed + (size_t)stages * stage_floats * 4;
   if (smem > (size_t)ctx->smem_optin) return fail(ADF_E_ARG, "grid too wide for shared memory");
@@ -670,12 +731,13 @@ static void psi_copy(Solve& s, int axis, bool vside, float* host, bool upload, i
   float* base = vside ? d.psi_v[axis] : d.psi_p[axis];
   const long long side = vside ? d.psi_v_side[axis] : d.psi_p_side[axis];
   float* dev = base + (long long)buffer * 2 * side;
-  if (axis == 0) {
-    size_t bytes = (size_t)2 * side * 4;
+  if (axis == 0) {  // rows of n values, device pitch padded to npp / nvp
+    const size_t pitch = (size_t)(vside ? d.nvp : d.npp) * 4;
+    const size_t rows = (size_t)d.ny * d.nz * 2;
     if (upload)
-      cudaMemcpy(dev, host, bytes, cudaMemcpyHostToDevice);
+      cudaMemcpy2D(dev, pitch, host, (size_t)n * 4, (size_t)n * 4, rows, cudaMemcpyHostToDevice);
     else
-      cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost);
+      cudaMemcpy2D(host, (size_t)n * 4, dev, pitch, (size_t)n * 4, rows, cudaMemcpyDeviceToHost);
     return;
   }
   const size_t rows = axis == 1 ? (size_t)n * d.nz * 2 : (size_t)d.ny * n * 2;
@@ -844,6 +906,7 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
   if (flags != ADF_ARITH_PROMOTE && flags != ADF_ARITH_FP32) return fail(ADF_E_ARG, "bad flags");
   const int64_t npml = cpml ? cpml->npml : 0;
   if (npml < 0 || (npml > 0 && !cpml->coef)) return fail(ADF_E_ARG, "bad cpml");
+  if (npml > 63) return fail(ADF_E_ARG, "npml > 63 is not supported");
   if (stop_step < start_step) return ADF_OK;
   cudaSetDevice(ctx->device);
   const size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);

@@ -63,7 +63,7 @@ struct Solve {
   SolveDev dev;
   std::vector<void*> allocs;
   size_t bytes = 0;
-  CUtensorMap tm[3];
+  CUtensorMap tm[kTmaps];
   int nzc = 32;
   int xh = 1;
   uint32_t* mask_bits = nullptr;

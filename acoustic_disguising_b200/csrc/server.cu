@@ -87,7 +87,7 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
   const adf_gf_request& r = j.req;
   const adf_domain& dd = r.dom;
   if (dd.nx < 4 || dd.ny < 4 || dd.nz < 4 || dd.nx > 512 || dd.nt < 1 || r.n_rec < 0 ||
-      r.npml < 0 || !r.src_tf || (r.n_rec > 0 && (!r.rec_points || !r.rec_normals)) ||
+      r.npml < 0 || r.npml > 63 || !r.src_tf || (r.n_rec > 0 && (!r.rec_points || !r.rec_normals)) ||
       !r.out_p || !r.out_vn)
     return fail(ADF_E_ARG, "bad GF request");
   auto s = std::make_unique<Solve>();
