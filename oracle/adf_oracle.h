@@ -1,7 +1,7 @@
 /*
  * adf_oracle.h -- CPU oracle for the AcousticDisguising FDTD + KH hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is a plain C++17/OpenMP
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain C++17 (std::thread)
  * restatement of the reference's CPU ("Threads" backend) arithmetic.  Only
  * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg / reference
  * arm may load it, and only as the checker or as the timed CPU baseline.  The
