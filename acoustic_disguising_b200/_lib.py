@@ -98,6 +98,9 @@ SIGNATURES = [
     ("adf_time_axis", C.c_int, [C.POINTER(Domain), C.c_void_p]),
     ("adf_cpml_profiles", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
+    ("adf_cpml_profiles_static", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                           C.c_void_p]),
     ("adf_build_mask", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_int, C.c_void_p,
                                  C.c_void_p]),
     ("adf_pack_transceivers", C.c_int, [C.POINTER(Domain), C.c_void_p, C.c_void_p, C.c_void_p,

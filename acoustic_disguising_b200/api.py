@@ -164,6 +164,23 @@ def cpml_profiles(npml: int, vel_max: float, dt: float, rcoef: float, thickness:
     return o32, o64
 
 
+STATIC_CPML_MAX_NPML = 63
+
+
+def cpml_profiles_static(npml: int, vel_max: float, dt: float, rcoef: float, thickness: float,
+                         fc: float, ctx: Context | None = None):
+    """cpml_profiles through adf_cpml_profiles_static: the same values, computed
+    with fixed device scratch (npml <= STATIC_CPML_MAX_NPML) and no device
+    allocation.  The first call per device sets the scratch up, so make it
+    before any stream capture; concurrent calls on one device race."""
+    ctx = ctx or default_context()
+    o32 = np.zeros(8 * npml + 4, np.float32)
+    o64 = np.zeros(8 * npml + 4, np.float64)
+    L.check(L.lib().adf_cpml_profiles_static(ctx.h, npml, vel_max, dt, rcoef, thickness, fc,
+                                             _p(o32), _p(o64)), "cpml_profiles_static")
+    return o32, o64
+
+
 def split_profiles(flat: np.ndarray, npml: int) -> dict:
     n = npml
     sizes = [("a_l", n), ("a_r", n), ("a_hl", n + 1), ("a_hr", n + 1), ("b_l", n), ("b_r", n),

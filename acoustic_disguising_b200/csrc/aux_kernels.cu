@@ -219,4 +219,26 @@ cudaError_t launch_scale_traces(const float* in, float* out, long long n, const 
   return cudaGetLastError();
 }
 
+// Fixed scratch for adf_cpml_profiles_static: room for the profiles of
+// npml <= kStaticCpmlMaxNpml (8*npml+4 values) in Float64 followed by Float32.
+// Nothing in it has to start at zero: the profile kernel writes every value
+// that the copies back to the host read.
+constexpr int kStaticCpmlMaxNpml = 63;
+constexpr int kStaticCpmlMaxVals = 8 * kStaticCpmlMaxNpml + 4;
+static __device__ __align__(256) double g_cpml_scratch[kStaticCpmlMaxVals + kStaticCpmlMaxVals / 2 + 1];
+
+int static_cpml_max_npml() { return kStaticCpmlMaxNpml; }
+
+// Device address of the scratch on the current device.  Taking it is the one
+// set-up step (it may load this module onto the device), so callers do it
+// once per device and keep the pointer.
+cudaError_t static_cpml_scratch(double** d64, float** d32) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_cpml_scratch);
+  if (e != cudaSuccess) return e;
+  *d64 = static_cast<double*>(p);
+  *d32 = reinterpret_cast<float*>(static_cast<double*>(p) + kStaticCpmlMaxVals);
+  return cudaSuccess;
+}
+
 }  // namespace adf

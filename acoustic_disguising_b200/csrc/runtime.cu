@@ -32,6 +32,8 @@ cudaError_t launch_pack_mask(const uint8_t* jl, int nx, int ny, int nz, int mw, 
                              cudaStream_t s);
 cudaError_t launch_injection_coef(double radius, long long n, double dt, double rho, double dx,
                                   double z0, double* out, cudaStream_t s);
+int static_cpml_max_npml();
+cudaError_t static_cpml_scratch(double** d64, float** d32);
 
 thread_local std::string g_err;
 int fail(int code, const std::string& msg) {
@@ -863,6 +865,59 @@ int adf_cpml_profiles(adf_ctx* ctx, int64_t npml, double vel_max, double dt, dou
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   cudaFree(d32);
   cudaFree(d64);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+// adf_cpml_profiles with its scratch in a fixed device array instead of
+// cudaMalloc/cudaFree.  The scratch address is taken once per device, on the
+// first call with that device current, and cached.
+int adf_cpml_profiles_static(adf_ctx* ctx, int64_t npml, double vel_max, double dt,
+                             double rcoef, double thickness, double fc, float* out32,
+                             double* out64) {
+  static std::mutex mu;
+  static int n_dev = -1;
+  static std::vector<double*> dev64;
+  static std::vector<float*> dev32;
+  if (!ctx || npml < 0 || !out32) return fail(ADF_E_ARG, "bad cpml arguments");
+  const int max_npml = static_cpml_max_npml();
+  if (npml > max_npml)
+    return fail(ADF_E_ARG, "npml " + std::to_string(npml) +
+                               " exceeds the fixed scratch of adf_cpml_profiles_static (max " +
+                               std::to_string(max_npml) + "); use adf_cpml_profiles");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  double* d64 = nullptr;
+  float* d32 = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (n_dev < 0) {
+      e = cudaGetDeviceCount(&n_dev);
+      if (e != cudaSuccess) {
+        n_dev = -1;
+        return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+      }
+      dev64.assign((size_t)n_dev, nullptr);
+      dev32.assign((size_t)n_dev, nullptr);
+    }
+    if (ctx->device < 0 || ctx->device >= n_dev) return fail(ADF_E_ARG, "bad device");
+    if (!dev64[(size_t)ctx->device]) {
+      e = static_cpml_scratch(&d64, &d32);
+      if (e != cudaSuccess)
+        return fail(ADF_E_DEVICE, std::string("scratch address: ") + cudaGetErrorString(e));
+      dev64[(size_t)ctx->device] = d64;
+      dev32[(size_t)ctx->device] = d32;
+    }
+    d64 = dev64[(size_t)ctx->device];
+    d32 = dev32[(size_t)ctx->device];
+  }
+  const size_t n = (size_t)(8 * npml + 4);
+  e = launch_cpml_profiles((int)npml, vel_max, dt, rcoef, thickness, fc, d32, d64, ctx->stream);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  e = cudaMemcpyAsync(out32, d32, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && out64)
+    e = cudaMemcpyAsync(out64, d64, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
   return ADF_OK;
 }

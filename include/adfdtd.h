@@ -122,6 +122,21 @@ int adf_time_axis(const adf_domain* d, double* out);
 int adf_cpml_profiles(adf_ctx* ctx, int64_t npml, double vel_max, double dt, double rcoef,
                       double thickness, double fc, float* out32, double* out64);
 
+/* adf_cpml_profiles without any device allocation; no counterpart in the
+ * reference.  For callers that must not allocate or free device memory while
+ * work is in flight: cudaFree synchronizes the whole device (stalling solves
+ * running on other streams), and a serving process may have handed all of
+ * HBM to its solve budget.  Scratch is a fixed device array sized for
+ * npml <= 63 (the largest npml the step kernel accepts); larger npml returns
+ * ADF_E_ARG.  The first call on each device does a one-time set-up (it takes
+ * the array's address, which may load the module), so make it before any
+ * stream capture.  Nothing has to be zeroed first.  Calls that overlap on
+ * one device share the array and race: serialize them.  Results equal
+ * adf_cpml_profiles bit for bit.                                          */
+int adf_cpml_profiles_static(adf_ctx* ctx, int64_t npml, double vel_max, double dt,
+                             double rcoef, double thickness, double fc, float* out32,
+                             double* out64);
+
 /* build_update_mask (src/geometry.jl:250-280), evaluated on the GPU.
  * out_bool: (nx,ny,nz,4) uint8 Julia layout, or NULL.  Returns 1 (writing
  * nothing) for ADF_SHAPE_NONE, as the reference returns `nothing`.        */
