@@ -124,6 +124,7 @@ SIGNATURES = [
     ("adf_server_stop", C.c_int, [C.c_void_p]),
     ("adf_kh_pressure", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
+    ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("adf_injection_coefficients", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_double,
                                              C.c_int64, C.c_void_p]),
 ]

@@ -392,6 +392,41 @@ def injection_coefficients(d: L.Domain, radius: float, n_points: int,
 
 
 # ---------------------------------------------------------------------------
+# Kirchhoff-Helmholtz extrapolation (src/kh_kernels.jl:106-157, 256-296)
+# ---------------------------------------------------------------------------
+def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt: float, sigma: float, c0: float,
+                aq: float, af: float, rho: float = 1.2, window_sigmas: float = 6.0,
+                ctx: Context | None = None) -> np.ndarray:
+    """Two-way KH pressure at targets:
+    out[t, r] = aq sum_s p_p(s,r) (*) in_q[:, s] + af sum_s p_v(s,r) (*) in_f[:, s]
+    with the Gaussian kernels of eval_one_kernel (kh_kernels.jl:106-157).
+    s_pts, s_nrm (ns, 3), r_pts (nr, 3) Float64; in_q, in_f (nt, ns) Float32.
+    Returns out (nt, nr) Float32, Julia (column-major) layout."""
+    ctx = ctx or default_context()
+    f64 = lambda a: np.asfortranarray(a, np.float64)
+    f32 = lambda a: np.asfortranarray(a, np.float32)
+    sp, sn, rp = f64(s_pts), f64(s_nrm), f64(r_pts)
+    q, f = f32(in_q), f32(in_f)
+    ns, nr, nt = sp.shape[0], rp.shape[0], q.shape[0]
+    if sn.shape != (ns, 3) or rp.shape[1] != 3 or q.shape != (nt, ns) or f.shape != (nt, ns):
+        raise ValueError("kh_pressure: shape mismatch")
+    desc = L.KhDescC(ns=ns, nr=nr, nt=nt, dt=dt, sigma=sigma, c0=c0, rho=rho, aq=aq, af=af,
+                     window_sigmas=window_sigmas, s_pts=sp.ctypes.data, s_nrm=sn.ctypes.data,
+                     r_pts=rp.ctypes.data)
+    out = np.zeros((nt, nr), np.float32, order="F")
+    L.check(L.lib().adf_kh_pressure(ctx.h, C.byref(desc), _p(q), _p(f), _p(out)), "kh_pressure")
+    return out
+
+
+def fp32_fma_peak(ctx: Context | None = None):
+    """Measured FP32 FMA throughput (TFLOP/s) and the probe's duration (ms)."""
+    ctx = ctx or default_context()
+    tf, ms = C.c_double(), C.c_double()
+    L.check(L.lib().adf_fp32_fma_peak(ctx.h, C.byref(tf), C.byref(ms)), "fp32_fma_peak")
+    return tf.value, ms.value
+
+
+# ---------------------------------------------------------------------------
 # Impulsive Green's-function solves (src/greens.jl:48-234)
 # ---------------------------------------------------------------------------
 @dataclass

@@ -248,6 +248,11 @@ typedef struct {
 int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
                     const float* in_f, float* out);
 
+/* Measured FP32 FMA throughput of the device (TFLOP/s, 2 FLOP per FMA): the
+ * roofline denominator of adf_kh_pressure.  Measurement helper with no
+ * reference counterpart; ms (optional) receives the probe's duration.      */
+int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms);
+
 /* C_for_N (diagnostics/_check_inject_kh/injection_coefficients.jl:467-472)
  * with fib_sphere_area (src/io.jl:131), in FP64 on the GPU:
  * out[0]=C_f, out[1]=C_q, out[2]=dS.                                       */
