@@ -31,6 +31,7 @@
 // variant.  Injection/recording (derivatives.jl:30-60) is pure Float32 with
 // separate multiply and add, as the reference computes it.
 #include "adf_internal.h"
+#include "ptx_util.h"
 
 namespace adf {
 
@@ -40,46 +41,12 @@ constexpr int NTHREADS = NCT + 32;
 constexpr int kMaxStages = 8;
 constexpr int kPnBufs = 3;
 constexpr int kMaxCoef = 8 * 63 + 4;  // CPML coefficients for npml <= 63
-constexpr uint32_t kWaitLimit = 1u << 24;
 
 int consumer_threads() { return NCT; }
 
 // ---------------------------------------------------------------------------
-// PTX wrappers
+// TMA tensor loads (no multicast)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t a) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: gives up after kWaitLimit polls so that a logic error
-// surfaces as an error code instead of a hung GPU.  try_wait itself suspends
-// the thread for a bounded, hardware-chosen interval, so the loop does not
-// spin hot and wakes as soon as the phase completes.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
-    if (mbar_try_wait(a, parity)) return true;
-  return false;
-}
 __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
                                             int c0, int c1, int c2, int c3, int c4) {
   asm volatile(

@@ -16,14 +16,19 @@
 // surface point) pair's taps are evaluated on the fly from its geometry.
 //
 // Work decomposition (CUDA cores, FP32 FMA bound):
-//   CTA   = 32 targets x one block of 256 output samples, 8 warps
-//   warp  = 4 targets; lane = 8 consecutive output samples of each
-//   loop  = surface points in chunks of SC: the chunk's input windows are
-//           staged in shared memory (skewed by one word per eight so that
-//           lanes reading 8 samples apart hit distinct banks), the chunk's
-//           pair geometry is computed in FP64, each pair's 2*LM taps are
+//   CTA   = 32 targets x one block of 32*T output samples, 16 warps
+//   warp  = 2 targets; lane = T consecutive output samples of each (T odd)
+//   loop  = surface points in chunks of SC.  One thread stages chunk c+1's
+//           input windows into shared memory with bulk async copies while
+//           the CTA works on chunk c (double buffer, mbarrier completion);
+//           the input columns are zero-padded on the device so that every
+//           window is one aligned, in-bounds copy.  Each chunk's pair
+//           geometry is computed in FP64, each pair's 2*LM taps are
 //           evaluated one per lane into a per-warp buffer, and every lane
-//           forms its 8 outputs with 2*LM*8 register FMAs.
+//           forms its T outputs with LM*T paired FMAs (__ffma2_rn: the
+//           monopole and dipole channel in one instruction) from a window
+//           of T+LM-1 samples per channel.  Lanes start T samples apart, an
+//           odd stride, so the 32 lanes of a window load hit 32 banks.
 //   The per-pair partial sums are added to the output accumulators with a
 //   compensated (Kahan) FP32 sum, so the sum over thousands of surface
 //   points keeps FP32 round-off at the level of a single addition.
@@ -31,25 +36,37 @@
 #include <cstring>
 #include <vector>
 
+#include "ptx_util.h"
 #include "runtime.h"
 
 namespace adf {
 
 namespace {
 
-constexpr int KH_T = 8;                 // output samples per lane
-constexpr int KH_WARPS = 8;
+#ifndef KH_NT
+#define KH_NT 9
+#endif
+#ifndef KH_NWARPS
+#define KH_NWARPS 16
+#endif
+#ifndef KH_NRW
+#define KH_NRW 2
+#endif
+constexpr int KH_T = KH_NT;              // output samples per lane (odd)
+constexpr int KH_WARPS = KH_NWARPS;
 constexpr int KH_THREADS = 32 * KH_WARPS;
-constexpr int KH_TB = 32 * KH_T;        // output samples per CTA
-constexpr int KH_RW = 4;                // targets per warp
-constexpr int KH_RT = KH_WARPS * KH_RW; // targets per CTA
-constexpr int KH_SC_MAX = 32;           // surface points per staged chunk
+constexpr int KH_TB = 32 * KH_T;         // output samples per CTA
+constexpr int KH_RW = KH_NRW;            // targets per warp
+constexpr int KH_RT = KH_WARPS * KH_RW;  // targets per CTA
+constexpr int KH_SC_MAX = 32;            // surface points per staged chunk
+static_assert(KH_T % 2 == 1, "lanes must start an odd number of samples apart");
 
 struct KhParams {
   int ns, nr, nt;
   int sc;           // surface points per chunk
-  int wlen;         // staged samples per channel and surface point
-  int rowpad;       // floats per staged row (skewed)
+  int rowpad;       // staged floats per channel and surface point (multiple of 4)
+  int pad;          // zero samples in front of each padded input column
+  long long pitch;  // floats per padded input column (multiple of 4)
   double inv_c0dt;  // 1 / (c0 dt)
   double hw;        // window half width in samples
   double cq;        // -aq C dt / sigma^2            (C = 1/(sqrt(2 pi) sigma))
@@ -60,84 +77,75 @@ struct KhParams {
   const double* sn;
   const double* rp;  // (nr,3)
   const int2* tile_lo;  // per target tile: {lo_min, lo_max}
-  const float* in_q;    // (nt, ns)
+  const float* in_q;    // (pitch, ns): zero-padded columns, sample t at pad + t
   const float* in_f;
   float* out;           // (nt, nr)
   int* err;
 };
-
-// Loads 8+LM-1 consecutive staged samples.  The staged address of sample m
-// is m + m/8; a lane's window starts at m0 = 8*(lane+q) + rho, so with the
-// base at 9*(lane+q) the offsets are compile-time for each rho.
-template <int XN, int RHO>
-__device__ __forceinline__ void kh_load_win(const float* __restrict__ b, float* x) {
-#pragma unroll
-  for (int i = 0; i < XN; ++i) x[i] = b[RHO + i + ((RHO + i) >> 3)];
-}
-
-template <int XN>
-__device__ __forceinline__ void kh_load(const float* b, int rho, float* x) {
-  switch (rho) {
-    case 0: kh_load_win<XN, 0>(b, x); break;
-    case 1: kh_load_win<XN, 1>(b, x); break;
-    case 2: kh_load_win<XN, 2>(b, x); break;
-    case 3: kh_load_win<XN, 3>(b, x); break;
-    case 4: kh_load_win<XN, 4>(b, x); break;
-    case 5: kh_load_win<XN, 5>(b, x); break;
-    case 6: kh_load_win<XN, 6>(b, x); break;
-    default: kh_load_win<XN, 7>(b, x); break;
-  }
-}
 
 }  // namespace
 
 template <int LM>
 __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams p) {
   constexpr int XN = KH_T + LM - 1;
-  extern __shared__ __align__(16) float smem[];
+  extern __shared__ __align__(128) float smem[];
+  __shared__ __align__(8) uint64_t full[2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x;
   const int tb = blockIdx.y * KH_TB;
   const int r_base = tile * KH_RT;
   const int2 lob = p.tile_lo[tile];
   const int lo_min = lob.x, lo_max = lob.y;
+  // first staged sample, rounded down to a 16-B boundary of the padded column
   const int g0 = tb - lo_max - (LM - 1);
+  const int col0 = p.pad + g0;
+  const int shift = col0 & 3;
+  const float* colq = p.in_q + (col0 - shift);
+  const float* colf = p.in_f + (col0 - shift);
+  const int npair = KH_RT * p.sc;
 
-  float* win = smem;                                     // [sc][2][rowpad]
-  int* pr_lo = reinterpret_cast<int*>(win + (size_t)p.sc * 2 * p.rowpad);
-  int* pr_n = pr_lo + KH_RT * p.sc;
-  float* pr_wb = reinterpret_cast<float*>(pr_n + KH_RT * p.sc);
-  float* pr_q = pr_wb + KH_RT * p.sc;
-  float* pr_f1 = pr_q + KH_RT * p.sc;
-  float* pr_f2 = pr_f1 + KH_RT * p.sc;
-  float* taps = pr_f2 + KH_RT * p.sc;                    // [warps][RW][2][LM]
+  // shared memory: 2 window buffers [sc][2][rowpad], 2 pair-parameter
+  // buffers [6][RT*sc], per-warp taps [warps][RW][LM][2]
+  const int wbuf = p.sc * 2 * p.rowpad;
+  float* const par0 = smem + 2 * wbuf;
+  float* taps = par0 + 12 * npair;
   float* my_taps = taps + warp * (KH_RW * 2 * LM);
 
-  float sum[KH_RW][KH_T], comp[KH_RW][KH_T];
-#pragma unroll
-  for (int r = 0; r < KH_RW; ++r)
-#pragma unroll
-    for (int j = 0; j < KH_T; ++j) sum[r][j] = comp[r][j] = 0.f;
+  const int nchunks = (p.ns + p.sc - 1) / p.sc;
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&full[0]), 1);
+    mbar_init(smem_u32(&full[1]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
-  for (int s0 = 0; s0 < p.ns; s0 += p.sc) {
+  // bulk copies of chunk c (one thread)
+  auto stage = [&](int c) {
+    const int s0 = c * p.sc;
     const int nsc = min(p.sc, p.ns - s0);
-    __syncthreads();  // the previous chunk's readers are done
-    // stage the chunk's input windows, zero outside [0, nt)
-    const int per_row = p.wlen;
-    const int total = nsc * 2 * per_row;
-    for (int idx = threadIdx.x; idx < total; idx += KH_THREADS) {
-      const int row = idx / per_row;
-      const int m = idx - row * per_row;
-      const int sl = row >> 1;
-      const int g = g0 + m;
-      float v = 0.f;
-      if (g >= 0 && g < p.nt) {
-        const float* src = (row & 1) ? p.in_f : p.in_q;
-        v = __ldg(src + (size_t)(s0 + sl) * p.nt + g);
-      }
-      win[(size_t)row * p.rowpad + m + (m >> 3)] = v;
+    const uint32_t mb = smem_u32(&full[c & 1]);
+    const uint32_t row_bytes = (uint32_t)p.rowpad * 4u;
+    // the buffer's previous contents were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(mb, row_bytes * 2u * (uint32_t)nsc);
+    float* w = smem + (c & 1) * wbuf;
+    for (int sl = 0; sl < nsc; ++sl) {
+      const size_t off = (size_t)(s0 + sl) * p.pitch;
+      bulk_load(smem_u32(w + (size_t)(2 * sl) * p.rowpad), colq + off, row_bytes, mb);
+      bulk_load(smem_u32(w + (size_t)(2 * sl + 1) * p.rowpad), colf + off, row_bytes, mb);
     }
-    // pair geometry in FP64
+  };
+  // pair geometry of chunk c in FP64 (all threads)
+  auto params = [&](int c) {
+    const int s0 = c * p.sc;
+    const int nsc = min(p.sc, p.ns - s0);
+    float* pb = par0 + (c & 1) * 6 * npair;
+    int* pr_lo = reinterpret_cast<int*>(pb);
+    int* pr_n = pr_lo + npair;
+    float* pr_wb = pb + 2 * npair;
+    float* pr_q = pb + 3 * npair;
+    float* pr_f1 = pb + 4 * npair;
+    float* pr_f2 = pb + 5 * npair;
     for (int idx = threadIdx.x; idx < KH_RT * nsc; idx += KH_THREADS) {
       const int rr = idx % KH_RT, sl = idx / KH_RT;
       const int r = r_base + rr, s = s0 + sl;
@@ -177,9 +185,39 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
       pr_f1[pi] = f1;
       pr_f2[pi] = f2;
     }
-    __syncthreads();
+  };
 
-    for (int sl = 0; sl < nsc; ++sl) {
+  float sum[KH_RW][KH_T], comp[KH_RW][KH_T];
+#pragma unroll
+  for (int r = 0; r < KH_RW; ++r)
+#pragma unroll
+    for (int j = 0; j < KH_T; ++j) sum[r][j] = comp[r][j] = 0.f;
+
+  if (threadIdx.x == 0) stage(0);
+  params(0);
+  __syncthreads();
+  bool ok = true;
+  for (int c = 0; c < nchunks; ++c) {
+    // chunk c+1's buffers were last read in chunk c-1, which every thread
+    // has finished (barrier at the end of the previous iteration)
+    if (c + 1 < nchunks) {
+      if (threadIdx.x == 0) stage(c + 1);
+      params(c + 1);
+    }
+    if (!mbar_wait(smem_u32(&full[c & 1]), (uint32_t)(c >> 1) & 1u)) {
+      if (threadIdx.x == 0) atomicOr(p.err, 2);
+      ok = false;
+    }
+    const int nsc = min(p.sc, p.ns - c * p.sc);
+    const float* win = smem + (c & 1) * wbuf + shift;
+    const float* pb = par0 + (c & 1) * 6 * npair;
+    const int* pr_lo = reinterpret_cast<const int*>(pb);
+    const int* pr_n = pr_lo + npair;
+    const float* pr_wb = pb + 2 * npair;
+    const float* pr_q = pb + 3 * npair;
+    const float* pr_f1 = pb + 4 * npair;
+    const float* pr_f2 = pb + 5 * npair;
+    for (int sl = 0; ok && sl < nsc; ++sl) {
       const float* wq = win + (size_t)(2 * sl) * p.rowpad;
       const float* wf = wq + p.rowpad;
       // taps of this warp's targets: lane-parallel, one exp per tap
@@ -194,43 +232,37 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
           const float w = wb + (float)kp;
           const float e = expf(-p.a * (w * w));
           const float v = kk < LM ? pr_q[pi] * w * e : (pr_f1[pi] + pr_f2[pi] * w) * e;
-          my_taps[rho * 2 * LM + kk] = kp < n ? v : 0.f;
+          // interleaved {monopole, dipole} per tap for the paired FMA
+          my_taps[rho * 2 * LM + 2 * kp + (kk >= LM)] = kp < n ? v : 0.f;
         }
       }
       __syncwarp();
 #pragma unroll
       for (int rho = 0; rho < KH_RW; ++rho) {
         const int pi = sl * KH_RT + warp * KH_RW + rho;
-        const int d = lo_max - pr_lo[pi];
-        const int base = 9 * (lane + (d >> 3));
-        float xq[XN], xf[XN];
-        kh_load<XN>(wq + base, d & 7, xq);
-        kh_load<XN>(wf + base, d & 7, xf);
-        float c[KH_T];
+        const int base = KH_T * lane + (lo_max - pr_lo[pi]);
+        // {monopole, dipole} input pairs: one paired FMA per tap and sample
+        float2 x2[XN];
 #pragma unroll
-        for (int j = 0; j < KH_T; ++j) c[j] = 0.f;
-        const float4* tq = reinterpret_cast<const float4*>(my_taps + rho * 2 * LM);
-        const float4* tf = tq + LM / 4;
+        for (int i = 0; i < XN; ++i) x2[i] = make_float2(wq[base + i], wf[base + i]);
+        float2 c2[KH_T];
 #pragma unroll
-        for (int k4 = 0; k4 < LM / 4; ++k4) {
-          const float4 a4 = tq[k4];
-          const float4 b4 = tf[k4];
-          const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-          const float bv[4] = {b4.x, b4.y, b4.z, b4.w};
+        for (int j = 0; j < KH_T; ++j) c2[j] = make_float2(0.f, 0.f);
+        const float4* t4p = reinterpret_cast<const float4*>(my_taps + rho * 2 * LM);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int k = 4 * k4 + q;
+        for (int k2 = 0; k2 < LM / 2; ++k2) {
+          const float4 t4 = t4p[k2];
+          const float2 ta = make_float2(t4.x, t4.y), tb2 = make_float2(t4.z, t4.w);
 #pragma unroll
-            for (int j = 0; j < KH_T; ++j) {
-              c[j] = fmaf(av[q], xq[j + LM - 1 - k], c[j]);
-              c[j] = fmaf(bv[q], xf[j + LM - 1 - k], c[j]);
-            }
-          }
+          for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(ta, x2[j + LM - 1 - 2 * k2], c2[j]);
+#pragma unroll
+          for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(tb2, x2[j + LM - 2 - 2 * k2], c2[j]);
         }
         // compensated accumulation over surface points
 #pragma unroll
         for (int j = 0; j < KH_T; ++j) {
-          const float y = __fsub_rn(c[j], comp[rho][j]);
+          const float cj = __fadd_rn(c2[j].x, c2[j].y);
+          const float y = __fsub_rn(cj, comp[rho][j]);
           const float t = __fadd_rn(sum[rho][j], y);
           comp[rho][j] = __fsub_rn(__fsub_rn(t, sum[rho][j]), y);
           sum[rho][j] = t;
@@ -238,23 +270,19 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
       }
       __syncwarp();  // taps of the next surface point overwrite the buffer
     }
+    __syncthreads();
   }
 
-  // outputs: lane owns samples tb + 8*lane .. +7 of each of its targets
+  // outputs: lane owns samples tb + T*lane .. +T-1 of each of its targets
 #pragma unroll
   for (int rho = 0; rho < KH_RW; ++rho) {
     const int r = r_base + warp * KH_RW + rho;
     if (r >= p.nr) continue;
     const int t0 = tb + KH_T * lane;
     float* o = p.out + (size_t)r * p.nt + t0;
-    if (t0 + KH_T <= p.nt && ((p.nt & 3) == 0)) {
-      reinterpret_cast<float4*>(o)[0] = make_float4(sum[rho][0], sum[rho][1], sum[rho][2], sum[rho][3]);
-      reinterpret_cast<float4*>(o)[1] = make_float4(sum[rho][4], sum[rho][5], sum[rho][6], sum[rho][7]);
-    } else {
 #pragma unroll
-      for (int j = 0; j < KH_T; ++j)
-        if (t0 + j < p.nt) o[j] = sum[rho][j];
-    }
+    for (int j = 0; j < KH_T; ++j)
+      if (t0 + j < p.nt) o[j] = sum[rho][j];
   }
 }
 
@@ -332,7 +360,7 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
   const double inv_c0dt = 1.0 / (d->c0 * d->dt);
   const int ntiles = (nr + KH_RT - 1) / KH_RT;
   std::vector<int2> tlo((size_t)ntiles);
-  int wmax = 0;
+  int wmax = 0, lo_all = 0;
   for (int t = 0; t < ntiles; ++t) {
     double dmin = 1e300, dmax = 0;
     for (int r = t * KH_RT; r < std::min(nr, (t + 1) * KH_RT); ++r) {
@@ -348,15 +376,25 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
     lo_min = std::min(lo_min, lo_max);
     tlo[(size_t)t] = make_int2(lo_min, lo_max);
     wmax = std::max(wmax, KH_TB + (lo_max - lo_min) + lm - 1);
+    lo_all = std::max(lo_all, lo_max);
   }
   // multiple of 4 floats so the tap buffer behind the rows stays 16-B aligned
-  const int rowpad = ((wmax - 1) + ((wmax - 1) >> 3) + 1 + 3) / 4 * 4;
+  // A staged row starts up to 3 samples early (16-B aligned source) and is a
+  // multiple of 4 floats, so every bulk copy and the tap buffer stay aligned.
+  const int rowpad = (wmax + 3 + 3) / 4 * 4;
   const size_t tap_bytes = (size_t)KH_WARPS * KH_RW * 2 * lm * 4;
-  const size_t per_s = (size_t)2 * rowpad * 4 + (size_t)6 * KH_RT * 4;
+  const size_t per_s = 2 * ((size_t)2 * rowpad * 4 + (size_t)6 * KH_RT * 4);  // double-buffered
+  const size_t smem_cap = (size_t)ctx->smem_optin - 256;  // static mbarriers
   int sc = KH_SC_MAX;
-  while (sc > 1 && per_s * sc + tap_bytes > (size_t)ctx->smem_optin) --sc;
+  while (sc > 1 && per_s * sc + tap_bytes > smem_cap) --sc;
   const size_t smem = per_s * sc + tap_bytes;
-  if (smem > (size_t)ctx->smem_optin)
+  // Input columns are zero-padded so that every staged window lies inside
+  // its column: pad zeros before sample 0 cover the earliest window start,
+  // the tail covers the last time block's window end.
+  const int nblk = (nt + KH_TB - 1) / KH_TB;
+  const int pad = (lo_all + lm + 4 + 3) / 4 * 4;
+  const long long pitch = ((long long)pad + (long long)nblk * KH_TB + lo_all + 16 + 3) / 4 * 4;
+  if (smem > smem_cap)
     return fail(ADF_E_ARG, "adf_kh_pressure: the targets' delay spread needs a " +
                                std::to_string(wmax) + "-sample window, more than shared memory holds");
 
@@ -365,21 +403,27 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
   DevBuf<int2> dtlo;
   DevBuf<int> derr;
   if (!dsp.alloc((size_t)3 * ns) || !dsn.alloc((size_t)3 * ns) || !drp.alloc((size_t)3 * nr) ||
-      !dq.alloc((size_t)nt * ns) || !df.alloc((size_t)nt * ns) || !dout.alloc((size_t)nt * nr) ||
+      !dq.alloc((size_t)pitch * ns) || !df.alloc((size_t)pitch * ns) ||
+      !dout.alloc((size_t)nt * nr) ||
       !dtlo.alloc((size_t)ntiles) || !derr.alloc(1))
     return fail(ADF_E_NOMEM, "adf_kh_pressure: device allocation failed");
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(dsp.p, d->s_pts, (size_t)24 * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(dsn.p, d->s_nrm, (size_t)24 * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(drp.p, d->r_pts, (size_t)24 * nr, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(dq.p, in_q, (size_t)4 * nt * ns, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(df.p, in_f, (size_t)4 * nt * ns, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dq.p, 0, (size_t)4 * pitch * ns, st);
+  cudaMemsetAsync(df.p, 0, (size_t)4 * pitch * ns, st);
+  cudaMemcpy2DAsync(dq.p + pad, (size_t)4 * pitch, in_q, (size_t)4 * nt, (size_t)4 * nt, ns,
+                    cudaMemcpyHostToDevice, st);
+  cudaMemcpy2DAsync(df.p + pad, (size_t)4 * pitch, in_f, (size_t)4 * nt, (size_t)4 * nt, ns,
+                    cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(dtlo.p, tlo.data(), sizeof(int2) * ntiles, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(derr.p, 0, sizeof(int), st);
 
   KhParams p;
   p.ns = ns; p.nr = nr; p.nt = nt;
-  p.sc = sc; p.wlen = wmax; p.rowpad = rowpad;
+  p.sc = sc; p.rowpad = rowpad;
+  p.pad = pad; p.pitch = pitch;
   p.inv_c0dt = inv_c0dt;
   p.hw = hw;
   const double C = 1.0 / (std::sqrt(2.0 * M_PI) * d->sigma);
