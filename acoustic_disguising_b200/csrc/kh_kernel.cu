@@ -16,8 +16,9 @@
 // surface point) pair's taps are evaluated on the fly from its geometry.
 //
 // Work decomposition (CUDA cores, FP32 FMA bound):
-//   CTA   = 32 targets x one block of 32*T output samples, 16 warps
-//   warp  = 2 targets; lane = T consecutive output samples of each (T odd)
+//   CTA   = 16 targets x one block of 32*T output samples, 16 warps
+//   warp  = KH_RW targets (default 1); lane = T consecutive output samples
+//           of each (T odd, default 13)
 //   loop  = surface points in chunks of SC.  One thread stages chunk c+1's
 //           input windows into shared memory with bulk async copies while
 //           the CTA works on chunk c (double buffer, mbarrier completion);
@@ -44,13 +45,13 @@ namespace adf {
 namespace {
 
 #ifndef KH_NT
-#define KH_NT 9
+#define KH_NT 13
 #endif
 #ifndef KH_NWARPS
 #define KH_NWARPS 16
 #endif
 #ifndef KH_NRW
-#define KH_NRW 2
+#define KH_NRW 1
 #endif
 constexpr int KH_T = KH_NT;              // output samples per lane (odd)
 constexpr int KH_WARPS = KH_NWARPS;

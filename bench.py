@@ -15,6 +15,15 @@ time step, graph-captured), and the p / v_n traces copied back.
   roofline : the fused step kernel's algorithmic HBM bytes per launch over
           its mean launch time (per-launch CUDA events), against the
           measured copy bandwidth
+  kh    : Kirchhoff-Helmholtz extrapolation of 4096 surface points (Ricker-
+          filtered noise traces, 2048 samples at 5 us) to 16384 targets on a
+          2 m sphere: TFLOP/s of the KH kernel against the FP32 FMA peak
+          measured in the same run, the C-ABI call's wall time, and the
+          relative L2 error of a sample of targets against the FP64 oracle
+  serving : a Poisson stream of GF solves of mixed grid sizes (96..256^3),
+          step counts (500..3000) and scatterers, offered at 1.5x the plain
+          path's capacity: p50/p99 latency and solves/s of the continuous-
+          batching server against the plain one-solve-at-a-time path
 
 `--impl reference` times the CPU restatement of the reference's Threads
 path (oracle/) on this host's cores on a bounded sample of the same solve.
@@ -72,6 +81,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT,
                     help="steps per solve (profiling runs only; the metric uses 2000)")
+    ap.add_argument("--no-kh", action="store_true", help="skip the KH section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--serving-requests", type=int, default=20)
     return ap.parse_args()
 
 
@@ -239,6 +251,170 @@ def reference_arm(args):
     return 0
 
 
+
+# ---------------------------------------------------------------------------
+# Kirchhoff-Helmholtz extrapolation: 4096 surface points -> 16384 targets
+# ---------------------------------------------------------------------------
+KH_NS, KH_NR, KH_NT, KH_DT = 4096, 16384, 2048, 5e-6
+KH_R_SURF, KH_R_TGT, KH_F3DB, KH_SEED = 0.25, 2.0, 20e3, 20261203
+
+
+def ricker_noise(rng, nt, ns, dt, fc):
+    """Ricker-filtered Gaussian noise (nt, ns), unit RMS per column, float32."""
+    x = rng.standard_normal((nt, ns))
+    half = int(2.0 / fc / dt)
+    tw = np.arange(-half, half + 1) * dt
+    w = np.pi * fc * tw
+    r = (1 - 2 * w * w) * np.exp(-w * w)
+    nfft = 1 << int(math.ceil(math.log2(nt + len(r))))
+    y = np.fft.irfft(np.fft.rfft(x, nfft, axis=0) * np.fft.rfft(r, nfft)[:, None], nfft,
+                     axis=0)[half:half + nt]
+    y /= np.sqrt((y * y).mean(axis=0, keepdims=True))
+    return np.asfortranarray(y.astype(np.float32))
+
+
+def kh_section(A, ctx, steps, warmup):
+    sp, sn = A.fibonacci_sphere(KH_NS, KH_R_SURF)
+    rp, _ = A.fibonacci_sphere(KH_NR, KH_R_TGT)
+    rng = np.random.default_rng(KH_SEED)
+    p_tr = ricker_noise(rng, KH_NT, KH_NS, KH_DT, 8e3)
+    vn_tr = ricker_noise(rng, KH_NT, KH_NS, KH_DT, 8e3)
+    sigma = math.sqrt(math.log(2.0)) / (2 * math.pi * KH_F3DB)
+    dS = 4 * math.pi * KH_R_SURF ** 2 / KH_NS
+    aq, af = -RHO * dS * KH_DT, -dS * KH_DT  # part3_kh_extrapolation.jl:168-185 scales
+    peak_tf, _ = A.fp32_fma_peak(ctx)
+    out = None
+    kms, walls = [], []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        out = A.kh_pressure(sp, sn, rp, vn_tr, p_tr, KH_DT, sigma, C0, aq, af, rho=RHO, ctx=ctx)
+        w = time.perf_counter() - t0
+        ms, _ = ctx.last_timing()
+        if i >= warmup:
+            kms.append(ms)
+            walls.append(w)
+    h2d, d2h = ctx.last_io_bytes()
+    flop = 64.0 * KH_NS * KH_NR * KH_NT  # 2 channels x 16 taps x 2 FLOP per pair-sample
+    k_ms = statistics.mean(kms)
+    achieved = flop / (k_ms / 1e3) / 1e12
+    # parity sample: the first 16 targets against the FP64 oracle
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+
+    O.build()
+    nchk = 16
+    ref = O.kh_pressure(sp, sn, rp, vn_tr, p_tr, KH_DT, sigma, C0, aq, af, r_begin=0,
+                        r_end=nchk, mode=1)
+    rel = float(np.linalg.norm(out[:, :nchk] - ref) / np.linalg.norm(ref))
+    return {
+        "workload": "KH pressure, 4096 Fibonacci surface points r=0.25 m with normals -> "
+                    "16384 targets on a 2 m sphere, 2048 samples at dt=5 us, Gaussian kernel "
+                    "f_3db=20 kHz (+-6 sigma, 16 taps), Ricker-filtered noise traces (seeded)",
+        "value": flop / (k_ms / 1e3) / 1e12, "unit": "TFLOP/s", "kernel_ms": k_ms,
+        "e2e": {"value": flop / statistics.mean(walls) / 1e12, "unit": "TFLOP/s",
+                "wall_ms": statistics.mean(walls) * 1e3, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "fp32 fma", "achieved": achieved, "peak": peak_tf,
+                     "unit": "TFLOP/s", "frac": achieved / peak_tf,
+                     "peak_source": "measured in this run (adf_fp32_fma_peak)",
+                     "flop_per_launch": flop, "traffic": None},
+        "rel_l2_vs_fp64_oracle": rel, "parity_sample": f"targets 0..{nchk - 1}, all samples",
+        "tolerance": 1e-5, "steps": steps, "warmup": warmup,
+    }
+
+
+# ---------------------------------------------------------------------------
+# Serving: Poisson stream of mixed GF solves, batched server vs plain path
+# ---------------------------------------------------------------------------
+SERVE_SIZES = (96, 128, 160, 192, 256)
+SERVE_BUDGET = 120 * 10 ** 9
+
+
+def serving_requests(A, n_req, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_req):
+        n = int(rng.choice(SERVE_SIZES))
+        steps = int(rng.integers(500, 3001))
+        xmax = (n - 1) * DX / 2
+        d = A.Domain(tmax=tmax_of(steps), xmax=xmax, nx=n, c0=C0, r0=RHO, cf=0.5)
+        tf, _ = A.impulsive_wavelet(d, F3DB)
+        shape = str(rng.choice(["none", "sphere", "cube", "ellipsoid"]))
+        size = rng.uniform(0.1, 0.3) * 2 * xmax  # at most 30 % of the domain
+        centre = rng.uniform(-0.2, 0.2, 3) * xmax
+        kw = {}
+        if shape == "sphere":
+            kw = dict(radius=size / 2, center=tuple(centre))
+        elif shape == "cube":
+            kw = dict(length=size, center=tuple(centre))
+        elif shape == "ellipsoid":
+            kw = dict(semi_axes=tuple(size / 2 * rng.uniform(0.5, 1.0, 3)), center=tuple(centre))
+        u = rng.standard_normal(3)
+        src = 0.75 * xmax * u / np.linalg.norm(u)
+        rp, rn = A.fibonacci_sphere(256, 0.6 * xmax)
+        out.append(A.GfRequest(d, src, [1.0, 0.0, 0.0, 0.0], tf, rp, rn, npml=NPML,
+                               pml_rcoef=1e-4, pml_fc=PML_FC, scatterer=shape, scatterer_kw=kw))
+    return out
+
+
+def serving_section(A, ctx, n_req):
+    seed = 20261203
+    # plain path: one solve at a time, service time per request
+    service = []
+    for r in serving_requests(A, n_req, seed):
+        t0 = time.perf_counter()
+        A.gf_solve_batch([r], batched=False, ctx=ctx)
+        service.append(time.perf_counter() - t0)
+    cap = n_req / sum(service)
+    lam = 1.5 * cap
+    arr = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / lam, n_req))
+    arr -= arr[0]
+    fin, t = [], 0.0
+    for a, s in zip(arr, service):  # FIFO single server
+        t = max(t, a) + s
+        fin.append(t)
+    plain_lat = np.array(fin) - arr
+    plain_sps = n_req / (fin[-1] - arr[0])
+    # batched: the continuous-batching server fed the same arrivals in real time
+    reqs = serving_requests(A, n_req, seed)
+    srv = A.Server(hbm_budget=SERVE_BUDGET, ctx=ctx)
+    ids = []
+    t0 = time.perf_counter()
+    for a, r in zip(arr, reqs):
+        dly = t0 + a - time.perf_counter()
+        if dly > 0:
+            time.sleep(dly)
+        ids.append(srv.submit(r))
+    lat, done_at = {}, {}
+    while len(lat) < n_req:
+        for i in ids:
+            if i in lat:
+                continue
+            st, ms = srv.poll(i)
+            if st == 1:
+                lat[i] = ms / 1e3
+                done_at[i] = time.perf_counter() - t0
+            elif st < 0:
+                raise RuntimeError(f"serving request {i} failed: {st}")
+        time.sleep(0.002)
+    srv.stop()
+    b_lat = np.array([lat[i] for i in ids])
+    b_sps = n_req / (max(done_at.values()) - arr[0])
+    pct = lambda x, q: float(np.percentile(x, q))
+    return {
+        "workload": f"{n_req} impulsive GF solves, grids {{96,128,160,192,256}}^3 drawn "
+                    "uniformly, 500-3000 steps, scatterer none/sphere/cube/ellipsoid (random "
+                    "centre, size <= 30% of the domain), 10-cell CPML, 256-point shell; "
+                    "Poisson arrivals at 1.5x the plain path's capacity; 120 GB HBM budget",
+        "batched": {"solves_per_s": b_sps, "p50_ms": pct(b_lat, 50) * 1e3,
+                    "p99_ms": pct(b_lat, 99) * 1e3},
+        "plain": {"solves_per_s": plain_sps, "p50_ms": pct(plain_lat, 50) * 1e3,
+                  "p99_ms": pct(plain_lat, 99) * 1e3,
+                  "note": "one solve per launch sequence; latencies from its measured "
+                          "per-request service times queued FIFO on the same arrivals"},
+        "speedup_solves_per_s": b_sps / plain_sps, "arrival_rate_per_s": lam,
+    }
+
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
@@ -309,6 +485,12 @@ def b200_arm(args):
     region = time.perf_counter() - t_region
     clk = clocks.stop()
     k_ms, k_n = ctx.kernel_timing(reset=True)
+    ctx.set_kernel_timing(False)
+    extra = {}
+    if world == 1 and not args.no_kh:
+        extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
+    if world == 1 and not args.no_serving:
+        extra["serving"] = serving_section(A, ctx, args.serving_requests)
     dev_total = reduce_max(sum(devs))
     wall_total = reduce_max(sum(walls))
     k_avg_ms = reduce_max(k_ms / max(k_n, 1))
@@ -354,6 +536,7 @@ def b200_arm(args):
         "clocks": clk,
         "region_wall_s": region,
     }
+    line.update(extra)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sec = cpu_sample(args.cpu_steps, threads)
