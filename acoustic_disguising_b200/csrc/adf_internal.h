@@ -139,10 +139,11 @@ inline __host__ __device__ int pn_plane_floats(int ty, int nxp) { return round32
 enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_DRAIN_TIMEOUT = 3 };
 
 // launch helpers implemented in fdtd_kernels.cu
+// two_per_sm selects the build of the step kernel sized for two CTAs per SM
 cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
-                        bool fp32);
+                        bool two_per_sm);
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
-cudaError_t step_kernel_attributes(size_t smem, bool fp32);
+cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm);
 int consumer_threads();
 
 }  // namespace adf

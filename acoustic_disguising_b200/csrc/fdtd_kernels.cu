@@ -404,6 +404,78 @@ __device__ __forceinline__ void v_quad(const SolveDev& S, const Regs<R>& g, cons
     st4(S.psi_v[2] + c.wb * S.psi_v_buf[2] + oz, make_float4(mzv[0], mzv[1], mzv[2], mzv[3]));
 }
 
+// ---- one cell of a boundary quad on an ordinary tile-plane: no rigid plane
+// and no y/z slab here, only the x slab and the last x cells.  Same
+// arithmetic as p_quad / v_quad for that cell.
+template <typename R>
+__device__ __forceinline__ void p_xcell(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
+                                        int r, int x, bool owned) {
+  const int nxp = g.nxp, nx = S.nx, npml = S.npml;
+  const int o = r * nxp + x;
+  const float P = c.sP[o];
+  const float X0 = c.sVx[o];
+  const float X1 = (x + 1 < nxp) ? c.sVx[o + 1] : 0.f;
+  const float dy = __fsub_rn(c.sVy[o + nxp], c.sVy[o]);
+  const float dz = __fsub_rn(c.sVz[o + c.R * nxp], c.sVz[o]);
+  uint32_t open = 1u;
+  if (c.has_mask) open = (c.sM[r * S.mw + (x >> 3)] >> (4 * (x & 7))) & 1u;
+  const bool upd = x <= nx - 2;
+  int side = -1, l = 0;
+  if (S.flags & SF_PCPML) {
+    side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
+    l = side == 0 ? x : x - (nx - npml);
+  }
+  const bool xs = side >= 0 && upd;
+  const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
+  float mx = c.sXp[(sd * c.R + r) * S.npp + ll];
+  const float ax = side >= 0 ? c.co[sd * npml + ll] : 0.f;
+  const float bx = side >= 0 ? c.co[4 * npml + 2 + sd * npml + ll] : 0.f;
+  float my = 0.f, mz = 0.f;
+  c.pn_cur[o] = p_cell_slow<R>(P, __fsub_rn(X1, X0), dy, dz, g, upd, open, xs, mx, ax, bx, false,
+                               my, 0.f, 0.f, false, mz, 0.f, 0.f);
+  if (owned && xs) {
+    const int j = c.j0 - 1 + r;
+    S.psi_p[0][c.wb * S.psi_p_buf[0] + sd * S.psi_p_side[0] +
+               ((long long)c.pl * S.ny + j) * S.npp + ll] = mx;
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void v_xcell(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
+                                        int r, int x, float& vx, float& vy, float& vz) {
+  const int nxp = g.nxp, nx = S.nx, npml = S.npml, nm = npml + 1;
+  const int j = c.j0 - 1 + r;
+  const int o = r * nxp + x;
+  const float Pc = c.pn_cur[o];
+  const float Pxm = x > 0 ? c.pn_cur[o - 1] : 0.f;
+  const float Pym = c.pn_cur[o - nxp];
+  const float Pzm = c.pn_prev[o];
+  uint32_t nib = 0xFu;
+  if (c.has_mask) nib = (c.sM[r * S.mw + (x >> 3)] >> (4 * (x & 7))) & 0xFu;
+  const bool in = x < nx;
+  int side = -1, l = 0;
+  if (S.flags & SF_VCPML) {
+    side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
+    l = side == 0 ? x : x - (nx - npml - 1);
+  }
+  const bool updx = in && x >= 1;
+  const bool xs = side >= 0 && updx;
+  const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
+  float mx = c.sXv[(sd * c.R + r) * S.nvp + ll];
+  const float axe = side >= 0 ? c.co[2 * npml + sd * nm + ll] : 0.f;
+  const float bxe = side >= 0 ? c.co[6 * npml + 2 + sd * nm + ll] : 0.f;
+  vx = v_cell_slow<R>(c.sVx[o], __fsub_rn(Pc, Pxm), g.fv, g.rdx, updx, (nib >> 1) & 1u, xs, mx,
+                      axe, bxe);
+  float dm = 0.f;
+  vy = v_cell_slow<R>(c.sVy[o], __fsub_rn(Pc, Pym), g.fv, g.rdy, in && j >= 1, (nib >> 2) & 1u,
+                      false, dm, 0.f, 0.f);
+  vz = v_cell_slow<R>(c.sVz[o], __fsub_rn(Pc, Pzm), g.fv, g.rdz, in && c.pl >= 1,
+                      (nib >> 3) & 1u, false, dm, 0.f, 0.f);
+  if (xs)
+    S.psi_v[0][c.wb * S.psi_v_buf[0] + sd * S.psi_v_side[0] +
+               ((long long)c.pl * S.ny + j) * S.nvp + ll] = mx;
+}
+
 // ---- fast paths: every cell of the quad is an interior cell of its update
 // (no rigid plane, no CPML slab, no grid edge); branch-free 4-wide code.
 template <typename R>
@@ -516,25 +588,45 @@ __device__ __forceinline__ void store_outputs(const SolveDev& S, const PlaneCtx&
         make_float4(-vz.x, -vz.y, -vz.z, -vz.w));
 }
 
+__device__ __forceinline__ void store_cell(const SolveDev& S, const PlaneCtx& c, int r, int x,
+                                           float P, float vx, float vy, float vz) {
+  const int j = c.j0 - 1 + r;
+  const int pl = c.pl;
+  float* out = S.field + (long long)c.wb * S.buf_stride;
+  const long long cell = ((long long)pl * S.ny + j) * S.nxp + x;
+  out[cell] = P;
+  out[S.chan_stride + cell] = vx;
+  if (j != 0) out[2 * S.chan_stride + cell] = vy;
+  if (j == 1) out[2 * S.chan_stride + cell - S.nxp] = -vy;
+  if (pl != 0) out[3 * S.chan_stride + cell] = vz;
+  if (pl == 1) out[3 * S.chan_stride + cell - (long long)S.ny * S.nxp] = -vz;
+}
+
 // Work index -> (row, quad) for an ordinary tile-plane: u < na_pad are the
 // boundary quads of each row (the first nl and the last nr quads), padded to
 // whole warps; the interior quads follow.  Division by the per-row counts
 // uses a 32.32 reciprocal (exact for u, divisor < 2^16).
+// The boundary quads are split into their four cells, one cell per thread,
+// so that the longer boundary update is spread over several warps instead of
+// making one warp the critical path of the plane.
 struct XSplit {
   int nl, ni, nb, na, na_pad, total;
   unsigned long long mb, mi;
-  __device__ __forceinline__ bool map(int u, int& row, int& q) const {
+  // u -> (row, quad, cell); cell = -1 for an interior quad (all four cells)
+  __device__ __forceinline__ void map(int u, int& row, int& q, int& e) const {
     if (u < na_pad) {
-      if (u >= na) { row = -1; return true; }
+      if (u >= na) { row = -1; e = 0; return; }
       row = (int)(((unsigned long long)u * mb) >> 32);
-      const int k = u - row * nb;
-      q = k < nl ? k : k + ni;
-      return true;
+      const int k = u - row * 4 * nb;
+      const int kq = k >> 2;
+      q = kq < nl ? kq : kq + ni;
+      e = k & 3;
+      return;
     }
     const int v = u - na_pad;
     row = (int)(((unsigned long long)v * mi) >> 32);
     q = nl + v - row * ni;
-    return false;
+    e = -1;
   }
 };
 __device__ __forceinline__ XSplit make_split(int xmin, int xmax, int nq, int nrows) {
@@ -543,10 +635,10 @@ __device__ __forceinline__ XSplit make_split(int xmin, int xmax, int nq, int nro
   const int qhi = xmax >= 3 ? (xmax - 3) / 4 : -1;  // last quad with x0+3 <= xmax
   s.ni = max(0, min(qhi, nq - 1) - s.nl + 1);
   s.nb = nq - s.ni;
-  s.na = nrows * s.nb;
+  s.na = nrows * s.nb * 4;
   s.na_pad = (s.na + 31) / 32 * 32;
   s.total = s.na_pad + nrows * s.ni;
-  s.mb = s.nb ? ((1ull << 32) + s.nb - 1) / s.nb : 0;
+  s.mb = s.nb ? ((1ull << 32) + 4 * s.nb - 1) / (4 * s.nb) : 0;
   s.mi = s.ni ? ((1ull << 32) + s.ni - 1) / s.ni : 0;
   return s;
 }
@@ -649,9 +741,13 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
       };
       if (pl_plain && tileP) {
         for (int u = tid; u < sP.total; u += NCT) {
-          int row, q;
-          const bool bnd = sP.map(u, row, q);
-          if (row >= 0) p_work(rP0 + row, q, !bnd);
+          int row, q, e;
+          sP.map(u, row, q, e);
+          if (row < 0) continue;
+          if (e < 0)
+            p_work(rP0 + row, q, true);
+          else
+            p_xcell<R>(S, g, c, rP0 + row, 4 * q + e, !prologue && rP0 + row >= 1);
         }
       } else {
         for (int r = r_first, q = q_first; r <= ty; q += dq, r += dr) {
@@ -700,9 +796,23 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
       };
       if (pl_vplain && tileV) {
         for (int u = tid; u < sV.total; u += NCT) {
-          int row, q;
-          const bool bnd = sV.map(u, row, q);
-          if (row >= 0) v_work(1 + row, q, !bnd);
+          int row, q, e;
+          sV.map(u, row, q, e);
+          if (row < 0) continue;
+          if (e < 0) {
+            v_work(1 + row, q, true);
+          } else {
+            const int r = 1 + row, x = 4 * q + e, o = r * nxp + x;
+            float vx, vy, vz;
+            v_xcell<R>(S, g, c, r, x, vx, vy, vz);
+            if (has_f) {  // stage into this slot's own row cells (only this thread reads them)
+              const_cast<float*>(c.sVx)[o] = vx;
+              const_cast<float*>(c.sVy)[o] = vy;
+              const_cast<float*>(c.sVz)[o] = vz;
+            } else {
+              store_cell(S, c, r, x, c.pn_cur[o], vx, vy, vz);
+            }
+          }
         }
       } else {
         for (int r = 1 + r_first, q = q_first; r <= ty; q += dq, r += dr) {
@@ -740,7 +850,10 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
   return true;
 }
 
-__global__ void __launch_bounds__(NTHREADS, 2) adf_fdtd_step_kernel(const StepParams p) {
+// MINB = CTAs per SM the launch is sized for: 2 caps registers so two CTAs
+// fit, 1 gives the kernel the registers it needs without spilling.
+template <int MINB>
+__global__ void __launch_bounds__(NTHREADS, MINB) adf_fdtd_step_kernel(const StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
   uint64_t* empty = full + kMaxStages;
@@ -939,16 +1052,21 @@ cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-const void* step_kernel_ptr() { return (const void*)adf_fdtd_step_kernel; }
+const void* step_kernel_ptr(bool two_per_sm) {
+  return two_per_sm ? (const void*)adf_fdtd_step_kernel<2> : (const void*)adf_fdtd_step_kernel<1>;
+}
 
-cudaError_t step_kernel_attributes(size_t smem, bool) {
-  return cudaFuncSetAttribute(adf_fdtd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem);
+cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm) {
+  return cudaFuncSetAttribute(step_kernel_ptr(two_per_sm),
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
-                        bool) {
-  adf_fdtd_step_kernel<<<grid, block, smem, s>>>(p);
+                        bool two_per_sm) {
+  if (two_per_sm)
+    adf_fdtd_step_kernel<2><<<grid, block, smem, s>>>(p);
+  else
+    adf_fdtd_step_kernel<1><<<grid, block, smem, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -489,6 +489,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   const size_t fixed = 256 + (size_t)3 * pn_floats * 4;
   const size_t per_cta2 = (size_t)ctx->smem_per_sm / 2 - 1024;
   int stages = (int)((per_cta2 > fixed ? per_cta2 - fixed : 0) / ((size_t)stage_floats * 4));
+  two_per_sm = stages >= 2;
   if (stages < 2) {
     const size_t per_cta1 = std::min((size_t)ctx->smem_optin, (size_t)ctx->smem_per_sm - 1024);
     stages = (int)((per_cta1 - fixed) / ((size_t)stage_floats * 4));
@@ -496,15 +497,19 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   stages = std::min(std::max(stages, 2), 8);
   if (const char* env = std::getenv("ADF_STAGES")) {  // sweep override
     const int v = std::atoi(env);
-    if (v >= 2 && v <= 8) stages = v;
+    if (v >= 2 && v <= 8) {
+      stages = v;
+      two_per_sm = fixed + (size_t)v * stage_floats * 4 <= per_cta2;
+    }
   }
   this->stages = stages;
   smem = fixed + (size_t)stages * stage_floats * 4;
   if (smem > (size_t)ctx->smem_optin) return fail(ADF_E_ARG, "grid too wide for shared memory");
-  if (cudaError_t ea = step_kernel_attributes(smem, false); ea != cudaSuccess)
+  if (cudaError_t ea = step_kernel_attributes(smem, two_per_sm); ea != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(ea));
   int bps = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, step_kernel_ptr(), consumer_threads() + 32,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, step_kernel_ptr(two_per_sm),
+                                                consumer_threads() + 32,
                                                 smem);
   if (bps < 1) bps = 1;
   grid = std::min(n_items, ctx->nsm * bps);
@@ -537,7 +542,8 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
       cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (timed && cudaEventRecordWithFlags(ctx->kev[2 * step], ctx->stream, evf) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("event record: ") + cudaGetErrorString(cudaGetLastError()));
-  cudaError_t e = adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, false);
+  cudaError_t e =
+      adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, two_per_sm);
   if (e != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("step launch failed: ") + cudaGetErrorString(e) +
                                   " (grid " + std::to_string(grid) + ", smem " +

@@ -88,6 +88,7 @@ struct Batch {
   int* d_err = nullptr;
   int cap_solves = 0, cap_items = 0;
   int n_items = 0, stages = 3, stage_floats = 0, pn_floats = 0, grid = 1, max_ntx = 0;
+  bool two_per_sm = false;  // ring sized so two CTAs share an SM
   size_t smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;
@@ -122,6 +123,6 @@ int pack_transceivers_host(const hm::Dom& d, const double* points, const double*
 
 // kernels (fdtd_kernels.cu)
 cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s);
-const void* step_kernel_ptr();
+const void* step_kernel_ptr(bool two_per_sm);
 
 }  // namespace adf

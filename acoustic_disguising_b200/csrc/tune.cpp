@@ -52,7 +52,7 @@ static void load_locked() {
 
 static Tune default_tune(int nx, int ny, int nz) {
   Tune t;
-  t.ty = nx > 256 ? 2 : 4;
+  t.ty = nx > 256 ? 2 : 3;  // 3 rows keep two CTAs per SM up to nx = 256
   t.nzc = nz >= 256 ? 32 : 16;
   (void)ny;
   return t;
