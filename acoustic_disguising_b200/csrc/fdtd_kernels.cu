@@ -35,7 +35,10 @@
 
 namespace adf {
 
-constexpr int NCT = 256;          // consumer threads
+#ifndef ADF_NCT
+#define ADF_NCT 256
+#endif
+constexpr int NCT = ADF_NCT;      // consumer threads
 constexpr int NCW = NCT / 32;     // consumer warps
 constexpr int NTHREADS = NCT + 32;
 constexpr int kMaxStages = 8;
@@ -602,31 +605,35 @@ __device__ __forceinline__ void store_cell(const SolveDev& S, const PlaneCtx& c,
   if (pl == 1) out[3 * S.chan_stride + cell - (long long)S.ny * S.nxp] = -vz;
 }
 
-// Work index -> (row, quad) for an ordinary tile-plane: u < na_pad are the
-// boundary quads of each row (the first nl and the last nr quads), padded to
-// whole warps; the interior quads follow.  Division by the per-row counts
-// uses a 32.32 reciprocal (exact for u, divisor < 2^16).
-// The boundary quads are split into their four cells, one cell per thread,
-// so that the longer boundary update is spread over several warps instead of
-// making one warp the critical path of the plane.
+// Work index -> (row, quad, cell) for an ordinary tile-plane.  Boundary quads
+// (the first nl and the last nb-nl quads of a row) are split into their four
+// cells, one cell per thread, so that the longer boundary update is spread
+// over several warps instead of making one warp the critical path of the
+// plane.  Work units: the interior quads of every row, then the boundary
+// cells.  Division by the per-row counts uses a 32.32 reciprocal (exact for
+// u, divisor < 2^16).
 struct XSplit {
   int nl, ni, nb, na, na_pad, total;
   unsigned long long mb, mi;
-  // u -> (row, quad, cell); cell = -1 for an interior quad (all four cells)
+  // u -> (row, quad, cell); cell = -1 for an interior quad (all four cells).
+  // Interior quads come first, so the threads whose unit is a boundary cell
+  // are the ones without a second unit in phases with more units than
+  // threads.
   __device__ __forceinline__ void map(int u, int& row, int& q, int& e) const {
-    if (u < na_pad) {
-      if (u >= na) { row = -1; e = 0; return; }
-      row = (int)(((unsigned long long)u * mb) >> 32);
-      const int k = u - row * 4 * nb;
-      const int kq = k >> 2;
-      q = kq < nl ? kq : kq + ni;
-      e = k & 3;
+    const int nint = total - na_pad;
+    if (u < nint) {
+      row = (int)(((unsigned long long)u * mi) >> 32);
+      q = nl + u - row * ni;
+      e = -1;
       return;
     }
-    const int v = u - na_pad;
-    row = (int)(((unsigned long long)v * mi) >> 32);
-    q = nl + v - row * ni;
-    e = -1;
+    u -= nint;
+    if (u >= na) { row = -1; e = 0; return; }
+    row = (int)(((unsigned long long)u * mb) >> 32);
+    const int k = u - row * 4 * nb;
+    const int kq = k >> 2;
+    q = kq < nl ? kq : kq + ni;
+    e = k & 3;
   }
 };
 __device__ __forceinline__ XSplit make_split(int xmin, int xmax, int nq, int nrows) {
