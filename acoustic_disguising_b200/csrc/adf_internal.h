@@ -21,6 +21,7 @@ enum : int {
   SF_PCPML = 2,     // p-side CPML active (npml>1, or npml>=1 with a mask)
   SF_VCPML = 4,     // v-side CPML active (npml>=1)
   SF_FP32 = 8,      // Float32 arithmetic instead of Float64 intermediates
+  SF_YZG = 16,      // y/z-slab CPML memory read from global memory, not staged
 };
 
 struct SolveDev {
@@ -97,7 +98,11 @@ struct SlotLayout {
   int reg, reg2, regm, regxp, regxv, regyz_p, regyz_v, total;
   int off_vz, off_m, off_xp, off_xv, off_py, off_vy, off_pz, off_vz2;
 };
-inline __host__ __device__ SlotLayout slot_layout(int ty, int nxp, int mw, int npp, int nvp) {
+// stage_yz = false leaves the y/z-slab boxes out (the kernel then reads that
+// CPML memory from global memory on slab planes), which makes room for
+// taller tiles.
+inline __host__ __device__ SlotLayout slot_layout(int ty, int nxp, int mw, int npp, int nvp,
+                                                  bool stage_yz) {
   SlotLayout L;
   const long long R = ty + 2;
   L.reg = round32(R * nxp);
@@ -105,8 +110,8 @@ inline __host__ __device__ SlotLayout slot_layout(int ty, int nxp, int mw, int n
   L.regm = round32(R * mw);
   L.regxp = round32(2 * R * npp);
   L.regxv = round32(2 * R * nvp);
-  L.regyz_p = npp ? L.reg : 0;
-  L.regyz_v = nvp ? L.reg : 0;
+  L.regyz_p = (npp && stage_yz) ? L.reg : 0;
+  L.regyz_v = (nvp && stage_yz) ? L.reg : 0;
   L.off_vz = 3 * L.reg;
   L.off_m = L.off_vz + L.reg2;
   L.off_xp = L.off_m + L.regm;

@@ -232,7 +232,8 @@ __device__ __forceinline__ void p_quad(const SolveDev& S, const Regs<R>& g, cons
   }
   if (zsd >= 0) {
     oz = (long long)zsd * S.psi_p_side[2] + ((long long)zl * ny + j) * nxp + x0;
-    mz = ld4(c.zP + r * nxp + x0);
+    mz = (S.flags & SF_YZG) ? ldg4(S.psi_p[2] + c.rb * S.psi_p_buf[2] + oz)
+                            : ld4(c.zP + r * nxp + x0);
     az = co[zsd * npml + zl];
     bz = co[4 * npml + 2 + zsd * npml + zl];
   }
@@ -347,7 +348,8 @@ __device__ __forceinline__ void v_quad(const SolveDev& S, const Regs<R>& g, cons
   }
   if (zsd >= 0) {
     oz = (long long)zsd * S.psi_v_side[2] + ((long long)zl * ny + j) * nxp + x0;
-    mz = ld4(c.zV + r * nxp + x0);
+    mz = (S.flags & SF_YZG) ? ldg4(S.psi_v[2] + c.rb * S.psi_v_buf[2] + oz)
+                            : ld4(c.zV + r * nxp + x0);
     az = co[2 * npml + zsd * nm + zl];
     bz = co[6 * npml + 2 + zsd * nm + zl];
   }
@@ -662,7 +664,7 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
   const bool has_mask = (S.flags & SF_MASK) != 0;
   const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
   const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
-                                   vcpml ? S.nvp : 0);
+                                   vcpml ? S.nvp : 0, !(S.flags & SF_YZG));
   const int pz0 = item.z > 0 ? item.z - 1 : 0;
   const int tid = threadIdx.x;
   Regs<R> g;
@@ -723,8 +725,8 @@ __device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, 
     c.zP = base + L.off_pz;
     c.zV = base + L.off_vz2;
     c.co = s_co;
-    c.ysP = pcpml ? tile_yside(j0, ty, ny, npml) : -1;
-    c.ysV = vcpml ? tile_yside(j0, ty, ny, npml + 1) : -1;
+    c.ysP = (pcpml && !(S.flags & SF_YZG)) ? tile_yside(j0, ty, ny, npml) : -1;
+    c.ysV = (vcpml && !(S.flags & SF_YZG)) ? tile_yside(j0, ty, ny, npml + 1) : -1;
     c.pn_cur = pn + (n % kPnBufs) * p.pn_floats;
     c.pn_prev = pn + ((n + kPnBufs - 1) % kPnBufs) * p.pn_floats;
     c.j0 = j0;
@@ -902,15 +904,16 @@ __global__ void __launch_bounds__(NTHREADS, MINB) adf_fdtd_step_kernel(const Ste
       const int j0 = item.y * ty;
       const bool has_mask = (S.flags & SF_MASK) != 0;
       const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
+      const bool stage_yz = !(S.flags & SF_YZG);
       const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
-                                       vcpml ? S.nvp : 0);
+                                       vcpml ? S.nvp : 0, stage_yz);
       const uint32_t bytes0 =
           (uint32_t)(5 * Rr * nxp * 4 + (has_mask ? Rr * S.mw * 4 : 0) +
                      (pcpml ? 2 * Rr * S.npp * 4 : 0) + (vcpml ? 2 * Rr * S.nvp * 4 : 0));
       const uint32_t box_bytes = (uint32_t)(Rr * nxp * 4);
       const int ny = S.ny, nz = S.nz, npml = S.npml;
-      const int ysP = pcpml ? tile_yside(j0, ty, ny, npml) : -1;
-      const int ysV = vcpml ? tile_yside(j0, ty, ny, npml + 1) : -1;
+      const int ysP = (pcpml && stage_yz) ? tile_yside(j0, ty, ny, npml) : -1;
+      const int ysV = (vcpml && stage_yz) ? tile_yside(j0, ty, ny, npml + 1) : -1;
       const int pz0 = item.z > 0 ? item.z - 1 : 0;
       bool ok = true;
       for (int pl = pz0; pl < item.w; ++pl, ++n) {
@@ -946,7 +949,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) adf_fdtd_step_kernel(const Ste
           tma_load_5d(smem_u32(base + L.off_vy), tm + 6, mb, 0, 0, l0, pl, 2 * rb + ysV);
           bytes += box_bytes;
         }
-        if (pcpml) {
+        if (pcpml && stage_yz) {
           const int zs = plane_zside(pl, nz, npml);
           if (zs >= 0) {
             const int l = zs == 0 ? pl : pl - (nz - npml);
@@ -954,7 +957,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) adf_fdtd_step_kernel(const Ste
             bytes += box_bytes;
           }
         }
-        if (vcpml) {
+        if (vcpml && stage_yz) {
           const int zs = plane_zside(pl, nz, npml + 1);
           if (zs >= 0) {
             const int l = zs == 0 ? pl : pl - (nz - npml - 1);

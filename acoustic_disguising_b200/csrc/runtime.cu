@@ -315,6 +315,12 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   d.ntx = ntx;
   d.flags = (has_mask ? SF_MASK : 0) | ((npml > 1 || (has_mask && npml >= 1)) ? SF_PCPML : 0) |
             (npml >= 1 ? SF_VCPML : 0) | (arith == ADF_ARITH_FP32 ? SF_FP32 : 0);
+  // tiles taller than 8 rows only fit the ring without the y/z-slab boxes
+  if (d.ty > 8) d.flags |= SF_YZG;
+  if (const char* env = std::getenv("ADF_YZG")) {  // sweep override
+    if (std::atoi(env) == 1) d.flags |= SF_YZG;
+    else if (d.ty <= 8) d.flags &= ~SF_YZG;
+  }
   d.fq = dom.fact_m0;
   d.fv = dom.fact_m1;
   d.rdx = 1.0 / dom.dx;
@@ -440,7 +446,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
     const SolveDev& d = list[i]->dev;
     const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
                                      (d.flags & SF_PCPML) ? d.npp : 0,
-                                     (d.flags & SF_VCPML) ? d.nvp : 0);
+                                     (d.flags & SF_VCPML) ? d.nvp : 0, !(d.flags & SF_YZG));
     max_stage = std::max(max_stage, L.total);
     max_pn = std::max(max_pn, pn_plane_floats(d.ty, d.nxp));
     max_ntx = std::max(max_ntx, d.ntx);
@@ -485,8 +491,11 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaStreamSynchronize(st);
   stage_floats = max_stage;
   pn_floats = max_pn;
-  // pipeline depth: as many slots as fit two CTAs per SM, else one CTA
-  const size_t fixed = 256 + (size_t)3 * pn_floats * 4;
+  // pipeline depth: as many slots as fit two CTAs per SM, else one CTA.
+  // The kernel's static shared memory counts against the same budget.
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, step_kernel_ptr(false));
+  const size_t fixed = 256 + (size_t)3 * pn_floats * 4 + fa.sharedSizeBytes;
   const size_t per_cta2 = (size_t)ctx->smem_per_sm / 2 - 1024;
   int stages = (int)((per_cta2 > fixed ? per_cta2 - fixed : 0) / ((size_t)stage_floats * 4));
   two_per_sm = stages >= 2;
@@ -503,8 +512,9 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
     }
   }
   this->stages = stages;
-  smem = fixed + (size_t)stages * stage_floats * 4;
-  if (smem > (size_t)ctx->smem_optin) return fail(ADF_E_ARG, "grid too wide for shared memory");
+  smem = fixed - fa.sharedSizeBytes + (size_t)stages * stage_floats * 4;  // dynamic part
+  if (smem + fa.sharedSizeBytes > (size_t)ctx->smem_optin)
+    return fail(ADF_E_ARG, "grid too wide for shared memory");
   if (cudaError_t ea = step_kernel_attributes(smem, two_per_sm); ea != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(ea));
   int bps = 0;

@@ -52,8 +52,12 @@ static void load_locked() {
 
 static Tune default_tune(int nx, int ny, int nz) {
   Tune t;
-  t.ty = nx > 256 ? 2 : 3;  // 3 rows keep two CTAs per SM up to nx = 256
-  t.nzc = nz >= 256 ? 32 : 16;
+  // Large grids: 8-row tiles (one CTA per SM, more work per thread and less
+  // halo recomputation) still give every SM several items per solve.  Small
+  // grids keep 3-row tiles so that a single solve fills the GPU.  Rows wider
+  // than 256 cells take two x boxes and 2-row tiles.
+  t.ty = nx > 256 ? 2 : ((ny >= 224 && nz >= 224) ? 8 : 3);
+  t.nzc = 16;
   (void)ny;
   return t;
 }
