@@ -10,7 +10,7 @@ from .api import (  # noqa: F401
     split_profiles, Cpml, shape_params,
     build_update_mask, Transceiver, TransceiverGrid, transceivers_to_grid, p_src, p_rec, vn_src,
     vn_rec, run_fdtd, injection_coefficients, kh_pressure, fp32_fma_peak, GfRequest,
-    gf_solve_batch, Server,
+    gf_solve_batch, autotune, Server,
 )
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -115,6 +115,9 @@ SIGNATURES = [
     ("adf_kernel_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                     C.c_int]),
     ("adf_gf_solve_batch", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(GfRequestC), C.c_int]),
+    ("adf_autotune", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int,
+                               C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               C.POINTER(C.c_double)]),
     ("adf_server_start", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
     ("adf_server_submit", C.c_int, [C.c_void_p, C.POINTER(GfRequestC), C.POINTER(C.c_int64)]),
     ("adf_server_poll", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int),

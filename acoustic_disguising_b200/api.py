@@ -497,6 +497,17 @@ def gf_solve_batch(reqs, batched: bool = True, ctx: Context | None = None):
     return ctx.last_timing()
 
 
+def autotune(nx: int, ny: int, nz: int, npml: int = 10, n_solves: int = 4, steps: int = 32,
+             ctx: Context | None = None):
+    """Times the step kernel's tile shapes on synthetic GF solves of this grid
+    size and stores the fastest in the tune table; returns (ty, nzc, ms)."""
+    ctx = ctx or default_context()
+    ty, nzc, ms = C.c_int(), C.c_int(), C.c_double()
+    L.check(L.lib().adf_autotune(ctx.h, nx, ny, nz, npml, n_solves, steps, C.byref(ty),
+                                 C.byref(nzc), C.byref(ms)), "autotune")
+    return ty.value, nzc.value, ms.value
+
+
 class Server:
     """Continuous-batching serving loop (adf_server_*)."""
 

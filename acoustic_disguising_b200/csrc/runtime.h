@@ -58,6 +58,7 @@ struct Tune {
 };
 Tune tune_lookup(int nx, int ny, int nz);
 int tune_store(int nx, int ny, int nz, Tune t);
+void tune_force(Tune t);  // {0,0} releases
 
 struct Solve {
   SolveDev dev;

@@ -210,6 +210,15 @@ typedef struct {
  * one solve at a time, one launch per step.                               */
 int adf_gf_solve_batch(adf_ctx* ctx, int64_t n, adf_gf_request* reqs, int batched);
 
+/* Autotuner of the fused step kernel's tile shape for one grid size; no
+ * counterpart in the reference.  Times n_solves synthetic GF solves of
+ * `steps` steps (CPML npml, centred rigid sphere, point source, receiver
+ * shell) for each candidate (tile rows, z-chunk depth), keeps the fastest
+ * in the tune table next to the library (or $ADF_TUNE_TABLE) that later
+ * solves of this size use, and returns it with its mean step-kernel time.  */
+int adf_autotune(adf_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, int64_t npml, int n_solves,
+                 int steps, int* best_ty, int* best_nzc, double* best_ms);
+
 /* ---- Serving loop: continuous batching of GF solves ----------------------
  * A host thread owns the device work: requests submitted while others are
  * on the GPU are admitted as slots and HBM budget free up, and all resident

@@ -168,9 +168,22 @@ def test_reciprocity_gpu(adf, oracle, ctx):
     (36, 33, 34, 1, "none"),       # npml=1: p-side CPML off without a mask
     (36, 33, 34, 1, "sphere"),     # npml=1 with a mask: p-side CPML on (no guard)
     (40, 40, 40, 0, "cube"),       # masked, no CPML
+    (300, 20, 18, 6, "sphere"),    # rows wider than 256 cells: two x boxes per row
 ])
 def test_run_fdtd_parity(adf, oracle, ctx, nx, ny, nz, npml, shape):
     case = make_case(adf, oracle, nx, ny, nz, steps=60, npml=npml, shape=shape, seed=nx + npml)
+    gpu, cpu = run_both(adf, oracle, case)
+    errs = assert_parity(gpu, cpu, 1e-6)
+    assert errs["rec0"] <= 1e-5
+
+
+@pytest.mark.parametrize("tile", ["8,16", "12,16", "2,8", "5,32"])
+def test_tile_shapes(adf, oracle, ctx, monkeypatch, tile):
+    """Every tile height / z-chunk depth gives the same result: 8-row tiles
+    (the large-grid default), 12-row tiles (y/z CPML memory read from global
+    memory instead of staged), 2-row tiles with short z chunks."""
+    monkeypatch.setenv("ADF_TILE", tile)
+    case = make_case(adf, oracle, 48, 44, 40, steps=50, npml=6, shape="sphere", seed=17)
     gpu, cpu = run_both(adf, oracle, case)
     errs = assert_parity(gpu, cpu, 1e-6)
     assert errs["rec0"] <= 1e-5

@@ -140,3 +140,14 @@ def test_kernel_timing_in_graphs(adf, ctx):
     ms, n = ctx.kernel_timing(reset=True)
     ctx.set_kernel_timing(False)
     assert n == 70 and ms > 0
+
+
+@pytest.mark.gpu
+def test_autotune_stores_a_shape_that_later_solves_use(adf, ctx, tmp_path, monkeypatch):
+    table = tmp_path / "tune_table.json"
+    monkeypatch.setenv("ADF_TUNE_TABLE", str(table))
+    monkeypatch.delenv("ADF_TILE", raising=False)
+    ty, nzc, ms = adf.autotune(72, 64, 60, npml=6, n_solves=2, steps=12, ctx=ctx)
+    assert ty in (2, 3, 4, 6, 8) and nzc in (8, 16, 32) and ms > 0
+    txt = table.read_text()
+    assert f'"72,64,60": [{ty}, {nzc}]' in txt
