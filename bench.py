@@ -416,6 +416,26 @@ def serving_section(A, ctx, n_req):
     }
 
 # ---------------------------------------------------------------------------
+# multi-rank plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+def rank_first_source(step_ix, world, rank, batch):
+    """First source index of this rank's batch in bench step `step_ix`: the
+    ranks take disjoint, consecutive blocks of `batch` sources (weak scaling)."""
+    return (step_ix * world + rank) * batch
+
+
+def reduce_max(x, dist=None, device=None):
+    """Maximum of x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 def b200_arm(args):
@@ -442,21 +462,12 @@ def b200_arm(args):
         if dist is not None:
             dist.barrier()
 
-    def reduce_max(x):
-        if dist is None:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     B = args.batch
     step_ix = 0
 
     def one_step():
         nonlocal step_ix
-        first = (step_ix * world + rank) * B
+        first = rank_first_source(step_ix, world, rank, B)
         step_ix += 1
         _, reqs = make_requests(A, first, B, args.arith, args.nt)
         t0 = time.perf_counter()
@@ -491,9 +502,9 @@ def b200_arm(args):
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
     if world == 1 and not args.no_serving:
         extra["serving"] = serving_section(A, ctx, args.serving_requests)
-    dev_total = reduce_max(sum(devs))
-    wall_total = reduce_max(sum(walls))
-    k_avg_ms = reduce_max(k_ms / max(k_n, 1))
+    dev_total = reduce_max(sum(devs), dist, f"cuda:{local}")
+    wall_total = reduce_max(sum(walls), dist, f"cuda:{local}")
+    k_avg_ms = reduce_max(k_ms / max(k_n, 1), dist, f"cuda:{local}")
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
