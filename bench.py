@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--no-kh", action="store_true", help="skip the KH section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--serving-requests", type=int, default=20)
+    ap.add_argument("--kh-only", action="store_true",
+                    help="run only the KH section and print it (profiling runs)")
     return ap.parse_args()
 
 
@@ -559,10 +561,23 @@ def b200_arm(args):
     return 0
 
 
+def kh_only(args):
+    import acoustic_disguising_b200 as A
+
+    if not os.path.exists(A.LIB_PATH):
+        A.build()
+    ctx = A.Context(0)
+    print(json.dumps({"kh": kh_section(A, ctx, steps=args.steps, warmup=args.warmup)}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.kh_only:
+        return kh_only(args)
     return b200_arm(args)
 
 
