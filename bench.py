@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--no-kh", action="store_true", help="skip the KH section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--serving-requests", type=int, default=20)
+    ap.add_argument("--serving-resident", type=int, default=2,
+                    help="server slot limit (0: HBM budget only)")
     ap.add_argument("--kh-only", action="store_true",
                     help="run only the KH section and print it (profiling runs)")
     return ap.parse_args()
@@ -359,7 +361,7 @@ def serving_requests(A, n_req, seed):
     return out
 
 
-def serving_section(A, ctx, n_req):
+def serving_section(A, ctx, n_req, max_resident=0):
     seed = 20261203
     # plain path: one solve at a time, service time per request
     service = []
@@ -379,7 +381,7 @@ def serving_section(A, ctx, n_req):
     plain_sps = n_req / (fin[-1] - arr[0])
     # batched: the continuous-batching server fed the same arrivals in real time
     reqs = serving_requests(A, n_req, seed)
-    srv = A.Server(hbm_budget=SERVE_BUDGET, ctx=ctx)
+    srv = A.Server(hbm_budget=SERVE_BUDGET, max_resident=max_resident, ctx=ctx)
     ids = []
     t0 = time.perf_counter()
     for a, r in zip(arr, reqs):
@@ -415,6 +417,7 @@ def serving_section(A, ctx, n_req):
                   "note": "one solve per launch sequence; latencies from its measured "
                           "per-request service times queued FIFO on the same arrivals"},
         "speedup_solves_per_s": b_sps / plain_sps, "arrival_rate_per_s": lam,
+        "max_resident": max_resident or "unlimited (HBM budget only)",
     }
 
 # ---------------------------------------------------------------------------
@@ -503,7 +506,8 @@ def b200_arm(args):
     if world == 1 and not args.no_kh:
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
     if world == 1 and not args.no_serving:
-        extra["serving"] = serving_section(A, ctx, args.serving_requests)
+        extra["serving"] = serving_section(A, ctx, args.serving_requests,
+                                           args.serving_resident)
     dev_total = reduce_max(sum(devs), dist, f"cuda:{local}")
     wall_total = reduce_max(sum(walls), dist, f"cuda:{local}")
     k_avg_ms = reduce_max(k_ms / max(k_n, 1), dist, f"cuda:{local}")
