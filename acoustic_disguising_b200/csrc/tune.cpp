@@ -55,8 +55,8 @@ static Tune default_tune(int nx, int ny, int nz) {
   // Large grids: 8-row tiles (one CTA per SM, more work per thread and less
   // halo recomputation) still give every SM several items per solve.  Small
   // grids keep 3-row tiles so that a single solve fills the GPU.  Rows wider
-  // than 256 cells take two x boxes and 2-row tiles.
-  t.ty = nx > 256 ? 2 : ((ny >= 224 && nz >= 224) ? 8 : 3);
+  // than 256 cells take two x boxes and 3-row tiles (autotuned at 512^3).
+  t.ty = nx > 256 ? 3 : ((ny >= 224 && nz >= 224) ? 8 : 3);
   t.nzc = 16;
   (void)ny;
   return t;

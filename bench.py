@@ -83,6 +83,7 @@ def parse():
                     help="steps per solve (profiling runs only; the metric uses 2000)")
     ap.add_argument("--no-kh", action="store_true", help="skip the KH section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--no-step512", action="store_true", help="skip the 512^3 step section")
     ap.add_argument("--serving-requests", type=int, default=20)
     ap.add_argument("--serving-resident", type=int, default=2,
                     help="server slot limit (0: HBM budget only)")
@@ -176,10 +177,10 @@ def make_requests(A, first_source, batch, arith, nt=NT):
     return d, reqs
 
 
-def algorithmic_bytes_per_solve_step():
-    cells = N ** 3
+def algorithmic_bytes_per_solve_step(n=N, npml=NPML):
+    cells = n ** 3
     field = 32.0 * cells + 0.5 * cells  # 4 fields read + written, 4-bit mask
-    psi = 8.0 * 6 * NPML * N * N + 8.0 * 6 * (NPML + 1) * N * N  # p- and v-side slabs, r+w
+    psi = 8.0 * 6 * npml * n * n + 8.0 * 6 * (npml + 1) * n * n  # p- and v-side slabs, r+w
     return field + psi
 
 
@@ -421,6 +422,43 @@ def serving_section(A, ctx, n_req, max_resident=0):
     }
 
 # ---------------------------------------------------------------------------
+# The 512^3 step: 12-cell CPML, rigid ellipsoid (semi-axes 80/60/40 cells)
+# ---------------------------------------------------------------------------
+def step512_section(A, ctx, nt=48, tune=True):
+    n, npml = 512, 12
+    d = A.Domain(tmax=tmax_of(nt), xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
+    tf, _ = A.impulsive_wavelet(d, F3DB)
+    rp, rn = A.fibonacci_sphere(256, 130 * DX)
+    req = A.GfRequest(d, [100 * DX, 0.0, 0.0], [1.0, 0.0, 0.0, 0.0], tf, rp, rn, npml=npml,
+                      pml_rcoef=1e-4, pml_fc=PML_FC, scatterer="ellipsoid",
+                      scatterer_kw=dict(semi_axes=(80 * DX, 60 * DX, 40 * DX)))
+    tuned = None
+    if tune:
+        tuned = A.autotune(n, n, n, npml=npml, n_solves=1, steps=16, ctx=ctx)
+    ctx.set_kernel_timing(True)
+    ctx.kernel_timing(reset=True)
+    A.gf_solve_batch([req], batched=True, ctx=ctx)
+    k_ms, k_n = ctx.kernel_timing(reset=True)
+    ctx.set_kernel_timing(False)
+    per = k_ms / max(k_n, 1)
+    byt = algorithmic_bytes_per_solve_step(n, npml)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs") or 6650.0
+    gbs = byt / (per / 1e3) / 1e9
+    return {"workload": "one 512^3 solve (dx=5 mm air), 12-cell CPML, rigid ellipsoid 80/60/40 "
+                        f"cells, point source, 256-point shell, {nt} steps",
+            "mean_launch_ms": per, "launches": k_n, "gcell_upd_per_s": n ** 3 / (per / 1e3) / 1e9,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak, "frac_of_nominal_8000": gbs / 8000.0,
+                         "bytes_per_launch": byt},
+            "tile": {"ty": tuned[0], "nzc": tuned[1]} if tuned else "table/default"}
+
+
+# ---------------------------------------------------------------------------
 # multi-rank plumbing (one process per GPU)
 # ---------------------------------------------------------------------------
 def rank_first_source(step_ix, world, rank, batch):
@@ -505,6 +543,8 @@ def b200_arm(args):
     extra = {}
     if world == 1 and not args.no_kh:
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
+    if world == 1 and not args.no_step512:
+        extra["step512"] = step512_section(A, ctx)
     if world == 1 and not args.no_serving:
         extra["serving"] = serving_section(A, ctx, args.serving_requests,
                                            args.serving_resident)
