@@ -84,6 +84,12 @@ class KhDescC(C.Structure):
     ]
 
 
+class GfMapC(C.Structure):
+    _fields_ = [("nt_gf", C.c_int64), ("nsrc", C.c_int64), ("nrec", C.c_int64),
+                ("p_pin", C.c_void_p), ("v_pin", C.c_void_p), ("i_src", C.c_void_p),
+                ("i_rec", C.c_void_p), ("z0", C.c_double), ("discard", C.c_int)]
+
+
 STEP_CB = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_void_p)
 
 # (name, restype, argtypes) for every entry point of include/adfdtd.h
@@ -108,6 +114,9 @@ SIGNATURES = [
     ("adf_run_fdtd", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_void_p, C.POINTER(TxGridC),
                                C.POINTER(CpmlC), C.c_void_p, C.c_int64, C.c_int64, C.c_int,
                                STEP_CB, C.c_void_p]),
+    ("adf_run_fdtd_gf", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_void_p,
+                                  C.POINTER(TxGridC), C.POINTER(CpmlC), C.c_void_p, C.c_int64,
+                                  C.c_int64, C.c_int, C.POINTER(GfMapC), STEP_CB, C.c_void_p]),
     ("adf_read_field", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("adf_last_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("adf_set_kernel_timing", C.c_int, [C.c_void_p, C.c_int]),

@@ -344,12 +344,42 @@ def vn_rec(g: TransceiverGrid):
 # ---------------------------------------------------------------------------
 # Time stepping (src/simulation.jl:542-557)
 # ---------------------------------------------------------------------------
+@dataclass
+class PVFromPin:
+    """PVFromPin GF map (src/kernels/extrapolation.jl:72-87): p_pin, v_pin
+    (nt_gf, nsrc, nrec) float32, iSrc/iRec 1-based transceiver indices.
+    discard=True reproduces the reference as shipped, whose extrapolate!
+    writes into slice copies so the sources never change."""
+
+    p_pin: np.ndarray
+    v_pin: np.ndarray
+    i_src: np.ndarray
+    i_rec: np.ndarray
+    discard: bool = False
+
+    def _c(self, z0: float):
+        self._pp = np.asfortranarray(self.p_pin, np.float32)
+        self._vp = np.asfortranarray(self.v_pin, np.float32)
+        self._is = np.ascontiguousarray(self.i_src, np.int64)
+        self._ir = np.ascontiguousarray(self.i_rec, np.int64)
+        if self._pp.shape != self._vp.shape or self._pp.ndim != 3:
+            raise ValueError("p_pin and v_pin must both be (nt_gf, nsrc, nrec)")
+        if self._is.size != self._pp.shape[1] or self._ir.size != self._pp.shape[2]:
+            raise ValueError("iSrc / iRec lengths must match the GF tensors")
+        return L.GfMapC(nt_gf=self._pp.shape[0], nsrc=self._pp.shape[1], nrec=self._pp.shape[2],
+                        p_pin=self._pp.ctypes.data, v_pin=self._vp.ctypes.data,
+                        i_src=self._is.ctypes.data, i_rec=self._ir.ctypes.data, z0=float(z0),
+                        discard=int(bool(self.discard)))
+
+
 def run_fdtd(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | None, va=None,
              start_step: int = 1, on_step=None, stop_step: int | None = None,
-             arith: str = "promote", ctx: Context | None = None) -> np.ndarray:
-    """run_fdtd!(dom, field, txs, cpml, va; start_step, on_step): advances
-    `field` (and the trace buffers and CPML memory) in place on the GPU.
-    on_step(it, read) is called after each step; read(c) returns channel c."""
+             arith: str = "promote", ctx: Context | None = None,
+             gf_map: PVFromPin | None = None) -> np.ndarray:
+    """run_fdtd!(dom, field, txs, cpml, va; start_step, on_step, gf_map):
+    advances `field` (and the trace buffers and CPML memory) in place on the
+    GPU.  on_step(it, read) is called after each step; read(c) returns
+    channel c.  gf_map drives the in-loop GF extrapolation."""
     ctx = ctx or default_context()
     stop_step = int(d.nt) if stop_step is None else int(stop_step)
     if field.dtype != np.float32 or not field.flags.f_contiguous:
@@ -374,6 +404,13 @@ def run_fdtd(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | 
                 return 1
             return 1 if r is False else 0
         cb = L.STEP_CB(_cb)
+    if gf_map is not None:
+        gm = gf_map._c(d.z0)
+        L.check(L.lib().adf_run_fdtd_gf(ctx.h, C.byref(d), _p(field), C.byref(cg),
+                                        C.byref(cc) if cc is not None else None, _p(mask),
+                                        int(start_step), stop_step, L.ARITH[arith],
+                                        C.byref(gm), cb, None), "run_fdtd_gf")
+        return field
     L.check(L.lib().adf_run_fdtd(ctx.h, C.byref(d), _p(field), C.byref(cg),
                                  C.byref(cc) if cc is not None else None, _p(mask),
                                  int(start_step), stop_step, L.ARITH[arith], cb, None),

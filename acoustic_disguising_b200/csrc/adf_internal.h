@@ -22,6 +22,7 @@ enum : int {
   SF_VCPML = 4,     // v-side CPML active (npml>=1)
   SF_FP32 = 8,      // Float32 arithmetic instead of Float64 intermediates
   SF_YZG = 16,      // y/z-slab CPML memory read from global memory, not staged
+  SF_GF = 32,       // in-loop GF extrapolation between v2vn and vn2v
 };
 
 struct SolveDev {
@@ -60,6 +61,15 @@ struct SolveDev {
   const float* dir;       // [ntx][4]
   int* err;               // per-solve error word
   int pad_;
+  // in-loop GF extrapolation (PVFromPin), SF_GF only
+  const float* gf_pp;     // (nt_gf, nsrc, nrec) column-major
+  const float* gf_vp;
+  const int* gf_isrc;     // [nsrc] 0-based transceiver column
+  const int* gf_irec;     // [nrec]
+  double* gf_pin;         // [nrec][nt] (p_rec - z0 vn_rec)/2 of recorded rows
+  double gf_z0;
+  int gf_nt, gf_nsrc, gf_nrec;
+  int gf_pad_;
 };
 
 constexpr int kTmaps = 9;
@@ -82,6 +92,7 @@ struct EpiParams {
   SolveDev* solves;
   int n_solves;
   int step;
+  int phase;  // 0: records, v2vn and vn2v; solves with SF_GF: 1 records + v2vn, 2 vn2v
 };
 
 // One ring slot (floats; every region 128-B aligned so TMA can land in it):
@@ -148,6 +159,7 @@ enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_
 cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
                         bool two_per_sm);
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_nsrc, cudaStream_t s);
 cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm);
 int consumer_threads();
 

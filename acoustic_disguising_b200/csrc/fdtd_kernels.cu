@@ -1023,6 +1023,18 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
   const int it = S.it_base + p.step;
   if (it > S.it_stop) return;
   const int ntx = S.ntx;
+  const bool gf = (S.flags & SF_GF) != 0;
+  if (p.phase == 2) {  // vn2v! of a GF solve, after the extrapolation wrote vn_src[it+1]
+    if (!gf || !S.vn_src || it >= S.nt) return;
+    for (int tx = blockIdx.x * blockDim.x + threadIdx.x; tx < ntx; tx += gridDim.x * blockDim.x) {
+      const long long nr = (long long)it * ntx + tx;
+      const float* d = S.dir + 4 * tx;
+      const float vs = S.vn_src[nr];
+#pragma unroll
+      for (int c = 1; c <= 3; ++c) S.src[c][nr] = __fadd_rn(S.src[c][nr], __fmul_rn(vs, d[c]));
+    }
+    return;
+  }
   for (int tx = blockIdx.x * blockDim.x + threadIdx.x; tx < ntx; tx += gridDim.x * blockDim.x) {
     const long long row = (long long)(it - 1) * ntx + tx;
     float r[4];
@@ -1041,7 +1053,7 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
     const float* d = S.dir + 4 * tx;
     S.vn_rec[row] =
         __fadd_rn(__fadd_rn(__fmul_rn(r[1], d[1]), __fmul_rn(r[2], d[2])), __fmul_rn(r[3], d[3]));
-    if (S.vn_src && it < S.nt) {
+    if (S.vn_src && it < S.nt && !gf) {
       const long long nr = row + ntx;
       const float vs = S.vn_src[nr];
 #pragma unroll
@@ -1052,6 +1064,67 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 
 // Advances it_base of every solve by `by` steps: the last node of a captured
 // chunk of steps, so replaying the graph continues where it stopped.
+// In-loop GF extrapolation, extrapolate!(::PVFromPin) with
+// extrapolate_pv_from_pin! (src/kernels/extrapolation.jl:139-170, 220-235),
+// after v2vn! of step it < nt.  One block per source column s:
+//   pin[t, r] = (p_rec[t, iRec[r]] - z0 * vn_rec[t, iRec[r]]) / 2   (Float64)
+//   psum/vsum = sum_r sum_tt p_pin/v_pin[T-tt+1, s, r] * pin[it-T+tt, r]
+// accumulated in Float64 (the Float32 zero is promoted by the first add),
+// stored as Float32 to p_src[it+1, iSrc[s]] = vsum, vn_src[it+1, iSrc[s]] =
+// psum.  Rows before `it` of pin come from gf_pin, row `it` is formed here and
+// block 0 files it for the later steps.
+__global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams p) {
+  const SolveDev& S = p.solves[blockIdx.y];
+  const int it = S.it_base + p.step;
+  if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
+  const int s = blockIdx.x;
+  if (s >= S.gf_nsrc) return;
+  const int nt = S.nt, ntx = S.ntx, ngf = S.gf_nt, nsrc = S.gf_nsrc, nrec = S.gf_nrec;
+  const int T = min(it, ngf);
+  const int t0 = it - T;  // 0-based row of tt = 1
+  const long long cur = (long long)(it - 1) * ntx;
+  auto pin_now = [&](int r) {
+    const int col = S.gf_irec[r];
+    return ((double)S.rec[0][cur + col] - (double)S.vn_rec[cur + col] * S.gf_z0) / 2.0;
+  };
+  if (s == 0)
+    for (int r = threadIdx.x; r < nrec; r += blockDim.x)
+      S.gf_pin[(long long)r * nt + (it - 1)] = pin_now(r);
+  double ps = 0.0, vs = 0.0;
+  const long long n = (long long)nrec * T;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    const int r = (int)(k / T);
+    const int tt = (int)(k - (long long)r * T);  // 0-based
+    const int row = t0 + tt;
+    const double pin = row == it - 1 ? pin_now(r) : S.gf_pin[(long long)r * nt + row];
+    const long long g = (long long)(T - 1 - tt) + (long long)ngf * (s + (long long)nsrc * r);
+    ps = __dadd_rn(ps, __dmul_rn((double)S.gf_pp[g], pin));
+    vs = __dadd_rn(vs, __dmul_rn((double)S.gf_vp[g], pin));
+  }
+  __shared__ double red[2][8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ps = __dadd_rn(ps, __shfl_down_sync(0xffffffffu, ps, o));
+    vs = __dadd_rn(vs, __shfl_down_sync(0xffffffffu, vs, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    red[0][w] = ps;
+    red[1][w] = vs;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a = __dadd_rn(a, red[0][k]);
+      b = __dadd_rn(b, red[1][k]);
+    }
+    const int col = S.gf_isrc[s];
+    S.src[0][(long long)it * S.src_ntx + col] = (float)b;  // p_src <- v_pin-derived
+    S.vn_src[(long long)it * ntx + col] = (float)a;        // vn_src <- p_pin-derived
+  }
+}
+
 __global__ void adf_advance_kernel(SolveDev* solves, int n, int by) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) solves[i].it_base += by;
@@ -1077,6 +1150,12 @@ cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, c
     adf_fdtd_step_kernel<2><<<grid, block, smem, s>>>(p);
   else
     adf_fdtd_step_kernel<1><<<grid, block, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_nsrc, cudaStream_t s) {
+  dim3 grid(max_nsrc > 0 ? max_nsrc : 1, p.n_solves);
+  adf_gf_extrapolate_kernel<<<grid, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -296,6 +296,7 @@ T* solve_dalloc(Solve& s, size_t n, int& rc) {
 }
 template float* solve_dalloc<float>(Solve&, size_t, int&);
 template int* solve_dalloc<int>(Solve&, size_t, int&);
+template double* solve_dalloc<double>(Solve&, size_t, int&);
 
 // Allocates everything except traces; field/psi zeroed.
 int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
@@ -440,8 +441,10 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   std::vector<int4> items;
   int max_stage = 0, max_pn = 0;
   max_ntx = 0;
+  max_gf_nsrc = 0;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
+    if (sd[i].flags & SF_GF) max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nsrc);
     for (int k = 0; k < kTmaps; ++k) tm[(size_t)kTmaps * i + k] = list[i]->tm[k];
     const SolveDev& d = list[i]->dev;
     const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
@@ -491,6 +494,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaStreamSynchronize(st);
   stage_floats = max_stage;
   pn_floats = max_pn;
+  per_step = max_gf_nsrc > 0 ? 4 : 2;
   // pipeline depth: as many slots as fit two CTAs per SM, else one CTA.
   // The kernel's static shared memory counts against the same budget.
   cudaFuncAttributes fa{};
@@ -564,9 +568,17 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   ep.solves = d_solves;
   ep.n_solves = (int)solves.size();
   ep.step = step;
+  ep.phase = 0;
   cudaError_t e2;
   if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
+  if (max_gf_nsrc > 0) {  // in-loop GF extrapolation, then vn2v! of those solves
+    if ((e2 = launch_gf_extrapolate(ep, max_gf_nsrc, ctx->stream)) != cudaSuccess)
+      return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
+    ep.phase = 2;
+    if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
+      return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
+  }
   return ADF_OK;
 }
 
@@ -578,7 +590,7 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
     for (int s = 0; s < nsteps; ++s) {
       int rc = launch_step(ctx, s);
       if (rc) return rc;
-      ctx->launches += 2;
+      ctx->launches += per_step;
     }
     return ADF_OK;
   }
@@ -603,13 +615,13 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
   while (nsteps - done >= chunk) {
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += 2 * chunk + 1;
+    ctx->launches += per_step * chunk + 1;
     done += chunk;
   }
   for (int s = 0; s < nsteps - done; ++s) {
     int rc = launch_step(ctx, s);
     if (rc) return rc;
-    ctx->launches += 2;
+    ctx->launches += per_step;
   }
   // restore it_base on the host-side copy's semantics: the caller re-uploads
   return ADF_OK;
@@ -638,7 +650,7 @@ int Batch::run_chunk(adf_ctx* ctx, int n, int chunk) {
     }
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += 2 * chunk + 1;
+    ctx->launches += per_step * chunk + 1;
     return ADF_OK;
   }
   for (int s = 0; s < n; ++s) {
@@ -646,7 +658,7 @@ int Batch::run_chunk(adf_ctx* ctx, int n, int chunk) {
     if (rc) return rc;
   }
   launch_advance(d_solves, (int)solves.size(), n, ctx->stream);
-  ctx->launches += 2 * n + 1;
+  ctx->launches += per_step * n + 1;
   return ADF_OK;
 }
 
@@ -739,6 +751,18 @@ static int download_traces(Solve& s, adf_txgrid* txs) {
     if (c > 0) down(d.src[c], txs->src[c]);
   }
   down(d.vn_rec, txs->vn_rec);
+  return ADF_OK;
+}
+
+// the GF extrapolation writes p_src and vn_src rows: both come back too
+static int download_gf_sources(Solve& s, adf_txgrid* txs) {
+  SolveDev& d = s.dev;
+  const int64_t nt = d.nt, ntx = d.ntx;
+  std::vector<float> tmp((size_t)(nt * ntx));
+  cudaMemcpy(tmp.data(), d.src[0], tmp.size() * 4, cudaMemcpyDeviceToHost);
+  transpose_to_julia(tmp.data(), txs->src[0], nt, ntx);
+  cudaMemcpy(tmp.data(), d.vn_src, tmp.size() * 4, cudaMemcpyDeviceToHost);
+  transpose_to_julia(tmp.data(), txs->vn_src, nt, ntx);
   return ADF_OK;
 }
 
@@ -966,10 +990,23 @@ int adf_pack_transceivers(const adf_domain* d, const double* points, const doubl
   return pack_transceivers_host(to_dom(*d), points, dirs, tf, o);
 }
 
-int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
-                 adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
-                 int flags, adf_step_cb cb, void* user) {
+static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                         adf_cpml* cpml, const uint8_t* mask, int64_t start_step,
+                         int64_t stop_step, int flags, const adf_gfmap* gf, adf_step_cb cb,
+                         void* user) {
   if (!ctx || !d || !field || !txs) return fail(ADF_E_ARG, "NULL argument");
+  const bool use_gf = gf && !gf->discard;
+  if (gf) {
+    if (gf->nt_gf < 1 || gf->nsrc < 1 || gf->nrec < 1 || !gf->i_src || !gf->i_rec ||
+        (use_gf && (!gf->p_pin || !gf->v_pin)))
+      return fail(ADF_E_ARG, "bad gf map");
+    for (int64_t k = 0; k < gf->nsrc; ++k)
+      if (gf->i_src[k] < 1 || gf->i_src[k] > txs->ntx)
+        return fail(ADF_E_ARG, "gf map iSrc outside 1..ntx");
+    for (int64_t k = 0; k < gf->nrec; ++k)
+      if (gf->i_rec[k] < 1 || gf->i_rec[k] > txs->ntx)
+        return fail(ADF_E_ARG, "gf map iRec outside 1..ntx");
+  }
   if (txs->nt != d->nt) return fail(ADF_E_ARG, "txs.nt must equal dom.nt");
   if (start_step < 1 || stop_step > d->nt) return fail(ADF_E_ARG, "step range outside 1..nt");
   if (d->nx < 4 || d->ny < 4 || d->nz < 4) return fail(ADF_E_ARG, "grid must be at least 4^3");
@@ -980,7 +1017,10 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
   if (npml > 63) return fail(ADF_E_ARG, "npml > 63 is not supported");
   if (stop_step < start_step) return ADF_OK;
   cudaSetDevice(ctx->device);
-  const size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
+  size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
+  if (use_gf)
+    need += (size_t)8 * gf->nt_gf * gf->nsrc * gf->nrec + (size_t)8 * gf->nrec * d->nt +
+            (size_t)4 * (gf->nsrc + gf->nrec);
   if (need > ctx->budget) return fail(ADF_E_BUDGET, "solve exceeds the context's HBM budget");
   auto s = std::make_unique<Solve>();
   const hm::Dom dom = to_dom(*d);
@@ -1009,6 +1049,43 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
       }
   }
   upload_traces(*s, txs, ctx->stream);
+  if (use_gf) {  // PVFromPin tensors, 0-based columns, Float64 pin history
+    const size_t ng = (size_t)gf->nt_gf * gf->nsrc * gf->nrec;
+    float* pp = solve_dalloc<float>(*s, ng, rc);
+    float* vp = rc ? nullptr : solve_dalloc<float>(*s, ng, rc);
+    int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->nsrc, rc);
+    int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->nrec, rc);
+    double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->nrec * d->nt, rc);
+    if (rc) return rc;
+    std::vector<int> cs((size_t)gf->nsrc), cr((size_t)gf->nrec);
+    for (int64_t k = 0; k < gf->nsrc; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
+    for (int64_t k = 0; k < gf->nrec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
+    cudaMemcpy(pp, gf->p_pin, ng * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(vp, gf->v_pin, ng * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(isrc, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(irec, cr.data(), cr.size() * 4, cudaMemcpyHostToDevice);
+    sd.gf_pp = pp;
+    sd.gf_vp = vp;
+    sd.gf_isrc = isrc;
+    sd.gf_irec = irec;
+    sd.gf_pin = pin;
+    sd.gf_z0 = gf->z0;
+    sd.gf_nt = (int)gf->nt_gf;
+    sd.gf_nsrc = (int)gf->nsrc;
+    sd.gf_nrec = (int)gf->nrec;
+    sd.flags |= SF_GF;
+    // pin rows recorded before start_step (a resumed run) from the host traces
+    if (start_step > 1) {
+      std::vector<double> h((size_t)gf->nrec * d->nt, 0.0);
+      for (int64_t r = 0; r < gf->nrec; ++r)
+        for (int64_t t = 0; t < start_step - 1; ++t) {
+          const int64_t o = t + d->nt * cr[(size_t)r];
+          h[(size_t)(r * d->nt + t)] =
+              ((double)txs->rec[0][o] - (double)txs->vn_rec[o] * gf->z0) / 2.0;
+        }
+      cudaMemcpy(pin, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+    }
+  }
   const float* idx[4] = {txs->idx[0], txs->idx[1], txs->idx[2], txs->idx[3]};
   const float* w[4] = {txs->w[0], txs->w[1], txs->w[2], txs->w[3]};
   rc = solve_finalize(ctx, *s, idx, w, nullptr);
@@ -1040,7 +1117,7 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
   } else {
     for (int k = 0; k < nsteps && !rc; ++k) {
       rc = b.launch_step(ctx, k);
-      ctx->launches += 2;
+      ctx->launches += b.per_step;
       if (rc) break;
       ctx->cur_it = start_step + k;
       cudaStreamSynchronize(ctx->stream);
@@ -1066,9 +1143,25 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
       if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], false, fb);
     }
   download_traces(*s, txs);
+  if (use_gf) download_gf_sources(*s, txs);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
   return ADF_OK;
+}
+
+int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                 adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                 int flags, adf_step_cb cb, void* user) {
+  return run_fdtd_impl(ctx, d, field, txs, cpml, mask, start_step, stop_step, flags, nullptr,
+                       cb, user);
+}
+
+int adf_run_fdtd_gf(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                    adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                    int flags, const adf_gfmap* gf, adf_step_cb cb, void* user) {
+  if (!gf) return fail(ADF_E_ARG, "NULL gf map");
+  return run_fdtd_impl(ctx, d, field, txs, cpml, mask, start_step, stop_step, flags, gf, cb,
+                       user);
 }
 
 int adf_read_field(adf_ctx* ctx, int chan, float* out) {

@@ -90,6 +90,8 @@ struct Batch {
   int cap_solves = 0, cap_items = 0;
   int n_items = 0, stages = 3, stage_floats = 0, pn_floats = 0, grid = 1, max_ntx = 0;
   bool two_per_sm = false;  // ring sized so two CTAs share an SM
+  int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
+  int per_step = 2;          // kernel launches per launch-step
   size_t smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;

@@ -161,6 +161,31 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
                  adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
                  int flags, adf_step_cb cb, void* user);
 
+/* GFMap of run_fdtd!(...; gf_map): a PVFromPin map (src/kernels/
+ * extrapolation.jl:72-87).  p_pin, v_pin (nt_gf, nsrc, nrec) Float32 Julia
+ * layout; i_src, i_rec 1-based transceiver indices (iSrc, iRec).          */
+typedef struct {
+  int64_t nt_gf, nsrc, nrec;
+  const float* p_pin;
+  const float* v_pin;
+  const int64_t* i_src;
+  const int64_t* i_rec;
+  double z0;
+  int discard;  /* 1: as the reference ships (extrapolation.jl:228-229 writes
+                   into slice copies, so the sources never change); 0: the
+                   documented intent, sources written into txs            */
+} adf_gfmap;
+
+/* run_fdtd! with a gf_map (src/simulation.jl:542-557, forward.jl:123-128):
+ * adf_run_fdtd plus, after v2vn! of each step it < nt, extrapolate!
+ * (extrapolation.jl:220-235 -> extrapolate_pv_from_pin!, :139-170) on the
+ * device: pin = (p_rec - z0 vn_rec)/2 over iRec (Float64), Float64 sums
+ * over receivers and lags, p_src[it+1, iSrc] and vn_src[it+1, iSrc] set
+ * before vn2v!.  txs->src[0] and txs->vn_src come back updated.            */
+int adf_run_fdtd_gf(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                    adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                    int flags, const adf_gfmap* gf, adf_step_cb cb, void* user);
+
 /* Inside an adf_step_cb: copy channel c (0=P..3=Vz) of the current field,
  * (nx,ny,nz) Float32 Julia layout, to host memory.                        */
 int adf_read_field(adf_ctx* ctx, int chan, float* out);

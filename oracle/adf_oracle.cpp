@@ -506,9 +506,36 @@ inline void interp_trilinear(View& v, int c, int64_t it, const float* idx, const
   }
 }
 
+// extrapolate!(::PVFromPin) (extrapolation.jl:220-235) with
+// extrapolate_pv_from_pin! (extrapolation.jl:139-170) at step it
+void gf_extrapolate(const or_gfmap* g, or_txgrid* txs, int64_t nt, int64_t it) {
+  const int64_t T = std::min(it, g->nt_gf);
+  const int64_t t_off = it - T + 1;
+  pfor(0, g->nsrc, [&](int64_t s) {
+    double psum = 0.0, vsum = 0.0;  // Float32 zero promoted by the first Float64 add
+    for (int64_t r = 0; r < g->nrec; ++r) {
+      const int64_t col = g->i_rec[r] - 1;
+      for (int64_t tt = 1; tt <= T; ++tt) {
+        const int64_t gi = T - tt + 1;
+        const int64_t row = t_off + tt - 1;  // 1-based
+        const double pin = ((double)txs->rec[0][(row - 1) + nt * col] -
+                            (double)txs->vn_rec[(row - 1) + nt * col] * g->z0) / 2.0;
+        const size_t k = (size_t)(gi - 1) + (size_t)g->nt_gf * (size_t)(s + g->nsrc * r);
+        psum += (double)g->p_pin[k] * pin;
+        vsum += (double)g->v_pin[k] * pin;
+      }
+    }
+    if (!g->discard) {
+      const int64_t col = g->i_src[s] - 1;
+      txs->src[0][it + nt * col] = (float)vsum;  // p_src <- v_pin-derived
+      txs->vn_src[it + nt * col] = (float)psum;  // vn_src <- p_pin-derived
+    }
+  });
+}
+
 template <typename R>
 int run_fdtd_t(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp,
-               const uint8_t* mask, int64_t start, int64_t stop) {
+               const uint8_t* mask, int64_t start, int64_t stop, const or_gfmap* gf = nullptr) {
   View v{d->nx, d->ny, d->nz, field};
   Scal<R> s{(R)d->fact_m0, (R)d->fact_m1, (R)d->dx, (R)d->dy, (R)d->dz};
   const int64_t nx = d->nx, ny = d->ny, nz = d->nz, nt = d->nt;
@@ -557,6 +584,8 @@ int run_fdtd_t(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp,
       int64_t o = (it - 1) + nt * is;
       txs->vn_rec[o] = txs->rec[1][o] * n[1] + txs->rec[2][o] * n[2] + txs->rec[3][o] * n[3];
     }
+    // forward.jl:123-128 in-loop GF extrapolation
+    if (gf && it < nt) gf_extrapolate(gf, txs, nt, it);
     // forward.jl:130-132 vn2v! into row it+1
     if (it < nt) {
       for (int64_t is = 0; is < txs->ntx; ++is) {
@@ -896,6 +925,21 @@ int or_pack_transceivers(const or_domain* d, const double* points, const double*
     }
   }
   return 0;
+}
+
+int or_run_fdtd_gf(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
+                   const uint8_t* mask, int64_t start_step, int64_t stop_step, int mode,
+                   const or_gfmap* gf, int nthreads) {
+  if (!d || !field || !txs || !gf) return -1;
+  if (start_step < 1 || stop_step > d->nt) return -1;
+  for (int64_t s = 0; s < gf->nsrc; ++s)
+    if (gf->i_src[s] < 1 || gf->i_src[s] > txs->ntx) return -1;
+  for (int64_t r = 0; r < gf->nrec; ++r)
+    if (gf->i_rec[r] < 1 || gf->i_rec[r] > txs->ntx) return -1;
+  set_threads(nthreads);
+  if (mode == OR_MODE_FP32)
+    return run_fdtd_t<float>(d, field, txs, cpml, mask, start_step, stop_step, gf);
+  return run_fdtd_t<double>(d, field, txs, cpml, mask, start_step, stop_step, gf);
 }
 
 int or_run_fdtd(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,

@@ -108,6 +108,29 @@ int or_run_fdtd(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
                 const uint8_t* mask, int64_t start_step, int64_t stop_step, int mode,
                 int nthreads);
 
+/* In-loop GF extrapolation of run_fdtd!(...; gf_map) for a PVFromPin map
+ * (src/kernels/extrapolation.jl:72-87, 139-170, 220-235; forward.jl:123-128):
+ * after v2vn! of step it (< nt), pin = (p_rec[:, iRec] - z0*vn_rec[:, iRec])/2
+ * (Float64, as Float32 traces times the Float64 z0 promote), and for every
+ * source column s
+ *   vsum = sum_r sum_tt v_pin[T-tt+1, s, r] * pin[it-T+tt, r]   (Float64)
+ *   psum = the same with p_pin,   T = min(it, nt_gf),
+ * stored as Float32 into p_src[it+1, iSrc[s]] = vsum and
+ * vn_src[it+1, iSrc[s]] = psum before vn2v! distributes vn_src.  discard = 1
+ * reproduces the shipped code, whose slice copies drop those writes.       */
+typedef struct {
+  int64_t nt_gf, nsrc, nrec;
+  const float* p_pin;    /* (nt_gf, nsrc, nrec) */
+  const float* v_pin;
+  const int64_t* i_src;  /* (nsrc), 1-based transceiver indices */
+  const int64_t* i_rec;  /* (nrec), 1-based */
+  double z0;
+  int discard;
+} or_gfmap;
+int or_run_fdtd_gf(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
+                   const uint8_t* mask, int64_t start_step, int64_t stop_step, int mode,
+                   const or_gfmap* gf, int nthreads);
+
 /* ---- Kirchhoff-Helmholtz (src/kh_kernels.jl) ----
  * which: 0=p_p 1=p_v 2=v_p 3=v_v.  Points (n,3) column-major Float64.   */
 int or_kh_eval_kernel(int which, int64_t n_outer, const double* outer_pts,

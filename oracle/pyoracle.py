@@ -58,6 +58,12 @@ class _Cpml(C.Structure):
                 ("coef", C.c_void_p)]
 
 
+class _GfMap(C.Structure):
+    _fields_ = [("nt_gf", C.c_int64), ("nsrc", C.c_int64), ("nrec", C.c_int64),
+                ("p_pin", C.c_void_p), ("v_pin", C.c_void_p), ("i_src", C.c_void_p),
+                ("i_rec", C.c_void_p), ("z0", C.c_double), ("discard", C.c_int)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -81,6 +87,9 @@ def lib():
                                            C.POINTER(_TxGrid)]
         L.or_run_fdtd.argtypes = [dp, C.c_void_p, C.POINTER(_TxGrid), C.POINTER(_Cpml),
                                   C.c_void_p, C.c_int64, C.c_int64, C.c_int, C.c_int]
+        L.or_run_fdtd_gf.argtypes = [dp, C.c_void_p, C.POINTER(_TxGrid), C.POINTER(_Cpml),
+                                     C.c_void_p, C.c_int64, C.c_int64, C.c_int,
+                                     C.POINTER(_GfMap), C.c_int]
         L.or_kh_eval_kernel.argtypes = [C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64,
                                         C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                         C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_int]
@@ -312,6 +321,29 @@ def run_fdtd(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask=None, start_st
     _chk(lib().or_run_fdtd(C.byref(d), _p(field), C.byref(cg), C.byref(cc) if cc else None,
                            _p(mask) if mask is not None else None, start_step, stop_step,
                            MODES[mode], nthreads), "run_fdtd")
+    return field
+
+
+def run_fdtd_gf(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask, p_pin, v_pin, i_src,
+                i_rec, z0, discard=False, start_step=1, stop_step=None, mode="promote",
+                nthreads=0):
+    """run_fdtd!(...; gf_map = PVFromPin(p_pin, v_pin) with iSrc/iRec): the in-loop
+    GF extrapolation (extrapolation.jl:139-170, 220-235).  p_pin, v_pin are
+    (nt_gf, nsrc, nrec) float32; i_src, i_rec 1-based transceiver indices."""
+    stop_step = d.nt if stop_step is None else stop_step
+    assert field.flags.f_contiguous and field.dtype == np.float32
+    pp = np.asfortranarray(p_pin, np.float32)
+    vp = np.asfortranarray(v_pin, np.float32)
+    isr = np.ascontiguousarray(i_src, np.int64)
+    irc = np.ascontiguousarray(i_rec, np.int64)
+    g = _GfMap(nt_gf=pp.shape[0], nsrc=pp.shape[1], nrec=pp.shape[2], p_pin=pp.ctypes.data,
+               v_pin=vp.ctypes.data, i_src=isr.ctypes.data, i_rec=irc.ctypes.data, z0=z0,
+               discard=int(bool(discard)))
+    cg = txs._c()
+    cc = cpml._c() if cpml is not None else None
+    _chk(lib().or_run_fdtd_gf(C.byref(d), _p(field), C.byref(cg), C.byref(cc) if cc else None,
+                              _p(mask) if mask is not None else None, start_step, stop_step,
+                              MODES[mode], C.byref(g), nthreads), "run_fdtd_gf")
     return field
 
 
