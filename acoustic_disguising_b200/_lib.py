@@ -85,9 +85,13 @@ class KhDescC(C.Structure):
 
 
 class GfMapC(C.Structure):
-    _fields_ = [("nt_gf", C.c_int64), ("nsrc", C.c_int64), ("nrec", C.c_int64),
-                ("p_pin", C.c_void_p), ("v_pin", C.c_void_p), ("i_src", C.c_void_p),
-                ("i_rec", C.c_void_p), ("z0", C.c_double), ("discard", C.c_int)]
+    _fields_ = [("kind", C.c_int), ("nt_gf", C.c_int64), ("n1", C.c_int64), ("n2", C.c_int64),
+                ("t", C.c_void_p * 4), ("i_src", C.c_void_p), ("n_src", C.c_int64),
+                ("i_rec", C.c_void_p), ("n_rec", C.c_int64), ("z0", C.c_double),
+                ("discard", C.c_int)]
+
+
+GF_KINDS = {"PVFromPin": 0, "PFromPin": 1, "PVFromPV": 2}
 
 
 STEP_CB = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_void_p)

@@ -345,37 +345,54 @@ def vn_rec(g: TransceiverGrid):
 # Time stepping (src/simulation.jl:542-557)
 # ---------------------------------------------------------------------------
 @dataclass
-class PVFromPin:
-    """PVFromPin GF map (src/kernels/extrapolation.jl:72-87): p_pin, v_pin
-    (nt_gf, nsrc, nrec) float32, iSrc/iRec 1-based transceiver indices.
-    discard=True reproduces the reference as shipped, whose extrapolate!
-    writes into slice copies so the sources never change."""
+class GfMap:
+    """A GFMap of run_fdtd!(...; gf_map) (src/kernels/extrapolation.jl:36-87).
+    kind "PVFromPin": tensors (p_pin, v_pin), each (nt_gf, #iSrc, #iRec);
+    kind "PFromPin": (pos, neg), each (nt_gf, #iRec, #iSrc);
+    kind "PVFromPV": (pp, pv, vp, vv), each (nt_gf, #iRec, #iSrc).
+    i_src / i_rec are 1-based transceiver indices.  discard=True reproduces
+    the reference as shipped, whose extrapolate! writes into slice copies so
+    the sources never change."""
 
-    p_pin: np.ndarray
-    v_pin: np.ndarray
+    kind: str
+    tensors: tuple
     i_src: np.ndarray
     i_rec: np.ndarray
     discard: bool = False
 
     def _c(self, z0: float):
-        self._pp = np.asfortranarray(self.p_pin, np.float32)
-        self._vp = np.asfortranarray(self.v_pin, np.float32)
+        self._t = [np.asfortranarray(t, np.float32) for t in self.tensors]
         self._is = np.ascontiguousarray(self.i_src, np.int64)
         self._ir = np.ascontiguousarray(self.i_rec, np.int64)
-        if self._pp.shape != self._vp.shape or self._pp.ndim != 3:
-            raise ValueError("p_pin and v_pin must both be (nt_gf, nsrc, nrec)")
-        if self._is.size != self._pp.shape[1] or self._ir.size != self._pp.shape[2]:
-            raise ValueError("iSrc / iRec lengths must match the GF tensors")
-        return L.GfMapC(nt_gf=self._pp.shape[0], nsrc=self._pp.shape[1], nrec=self._pp.shape[2],
-                        p_pin=self._pp.ctypes.data, v_pin=self._vp.ctypes.data,
-                        i_src=self._is.ctypes.data, i_rec=self._ir.ctypes.data, z0=float(z0),
-                        discard=int(bool(self.discard)))
+        want = 4 if self.kind == "PVFromPV" else 2
+        if len(self._t) != want or any(t.shape != self._t[0].shape or t.ndim != 3
+                                         for t in self._t):
+            raise ValueError(f"{self.kind} takes {want} tensors of one shape (nt_gf, n1, n2)")
+        g = L.GfMapC(kind=L.GF_KINDS[self.kind], nt_gf=self._t[0].shape[0],
+                     n1=self._t[0].shape[1], n2=self._t[0].shape[2], i_src=self._is.ctypes.data,
+                     n_src=self._is.size, i_rec=self._ir.ctypes.data, n_rec=self._ir.size,
+                     z0=float(z0), discard=int(bool(self.discard)))
+        for k, t in enumerate(self._t):
+            g.t[k] = t.ctypes.data
+        return g
+
+
+def PVFromPin(p_pin, v_pin, i_src, i_rec, discard=False) -> GfMap:
+    return GfMap("PVFromPin", (p_pin, v_pin), i_src, i_rec, discard)
+
+
+def PFromPin(pos, neg, i_src, i_rec, discard=False) -> GfMap:
+    return GfMap("PFromPin", (pos, neg), i_src, i_rec, discard)
+
+
+def PVFromPV(pp, pv, vp, vv, i_src, i_rec, discard=False) -> GfMap:
+    return GfMap("PVFromPV", (pp, pv, vp, vv), i_src, i_rec, discard)
 
 
 def run_fdtd(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | None, va=None,
              start_step: int = 1, on_step=None, stop_step: int | None = None,
              arith: str = "promote", ctx: Context | None = None,
-             gf_map: PVFromPin | None = None) -> np.ndarray:
+             gf_map: GfMap | None = None) -> np.ndarray:
     """run_fdtd!(dom, field, txs, cpml, va; start_step, on_step, gf_map):
     advances `field` (and the trace buffers and CPML memory) in place on the
     GPU.  on_step(it, read) is called after each step; read(c) returns

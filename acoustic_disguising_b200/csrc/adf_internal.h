@@ -25,6 +25,9 @@ enum : int {
   SF_GF = 32,       // in-loop GF extrapolation between v2vn and vn2v
 };
 
+// GF map kinds, as ADF_GF_* in include/adfdtd.h
+enum : int { ADF_GF_PV_FROM_PIN_ = 0, ADF_GF_P_FROM_PIN_ = 1, ADF_GF_PV_FROM_PV_ = 2 };
+
 struct SolveDev {
   int nx, ny, nz, nxp;
   int ty, nty;       // tile rows, number of y tiles
@@ -61,15 +64,14 @@ struct SolveDev {
   const float* dir;       // [ntx][4]
   int* err;               // per-solve error word
   int pad_;
-  // in-loop GF extrapolation (PVFromPin), SF_GF only
-  const float* gf_pp;     // (nt_gf, nsrc, nrec) column-major
-  const float* gf_vp;
-  const int* gf_isrc;     // [nsrc] 0-based transceiver column
-  const int* gf_irec;     // [nrec]
-  double* gf_pin;         // [nrec][nt] (p_rec - z0 vn_rec)/2 of recorded rows
+  // in-loop GF extrapolation, SF_GF only
+  const float* gf_t[4];   // (nt_gf, n1, n2) column-major tensors of the map kind
+  const int* gf_isrc;     // [n_out] 0-based transceiver columns driven
+  const int* gf_irec;     // [n_in] 0-based transceiver columns read
+  double* gf_pin;         // [n_in][nt] (p_rec - z0 vn_rec)/2 of recorded rows
   double gf_z0;
-  int gf_nt, gf_nsrc, gf_nrec;
-  int gf_pad_;
+  int gf_kind, gf_nt, gf_n1, gf_n2;
+  int gf_nout, gf_nin;
 };
 
 constexpr int kTmaps = 9;

@@ -1064,22 +1064,26 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 
 // Advances it_base of every solve by `by` steps: the last node of a captured
 // chunk of steps, so replaying the graph continues where it stopped.
-// In-loop GF extrapolation, extrapolate!(::PVFromPin) with
-// extrapolate_pv_from_pin! (src/kernels/extrapolation.jl:139-170, 220-235),
-// after v2vn! of step it < nt.  One block per source column s:
-//   pin[t, r] = (p_rec[t, iRec[r]] - z0 * vn_rec[t, iRec[r]]) / 2   (Float64)
-//   psum/vsum = sum_r sum_tt p_pin/v_pin[T-tt+1, s, r] * pin[it-T+tt, r]
-// accumulated in Float64 (the Float32 zero is promoted by the first add),
-// stored as Float32 to p_src[it+1, iSrc[s]] = vsum, vn_src[it+1, iSrc[s]] =
-// psum.  Rows before `it` of pin come from gf_pin, row `it` is formed here and
-// block 0 files it for the later steps.
+// In-loop GF extrapolation, extrapolate! (src/kernels/extrapolation.jl:204-249)
+// after v2vn! of step it < nt.  One block per driven source o:
+//   PVFromPin (:139-170): pin[t, r] = (p_rec - z0 vn_rec)/2 (Float64);
+//     ps/vs = sum_r sum_tt p_pin/v_pin[T-tt+1, o, r] * pin[it-T+tt, r];
+//     p_src[it+1, iSrc[o]] = vs, vn_src[it+1, iSrc[o]] = ps.
+//   PFromPin (:172-193, 237-249): pos/neg[o] = sums of pos/neg[., r, o] * pin,
+//     rounded to Float32; p_src = pos - neg, vn_src = (pos + neg) / z0.
+//   PVFromPV (:91-137, 204-218): ps += pv*p + pp*vn, vs += vv*p + vp*vn over
+//     the recorded p / v_n of the iRec columns (Float32 terms).
+// Sums are accumulated in Float64 (the Float32 zero of the reference is
+// promoted by the first Float64 add for the *FromPin kinds).  Rows before
+// `it` of pin come from gf_pin; row `it` is formed here and block 0 files it.
 __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it = S.it_base + p.step;
   if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
-  const int s = blockIdx.x;
-  if (s >= S.gf_nsrc) return;
-  const int nt = S.nt, ntx = S.ntx, ngf = S.gf_nt, nsrc = S.gf_nsrc, nrec = S.gf_nrec;
+  const int o = blockIdx.x;
+  if (o >= S.gf_nout) return;
+  const int nt = S.nt, ntx = S.ntx, ngf = S.gf_nt, n1 = S.gf_n1, nin = S.gf_nin;
+  const int kind = S.gf_kind;
   const int T = min(it, ngf);
   const int t0 = it - T;  // 0-based row of tt = 1
   const long long cur = (long long)(it - 1) * ntx;
@@ -1087,41 +1091,63 @@ __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams
     const int col = S.gf_irec[r];
     return ((double)S.rec[0][cur + col] - (double)S.vn_rec[cur + col] * S.gf_z0) / 2.0;
   };
-  if (s == 0)
-    for (int r = threadIdx.x; r < nrec; r += blockDim.x)
+  if (o == 0 && kind != ADF_GF_PV_FROM_PV_)
+    for (int r = threadIdx.x; r < nin; r += blockDim.x)
       S.gf_pin[(long long)r * nt + (it - 1)] = pin_now(r);
-  double ps = 0.0, vs = 0.0;
-  const long long n = (long long)nrec * T;
+  double a = 0.0, b = 0.0;
+  const long long n = (long long)nin * T;
   for (long long k = threadIdx.x; k < n; k += blockDim.x) {
     const int r = (int)(k / T);
     const int tt = (int)(k - (long long)r * T);  // 0-based
     const int row = t0 + tt;
-    const double pin = row == it - 1 ? pin_now(r) : S.gf_pin[(long long)r * nt + row];
-    const long long g = (long long)(T - 1 - tt) + (long long)ngf * (s + (long long)nsrc * r);
-    ps = __dadd_rn(ps, __dmul_rn((double)S.gf_pp[g], pin));
-    vs = __dadd_rn(vs, __dmul_rn((double)S.gf_vp[g], pin));
+    // tensor element [T-tt, ., .] (1-based lag) for this receiver and output
+    const long long g = (long long)(T - 1 - tt) +
+                        (long long)ngf * (kind == ADF_GF_PV_FROM_PIN_ ? o + (long long)n1 * r
+                                                                      : r + (long long)n1 * o);
+    if (kind == ADF_GF_PV_FROM_PV_) {
+      const int col = S.gf_irec[r];
+      const float pt = S.rec[0][(long long)row * ntx + col];
+      const float vt = S.vn_rec[(long long)row * ntx + col];
+      const float ps = __fadd_rn(__fmul_rn(S.gf_t[1][g], pt), __fmul_rn(S.gf_t[0][g], vt));
+      const float vs = __fadd_rn(__fmul_rn(S.gf_t[3][g], pt), __fmul_rn(S.gf_t[2][g], vt));
+      a = __dadd_rn(a, (double)ps);
+      b = __dadd_rn(b, (double)vs);
+    } else {
+      const double pin = row == it - 1 ? pin_now(r) : S.gf_pin[(long long)r * nt + row];
+      a = __dadd_rn(a, __dmul_rn((double)S.gf_t[0][g], pin));
+      b = __dadd_rn(b, __dmul_rn((double)S.gf_t[1][g], pin));
+    }
   }
   __shared__ double red[2][8];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ps = __dadd_rn(ps, __shfl_down_sync(0xffffffffu, ps, o));
-    vs = __dadd_rn(vs, __shfl_down_sync(0xffffffffu, vs, o));
+  for (int w = 16; w > 0; w >>= 1) {
+    a = __dadd_rn(a, __shfl_down_sync(0xffffffffu, a, w));
+    b = __dadd_rn(b, __shfl_down_sync(0xffffffffu, b, w));
   }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int wi = threadIdx.x >> 5, l = threadIdx.x & 31;
   if (l == 0) {
-    red[0][w] = ps;
-    red[1][w] = vs;
+    red[0][wi] = a;
+    red[1][wi] = b;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
+    double sa = 0.0, sb = 0.0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-      a = __dadd_rn(a, red[0][k]);
-      b = __dadd_rn(b, red[1][k]);
+      sa = __dadd_rn(sa, red[0][k]);
+      sb = __dadd_rn(sb, red[1][k]);
     }
-    const int col = S.gf_isrc[s];
-    S.src[0][(long long)it * S.src_ntx + col] = (float)b;  // p_src <- v_pin-derived
-    S.vn_src[(long long)it * ntx + col] = (float)a;        // vn_src <- p_pin-derived
+    const int col = S.gf_isrc[o];
+    float ps, vs;
+    if (kind == ADF_GF_P_FROM_PIN_) {
+      const float pos = (float)sa, neg = (float)sb;
+      ps = (float)((double)__fadd_rn(pos, neg) / S.gf_z0);  // vn_src
+      vs = __fsub_rn(pos, neg);                                            // p_src
+    } else {
+      ps = (float)sa;  // vn_src <- p_pin / (pv, pp)-derived
+      vs = (float)sb;  // p_src  <- v_pin / (vv, vp)-derived
+    }
+    S.src[0][(long long)it * S.src_ntx + col] = vs;
+    S.vn_src[(long long)it * ntx + col] = ps;
   }
 }
 
@@ -1154,6 +1180,7 @@ cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, c
 }
 
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_nsrc, cudaStream_t s) {
+  // one block per driven source of the largest map in the batch
   dim3 grid(max_nsrc > 0 ? max_nsrc : 1, p.n_solves);
   adf_gf_extrapolate_kernel<<<grid, 256, 0, s>>>(p);
   return cudaGetLastError();

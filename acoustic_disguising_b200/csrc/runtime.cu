@@ -444,7 +444,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   max_gf_nsrc = 0;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
-    if (sd[i].flags & SF_GF) max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nsrc);
+    if (sd[i].flags & SF_GF) max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
     for (int k = 0; k < kTmaps; ++k) tm[(size_t)kTmaps * i + k] = list[i]->tm[k];
     const SolveDev& d = list[i]->dev;
     const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
@@ -996,14 +996,24 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
                          void* user) {
   if (!ctx || !d || !field || !txs) return fail(ADF_E_ARG, "NULL argument");
   const bool use_gf = gf && !gf->discard;
+  int ntens = 0;
   if (gf) {
-    if (gf->nt_gf < 1 || gf->nsrc < 1 || gf->nrec < 1 || !gf->i_src || !gf->i_rec ||
-        (use_gf && (!gf->p_pin || !gf->v_pin)))
+    if (gf->kind < ADF_GF_PV_FROM_PIN || gf->kind > ADF_GF_PV_FROM_PV)
+      return fail(ADF_E_ARG, "unknown gf map kind");
+    ntens = gf->kind == ADF_GF_PV_FROM_PV ? 4 : 2;
+    // driven sources and read receivers per kind (extrapolation.jl:36-87)
+    const int64_t nout = gf->kind == ADF_GF_PV_FROM_PIN ? gf->n1 : gf->n2;
+    const int64_t nin = gf->kind == ADF_GF_PV_FROM_PIN ? gf->n2 : gf->n1;
+    if (gf->nt_gf < 1 || gf->n1 < 1 || gf->n2 < 1 || !gf->i_src || !gf->i_rec)
       return fail(ADF_E_ARG, "bad gf map");
-    for (int64_t k = 0; k < gf->nsrc; ++k)
+    if (gf->n_src != nout || gf->n_rec != nin)
+      return fail(ADF_E_ARG, "gf map: iSrc/iRec lengths do not match the tensor dimensions");
+    for (int k = 0; use_gf && k < ntens; ++k)
+      if (!gf->t[k]) return fail(ADF_E_ARG, "gf map: missing tensor");
+    for (int64_t k = 0; k < gf->n_src; ++k)
       if (gf->i_src[k] < 1 || gf->i_src[k] > txs->ntx)
         return fail(ADF_E_ARG, "gf map iSrc outside 1..ntx");
-    for (int64_t k = 0; k < gf->nrec; ++k)
+    for (int64_t k = 0; k < gf->n_rec; ++k)
       if (gf->i_rec[k] < 1 || gf->i_rec[k] > txs->ntx)
         return fail(ADF_E_ARG, "gf map iRec outside 1..ntx");
   }
@@ -1019,8 +1029,8 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   cudaSetDevice(ctx->device);
   size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
   if (use_gf)
-    need += (size_t)8 * gf->nt_gf * gf->nsrc * gf->nrec + (size_t)8 * gf->nrec * d->nt +
-            (size_t)4 * (gf->nsrc + gf->nrec);
+    need += (size_t)4 * ntens * gf->nt_gf * gf->n1 * gf->n2 + (size_t)8 * gf->n_rec * d->nt +
+            (size_t)4 * (gf->n_src + gf->n_rec);
   if (need > ctx->budget) return fail(ADF_E_BUDGET, "solve exceeds the context's HBM budget");
   auto s = std::make_unique<Solve>();
   const hm::Dom dom = to_dom(*d);
@@ -1049,35 +1059,37 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
       }
   }
   upload_traces(*s, txs, ctx->stream);
-  if (use_gf) {  // PVFromPin tensors, 0-based columns, Float64 pin history
-    const size_t ng = (size_t)gf->nt_gf * gf->nsrc * gf->nrec;
-    float* pp = solve_dalloc<float>(*s, ng, rc);
-    float* vp = rc ? nullptr : solve_dalloc<float>(*s, ng, rc);
-    int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->nsrc, rc);
-    int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->nrec, rc);
-    double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->nrec * d->nt, rc);
+  if (use_gf) {  // GF tensors, 0-based columns, Float64 pin history
+    const size_t ng = (size_t)gf->nt_gf * gf->n1 * gf->n2;
+    for (int k = 0; k < ntens && !rc; ++k) {
+      float* t = solve_dalloc<float>(*s, ng, rc);
+      if (!rc) cudaMemcpy(t, gf->t[k], ng * 4, cudaMemcpyHostToDevice);
+      sd.gf_t[k] = t;
+    }
+    int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_src, rc);
+    int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_rec, rc);
+    double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_rec * d->nt, rc);
     if (rc) return rc;
-    std::vector<int> cs((size_t)gf->nsrc), cr((size_t)gf->nrec);
-    for (int64_t k = 0; k < gf->nsrc; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
-    for (int64_t k = 0; k < gf->nrec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
-    cudaMemcpy(pp, gf->p_pin, ng * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(vp, gf->v_pin, ng * 4, cudaMemcpyHostToDevice);
+    std::vector<int> cs((size_t)gf->n_src), cr((size_t)gf->n_rec);
+    for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
+    for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
     cudaMemcpy(isrc, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(irec, cr.data(), cr.size() * 4, cudaMemcpyHostToDevice);
-    sd.gf_pp = pp;
-    sd.gf_vp = vp;
     sd.gf_isrc = isrc;
     sd.gf_irec = irec;
     sd.gf_pin = pin;
     sd.gf_z0 = gf->z0;
+    sd.gf_kind = gf->kind;
     sd.gf_nt = (int)gf->nt_gf;
-    sd.gf_nsrc = (int)gf->nsrc;
-    sd.gf_nrec = (int)gf->nrec;
+    sd.gf_n1 = (int)gf->n1;
+    sd.gf_n2 = (int)gf->n2;
+    sd.gf_nout = (int)gf->n_src;
+    sd.gf_nin = (int)gf->n_rec;
     sd.flags |= SF_GF;
     // pin rows recorded before start_step (a resumed run) from the host traces
-    if (start_step > 1) {
-      std::vector<double> h((size_t)gf->nrec * d->nt, 0.0);
-      for (int64_t r = 0; r < gf->nrec; ++r)
+    if (start_step > 1 && gf->kind != ADF_GF_PV_FROM_PV) {
+      std::vector<double> h((size_t)gf->n_rec * d->nt, 0.0);
+      for (int64_t r = 0; r < gf->n_rec; ++r)
         for (int64_t t = 0; t < start_step - 1; ++t) {
           const int64_t o = t + d->nt * cr[(size_t)r];
           h[(size_t)(r * d->nt + t)] =

@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--no-kh", action="store_true", help="skip the KH section")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-step512", action="store_true", help="skip the 512^3 step section")
+    ap.add_argument("--no-gf", action="store_true", help="skip the in-loop GF section")
     ap.add_argument("--serving-requests", type=int, default=20)
     ap.add_argument("--serving-resident", type=int, default=2,
                     help="server slot limit (0: HBM budget only)")
@@ -459,6 +460,40 @@ def step512_section(A, ctx, nt=48, tune=True):
 
 
 # ---------------------------------------------------------------------------
+# In-loop GF extrapolation (run_fdtd! gf_map = PVFromPin) on a 128^3 run
+# ---------------------------------------------------------------------------
+def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
+    d = A.Domain(tmax=tmax_of(nt), xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
+    tf = A.ricker_wavelet(d, 2000.0, injection=False)
+    rp, rn = A.fibonacci_sphere(n_io, 40 * DX)   # recording shell (iRec)
+    ip, inn = A.fibonacci_sphere(n_io, 30 * DX)  # injection surface (iSrc)
+    txs = [A.Transceiver(np.zeros(3), np.array([1.0, 0, 0, 0]), tf * 1e3)]
+    txs += [A.Transceiver(rp[k], np.r_[0.0, rn[k]], np.zeros(d.nt)) for k in range(n_io)]
+    txs += [A.Transceiver(ip[k], np.r_[0.0, inn[k]], np.zeros(d.nt)) for k in range(n_io)]
+    i_rec = np.arange(2, 2 + n_io, dtype=np.int64)
+    i_src = np.arange(2 + n_io, 2 + 2 * n_io, dtype=np.int64)
+    rng = np.random.default_rng(11)
+    shape = (nt_gf, n_io, n_io)
+    pp = (rng.standard_normal(shape) * 1e-4).astype(np.float32, order="F")
+    vp = (rng.standard_normal(shape) * 1e-4).astype(np.float32, order="F")
+    times = {}
+    for discard in (True, False):
+        g = A.transceivers_to_grid(d, txs)
+        cp = A.Cpml(d, NPML, 1e-4, PML_FC)
+        f = np.zeros((n, n, n, 4), np.float32, order="F")
+        A.run_fdtd(d, f, g, cp, ctx=ctx, gf_map=A.PVFromPin(pp, vp, i_src, i_rec, discard))
+        times[discard] = ctx.last_timing()[0]
+    gf_ms = times[False] - times[True]
+    lags = sum(min(it, nt_gf) for it in range(1, nt))
+    byts = 2.0 * 4 * n_io * n_io * lags  # both tensors' lag slices, read once per step
+    return {"workload": f"{n}^3 run_fdtd!, {nt} steps, PVFromPin map {nt_gf} lags x {n_io} "
+                        f"sources x {n_io} receivers",
+            "run_ms_without_map": times[True], "run_ms_with_map": times[False],
+            "gf_ms_per_step": gf_ms / (nt - 1),
+            "gf_tensor_gbs": byts / (gf_ms / 1e3) / 1e9 if gf_ms > 0 else None}
+
+
+# ---------------------------------------------------------------------------
 # multi-rank plumbing (one process per GPU)
 # ---------------------------------------------------------------------------
 def rank_first_source(step_ix, world, rank, batch):
@@ -543,6 +578,8 @@ def b200_arm(args):
     extra = {}
     if world == 1 and not args.no_kh:
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
+    if world == 1 and not args.no_gf:
+        extra["gf_map"] = gf_section(A, ctx)
     if world == 1 and not args.no_step512:
         extra["step512"] = step512_section(A, ctx)
     if world == 1 and not args.no_serving:

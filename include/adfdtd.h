@@ -161,27 +161,37 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
                  adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
                  int flags, adf_step_cb cb, void* user);
 
-/* GFMap of run_fdtd!(...; gf_map): a PVFromPin map (src/kernels/
- * extrapolation.jl:72-87).  p_pin, v_pin (nt_gf, nsrc, nrec) Float32 Julia
- * layout; i_src, i_rec 1-based transceiver indices (iSrc, iRec).          */
+/* GFMap of run_fdtd!(...; gf_map) (src/kernels/extrapolation.jl:36-87).
+ * Tensors are (nt_gf, n1, n2) Float32 in Julia layout; i_src/i_rec are
+ * 1-based transceiver indices (iSrc, iRec).
+ *   ADF_GF_PV_FROM_PIN  t = {p_pin, v_pin}, n1 = #iSrc, n2 = #iRec
+ *   ADF_GF_P_FROM_PIN   t = {pos, neg},     n1 = #iRec, n2 = #iSrc
+ *   ADF_GF_PV_FROM_PV   t = {pp, pv, vp, vv}, n1 = #iRec, n2 = #iSrc       */
+#define ADF_GF_PV_FROM_PIN 0
+#define ADF_GF_P_FROM_PIN 1
+#define ADF_GF_PV_FROM_PV 2
 typedef struct {
-  int64_t nt_gf, nsrc, nrec;
-  const float* p_pin;
-  const float* v_pin;
+  int kind;
+  int64_t nt_gf, n1, n2;
+  const float* t[4];
   const int64_t* i_src;
+  int64_t n_src;
   const int64_t* i_rec;
+  int64_t n_rec;
   double z0;
-  int discard;  /* 1: as the reference ships (extrapolation.jl:228-229 writes
-                   into slice copies, so the sources never change); 0: the
-                   documented intent, sources written into txs            */
+  int discard;  /* 1: as the reference ships (extrapolate! writes into slice
+                   copies, extrapolation.jl:215-216, 228-229, 246-247, so the
+                   sources never change); 0: the documented intent, the
+                   extrapolated samples are written into txs's sources     */
 } adf_gfmap;
 
 /* run_fdtd! with a gf_map (src/simulation.jl:542-557, forward.jl:123-128):
  * adf_run_fdtd plus, after v2vn! of each step it < nt, extrapolate!
- * (extrapolation.jl:220-235 -> extrapolate_pv_from_pin!, :139-170) on the
- * device: pin = (p_rec - z0 vn_rec)/2 over iRec (Float64), Float64 sums
- * over receivers and lags, p_src[it+1, iSrc] and vn_src[it+1, iSrc] set
- * before vn2v!.  txs->src[0] and txs->vn_src come back updated.            */
+ * (extrapolation.jl:204-249) on the device: rows it-T+1..it of the recorded
+ * p / v_n (T = min(it, nt_gf)), pin = (p_rec - z0 vn_rec)/2 in Float64 for
+ * the two *FromPin kinds, sums over receivers and lags accumulated in
+ * Float64, p_src[it+1, iSrc] and vn_src[it+1, iSrc] set before vn2v!.
+ * txs->src[0] and txs->vn_src come back updated.                          */
 int adf_run_fdtd_gf(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
                     adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
                     int flags, const adf_gfmap* gf, adf_step_cb cb, void* user);

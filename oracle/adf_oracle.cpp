@@ -506,31 +506,73 @@ inline void interp_trilinear(View& v, int c, int64_t it, const float* idx, const
   }
 }
 
-// extrapolate!(::PVFromPin) (extrapolation.jl:220-235) with
-// extrapolate_pv_from_pin! (extrapolation.jl:139-170) at step it
+// extrapolate! (extrapolation.jl:204-249) with its three kernels, step it
 void gf_extrapolate(const or_gfmap* g, or_txgrid* txs, int64_t nt, int64_t it) {
   const int64_t T = std::min(it, g->nt_gf);
   const int64_t t_off = it - T + 1;
-  pfor(0, g->nsrc, [&](int64_t s) {
-    double psum = 0.0, vsum = 0.0;  // Float32 zero promoted by the first Float64 add
-    for (int64_t r = 0; r < g->nrec; ++r) {
-      const int64_t col = g->i_rec[r] - 1;
-      for (int64_t tt = 1; tt <= T; ++tt) {
-        const int64_t gi = T - tt + 1;
-        const int64_t row = t_off + tt - 1;  // 1-based
-        const double pin = ((double)txs->rec[0][(row - 1) + nt * col] -
-                            (double)txs->vn_rec[(row - 1) + nt * col] * g->z0) / 2.0;
-        const size_t k = (size_t)(gi - 1) + (size_t)g->nt_gf * (size_t)(s + g->nsrc * r);
-        psum += (double)g->p_pin[k] * pin;
-        vsum += (double)g->v_pin[k] * pin;
+  auto pin = [&](int64_t row, int64_t col) {  // row 1-based, col 0-based
+    return ((double)txs->rec[0][(row - 1) + nt * col] -
+            (double)txs->vn_rec[(row - 1) + nt * col] * g->z0) / 2.0;
+  };
+  if (g->kind == 0) {  // PVFromPin, extrapolate_pv_from_pin! (:139-170)
+    pfor(0, g->n1, [&](int64_t s) {
+      double psum = 0.0, vsum = 0.0;  // Float32 zero promoted by the first Float64 add
+      for (int64_t r = 0; r < g->n2; ++r) {
+        const int64_t col = g->i_rec[r] - 1;
+        for (int64_t tt = 1; tt <= T; ++tt) {
+          const double pt = pin(t_off + tt - 1, col);
+          const size_t k = (size_t)(T - tt) + (size_t)g->nt_gf * (size_t)(s + g->n1 * r);
+          psum += (double)g->t[0][k] * pt;
+          vsum += (double)g->t[1][k] * pt;
+        }
       }
-    }
-    if (!g->discard) {
-      const int64_t col = g->i_src[s] - 1;
-      txs->src[0][it + nt * col] = (float)vsum;  // p_src <- v_pin-derived
-      txs->vn_src[it + nt * col] = (float)psum;  // vn_src <- p_pin-derived
-    }
-  });
+      if (!g->discard) {
+        const int64_t col = g->i_src[s] - 1;
+        txs->src[0][it + nt * col] = (float)vsum;  // p_src <- v_pin-derived
+        txs->vn_src[it + nt * col] = (float)psum;  // vn_src <- p_pin-derived
+      }
+    });
+  } else if (g->kind == 1) {  // PFromPin, extrapolate_p_from_pin (:172-193)
+    pfor(0, g->n2, [&](int64_t s) {
+      float pn[2];
+      for (int h = 0; h < 2; ++h) {
+        double sum = 0.0;
+        for (int64_t r = 0; r < g->n1; ++r) {
+          const int64_t col = g->i_rec[r] - 1;
+          for (int64_t tt = 1; tt <= T; ++tt) {
+            const size_t k = (size_t)(T - tt) + (size_t)g->nt_gf * (size_t)(r + g->n1 * s);
+            sum += (double)g->t[h][k] * pin(t_off + tt - 1, col);
+          }
+        }
+        pn[h] = (float)sum;  // out = zeros(Float32, nsrc)
+      }
+      if (!g->discard) {
+        const int64_t col = g->i_src[s] - 1;
+        txs->src[0][it + nt * col] = pn[0] - pn[1];
+        txs->vn_src[it + nt * col] = (float)((double)(pn[0] + pn[1]) / g->z0);
+      }
+    });
+  } else {  // PVFromPV, extrapolate_pv_from_pv (:91-137)
+    pfor(0, g->n2, [&](int64_t r) {
+      float psum = 0.0f, vsum = 0.0f;
+      for (int64_t m = 0; m < g->n1; ++m) {
+        const int64_t col = g->i_rec[m] - 1;
+        for (int64_t tt = 1; tt <= T; ++tt) {
+          const int64_t row = t_off + tt - 1;
+          const float p_t = txs->rec[0][(row - 1) + nt * col];
+          const float vn_t = txs->vn_rec[(row - 1) + nt * col];
+          const size_t k = (size_t)(T - tt) + (size_t)g->nt_gf * (size_t)(m + g->n1 * r);
+          psum += g->t[1][k] * p_t + g->t[0][k] * vn_t;  // pv*p + pp*vn
+          vsum += g->t[3][k] * p_t + g->t[2][k] * vn_t;  // vv*p + vp*vn
+        }
+      }
+      if (!g->discard) {
+        const int64_t col = g->i_src[r] - 1;
+        txs->src[0][it + nt * col] = vsum;
+        txs->vn_src[it + nt * col] = psum;
+      }
+    });
+  }
 }
 
 template <typename R>
@@ -932,9 +974,14 @@ int or_run_fdtd_gf(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp
                    const or_gfmap* gf, int nthreads) {
   if (!d || !field || !txs || !gf) return -1;
   if (start_step < 1 || stop_step > d->nt) return -1;
-  for (int64_t s = 0; s < gf->nsrc; ++s)
+  if (gf->kind < 0 || gf->kind > 2) return -1;
+  // output count and receiver columns per kind
+  const int64_t nout = gf->kind == 0 ? gf->n1 : gf->n2;
+  const int64_t nin = gf->kind == 0 ? gf->n2 : gf->n1;
+  if (gf->n_src != nout || gf->n_rec != nin) return -1;
+  for (int64_t s = 0; s < gf->n_src; ++s)
     if (gf->i_src[s] < 1 || gf->i_src[s] > txs->ntx) return -1;
-  for (int64_t r = 0; r < gf->nrec; ++r)
+  for (int64_t r = 0; r < gf->n_rec; ++r)
     if (gf->i_rec[r] < 1 || gf->i_rec[r] > txs->ntx) return -1;
   set_threads(nthreads);
   if (mode == OR_MODE_FP32)

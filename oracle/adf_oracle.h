@@ -108,22 +108,32 @@ int or_run_fdtd(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
                 const uint8_t* mask, int64_t start_step, int64_t stop_step, int mode,
                 int nthreads);
 
-/* In-loop GF extrapolation of run_fdtd!(...; gf_map) for a PVFromPin map
- * (src/kernels/extrapolation.jl:72-87, 139-170, 220-235; forward.jl:123-128):
- * after v2vn! of step it (< nt), pin = (p_rec[:, iRec] - z0*vn_rec[:, iRec])/2
- * (Float64, as Float32 traces times the Float64 z0 promote), and for every
- * source column s
- *   vsum = sum_r sum_tt v_pin[T-tt+1, s, r] * pin[it-T+tt, r]   (Float64)
- *   psum = the same with p_pin,   T = min(it, nt_gf),
- * stored as Float32 into p_src[it+1, iSrc[s]] = vsum and
- * vn_src[it+1, iSrc[s]] = psum before vn2v! distributes vn_src.  discard = 1
- * reproduces the shipped code, whose slice copies drop those writes.       */
+/* In-loop GF extrapolation of run_fdtd!(...; gf_map) (src/kernels/
+ * extrapolation.jl:36-87, 91-249; forward.jl:123-128), after v2vn! of each
+ * step it < nt, T = min(it, nt_gf), rows it-T+1..it of the traces:
+ *  kind 0 PVFromPin  t = {p_pin, v_pin} (nt_gf, nsrc, nrec), iRec -> nrec,
+ *    pin = (p_rec - z0*vn_rec)/2 (Float64); per s: psum/vsum = Float64 sums
+ *    of p_pin/v_pin[T-tt+1, s, r] * pin; p_src[it+1, iSrc[s]] = vsum,
+ *    vn_src[it+1, iSrc[s]] = psum (extrapolate_pv_from_pin!, :139-170).
+ *  kind 1 PFromPin   t = {pos, neg} (nt_gf, nrec, nsrc); pos[s], neg[s] =
+ *    Float64 sums of g[T-tt+1, r, s] * pin rounded to Float32;
+ *    p_src = pos - neg, vn_src = (pos + neg)/z0 (extrapolate_p_from_pin,
+ *    :172-193 and :237-249).
+ *  kind 2 PVFromPV   t = {pp, pv, vp, vv} (nt_gf, nm, nrec), iRec -> nm
+ *    columns of p_rec / vn_rec, per r: psum += pv*p + pp*vn, vsum += vv*p +
+ *    vp*vn (Float32 products and pair sum, accumulated sequentially in
+ *    Float32 as the reference does, :91-137); p_src[it+1, iSrc[r]] = vsum,
+ *    vn_src[it+1, iSrc[r]] = psum (:204-218).
+ * discard = 1 reproduces the shipped code, whose slice copies drop the
+ * writes.  i_src, i_rec are 1-based transceiver indices.                  */
 typedef struct {
-  int64_t nt_gf, nsrc, nrec;
-  const float* p_pin;    /* (nt_gf, nsrc, nrec) */
-  const float* v_pin;
-  const int64_t* i_src;  /* (nsrc), 1-based transceiver indices */
-  const int64_t* i_rec;  /* (nrec), 1-based */
+  int kind;
+  int64_t nt_gf, n1, n2;  /* tensor dims (nt_gf, n1, n2) */
+  const float* t[4];
+  const int64_t* i_src;
+  int64_t n_src;
+  const int64_t* i_rec;
+  int64_t n_rec;
   double z0;
   int discard;
 } or_gfmap;

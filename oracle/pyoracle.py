@@ -59,9 +59,13 @@ class _Cpml(C.Structure):
 
 
 class _GfMap(C.Structure):
-    _fields_ = [("nt_gf", C.c_int64), ("nsrc", C.c_int64), ("nrec", C.c_int64),
-                ("p_pin", C.c_void_p), ("v_pin", C.c_void_p), ("i_src", C.c_void_p),
-                ("i_rec", C.c_void_p), ("z0", C.c_double), ("discard", C.c_int)]
+    _fields_ = [("kind", C.c_int), ("nt_gf", C.c_int64), ("n1", C.c_int64), ("n2", C.c_int64),
+                ("t", C.c_void_p * 4), ("i_src", C.c_void_p), ("n_src", C.c_int64),
+                ("i_rec", C.c_void_p), ("n_rec", C.c_int64), ("z0", C.c_double),
+                ("discard", C.c_int)]
+
+
+GF_KINDS = {"PVFromPin": 0, "PFromPin": 1, "PVFromPV": 2}
 
 
 def lib():
@@ -324,21 +328,23 @@ def run_fdtd(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask=None, start_st
     return field
 
 
-def run_fdtd_gf(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask, p_pin, v_pin, i_src,
+def run_fdtd_gf(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask, kind, tensors, i_src,
                 i_rec, z0, discard=False, start_step=1, stop_step=None, mode="promote",
                 nthreads=0):
-    """run_fdtd!(...; gf_map = PVFromPin(p_pin, v_pin) with iSrc/iRec): the in-loop
-    GF extrapolation (extrapolation.jl:139-170, 220-235).  p_pin, v_pin are
-    (nt_gf, nsrc, nrec) float32; i_src, i_rec 1-based transceiver indices."""
+    """run_fdtd!(...; gf_map) with the in-loop GF extrapolation
+    (extrapolation.jl:36-249).  kind: "PVFromPin" (tensors p_pin, v_pin),
+    "PFromPin" (pos, neg) or "PVFromPV" (pp, pv, vp, vv), each (nt_gf, n1, n2)
+    float32; i_src, i_rec 1-based transceiver indices."""
     stop_step = d.nt if stop_step is None else stop_step
     assert field.flags.f_contiguous and field.dtype == np.float32
-    pp = np.asfortranarray(p_pin, np.float32)
-    vp = np.asfortranarray(v_pin, np.float32)
+    ts = [np.asfortranarray(t, np.float32) for t in tensors]
     isr = np.ascontiguousarray(i_src, np.int64)
     irc = np.ascontiguousarray(i_rec, np.int64)
-    g = _GfMap(nt_gf=pp.shape[0], nsrc=pp.shape[1], nrec=pp.shape[2], p_pin=pp.ctypes.data,
-               v_pin=vp.ctypes.data, i_src=isr.ctypes.data, i_rec=irc.ctypes.data, z0=z0,
-               discard=int(bool(discard)))
+    g = _GfMap(kind=GF_KINDS[kind], nt_gf=ts[0].shape[0], n1=ts[0].shape[1], n2=ts[0].shape[2],
+               i_src=isr.ctypes.data, n_src=isr.size, i_rec=irc.ctypes.data, n_rec=irc.size,
+               z0=z0, discard=int(bool(discard)))
+    for k, t in enumerate(ts):
+        g.t[k] = t.ctypes.data
     cg = txs._c()
     cc = cpml._c() if cpml is not None else None
     _chk(lib().or_run_fdtd_gf(C.byref(d), _p(field), C.byref(cg), C.byref(cc) if cc else None,
