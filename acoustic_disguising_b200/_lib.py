@@ -81,6 +81,7 @@ class KhDescC(C.Structure):
         ("dt", C.c_double), ("sigma", C.c_double), ("c0", C.c_double), ("rho", C.c_double),
         ("aq", C.c_double), ("af", C.c_double), ("window_sigmas", C.c_double),
         ("s_pts", C.c_void_p), ("s_nrm", C.c_void_p), ("r_pts", C.c_void_p),
+        ("r_nrm", C.c_void_p),
     ]
 
 
@@ -139,6 +140,8 @@ SIGNATURES = [
     ("adf_server_drain", C.c_int, [C.c_void_p]),
     ("adf_server_stop", C.c_int, [C.c_void_p]),
     ("adf_kh_pressure", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
+    ("adf_kh_velocity", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("adf_injection_coefficients", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_double,

@@ -472,6 +472,30 @@ def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt: float, sigma: float, c0: fl
     return out
 
 
+def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt: float, sigma: float, c0: float,
+                aq: float, af: float, rho: float = 1.2, window_sigmas: float = 6.0,
+                ctx: Context | None = None) -> np.ndarray:
+    """Two-way KH normal velocity at targets with normals r_nrm:
+    out[t, r] = aq sum_s v_p(s,r) (*) in_q[:, s] + af sum_s v_v(s,r) (*) in_f[:, s]
+    (eval_one_kernel's v_p, v_v, kh_kernels.jl:106-157; the non-decaying part
+    of v_v is carried as its limit times the running sum of in_f)."""
+    ctx = ctx or default_context()
+    f64 = lambda a: np.asfortranarray(a, np.float64)
+    f32 = lambda a: np.asfortranarray(a, np.float32)
+    sp, sn, rp, rn = f64(s_pts), f64(s_nrm), f64(r_pts), f64(r_nrm)
+    q, f = f32(in_q), f32(in_f)
+    ns, nr, nt = sp.shape[0], rp.shape[0], q.shape[0]
+    if (sn.shape != (ns, 3) or rp.shape[1] != 3 or rn.shape != rp.shape or
+            q.shape != (nt, ns) or f.shape != (nt, ns)):
+        raise ValueError("kh_velocity: shape mismatch")
+    desc = L.KhDescC(ns=ns, nr=nr, nt=nt, dt=dt, sigma=sigma, c0=c0, rho=rho, aq=aq, af=af,
+                     window_sigmas=window_sigmas, s_pts=sp.ctypes.data, s_nrm=sn.ctypes.data,
+                     r_pts=rp.ctypes.data, r_nrm=rn.ctypes.data)
+    out = np.zeros((nt, nr), np.float32, order="F")
+    L.check(L.lib().adf_kh_velocity(ctx.h, C.byref(desc), _p(q), _p(f), _p(out)), "kh_velocity")
+    return out
+
+
 def fp32_fma_peak(ctx: Context | None = None):
     """Measured FP32 FMA throughput (TFLOP/s) and the probe's duration (ms)."""
     ctx = ctx or default_context()

@@ -70,23 +70,31 @@ struct KhParams {
   long long pitch;  // floats per padded input column (multiple of 4)
   double inv_c0dt;  // 1 / (c0 dt)
   double hw;        // window half width in samples
-  double cq;        // -aq C dt / sigma^2            (C = 1/(sqrt(2 pi) sigma))
-  double cf1;       //  af C
-  double cf2;       // -af C dt / (sigma^2 c0)
+  double aq, af;    // channel scales
+  double C;         // 1 / (sqrt(2 pi) sigma)
+  double dts2;      // dt / sigma^2
+  double c0, inv_rho;
   float a;          // dt^2 / (2 sigma^2)
+  float dt_sigma;   // dt / sigma (argument scale of the Gaussian CDF)
   const double* sp;  // (ns,3) column-major
   const double* sn;
   const double* rp;  // (nr,3)
+  const double* rn;  // (nr,3) target normals (velocity output)
   const int2* tile_lo;  // per target tile: {lo_min, lo_max}
   const float* in_q;    // (pitch, ns): zero-padded columns, sample t at pad + t
   const float* in_f;
+  const float* cs_f;    // running sum of in_f, same layout (velocity output)
   float* out;           // (nt, nr)
   int* err;
 };
 
 }  // namespace
 
-template <int LM>
+// KIND 0: pressure (p_p on in_q, p_v on in_f).  KIND 1: normal velocity
+// (v_p on in_q, v_v on in_f); v_v's Gaussian-CDF term tends to a constant,
+// so beyond each pair's window it is that constant times the running sum of
+// in_f (staged as a third row per surface point).
+template <int LM, int KIND>
 __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams p) {
   constexpr int XN = KH_T + LM - 1;
   extern __shared__ __align__(128) float smem[];
@@ -103,13 +111,16 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
   const int shift = col0 & 3;
   const float* colq = p.in_q + (col0 - shift);
   const float* colf = p.in_f + (col0 - shift);
+  const float* colc = KIND ? p.cs_f + (col0 - shift) : nullptr;
   const int npair = KH_RT * p.sc;
+  constexpr int NROW = KIND ? 3 : 2;  // staged rows per surface point
+  constexpr int NPAR = 8;             // lo, n, wb, 5 coefficients
 
-  // shared memory: 2 window buffers [sc][2][rowpad], 2 pair-parameter
-  // buffers [6][RT*sc], per-warp taps [warps][RW][LM][2]
-  const int wbuf = p.sc * 2 * p.rowpad;
+  // shared memory: 2 window buffers [sc][NROW][rowpad], 2 pair-parameter
+  // buffers [NPAR][RT*sc], per-warp taps [warps][RW][LM][2]
+  const int wbuf = p.sc * NROW * p.rowpad;
   float* const par0 = smem + 2 * wbuf;
-  float* taps = par0 + 12 * npair;
+  float* taps = par0 + 2 * NPAR * npair;
   float* my_taps = taps + warp * (KH_RW * 2 * LM);
 
   const int nchunks = (p.ns + p.sc - 1) / p.sc;
@@ -128,30 +139,30 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     const uint32_t row_bytes = (uint32_t)p.rowpad * 4u;
     // the buffer's previous contents were read through the generic proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(mb, row_bytes * 2u * (uint32_t)nsc);
+    mbar_expect_tx(mb, row_bytes * (uint32_t)NROW * (uint32_t)nsc);
     float* w = smem + (c & 1) * wbuf;
     for (int sl = 0; sl < nsc; ++sl) {
       const size_t off = (size_t)(s0 + sl) * p.pitch;
-      bulk_load(smem_u32(w + (size_t)(2 * sl) * p.rowpad), colq + off, row_bytes, mb);
-      bulk_load(smem_u32(w + (size_t)(2 * sl + 1) * p.rowpad), colf + off, row_bytes, mb);
+      bulk_load(smem_u32(w + (size_t)(NROW * sl) * p.rowpad), colq + off, row_bytes, mb);
+      bulk_load(smem_u32(w + (size_t)(NROW * sl + 1) * p.rowpad), colf + off, row_bytes, mb);
+      if (KIND)
+        bulk_load(smem_u32(w + (size_t)(NROW * sl + 2) * p.rowpad), colc + off, row_bytes, mb);
     }
   };
   // pair geometry of chunk c in FP64 (all threads)
   auto params = [&](int c) {
     const int s0 = c * p.sc;
     const int nsc = min(p.sc, p.ns - s0);
-    float* pb = par0 + (c & 1) * 6 * npair;
+    float* pb = par0 + (c & 1) * NPAR * npair;
     int* pr_lo = reinterpret_cast<int*>(pb);
     int* pr_n = pr_lo + npair;
     float* pr_wb = pb + 2 * npair;
-    float* pr_q = pb + 3 * npair;
-    float* pr_f1 = pb + 4 * npair;
-    float* pr_f2 = pb + 5 * npair;
+    float* pr_c = pb + 3 * npair;  // 5 coefficient arrays
     for (int idx = threadIdx.x; idx < KH_RT * nsc; idx += KH_THREADS) {
       const int rr = idx % KH_RT, sl = idx / KH_RT;
       const int r = r_base + rr, s = s0 + sl;
       int lo = lo_max, n = 0;
-      float wb = 0.f, q = 0.f, f1 = 0.f, f2 = 0.f;
+      float wb = 0.f, k0 = 0.f, k1 = 0.f, k2 = 0.f, k3 = 0.f, k4 = 0.f;
       if (r < p.nr) {
         const double dx = p.rp[r] - p.sp[s];
         const double dy = p.rp[r + p.nr] - p.sp[s + p.ns];
@@ -172,9 +183,24 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
             const double i1 = 1.0 / (4.0 * M_PI * d);
             const double i2 = 1.0 / (4.0 * M_PI * (d * d));
             wb = (float)((double)l - u);
-            q = (float)(p.cq * i1);
-            f1 = (float)(p.cf1 * cs * i2);
-            f2 = (float)(p.cf2 * cs * i1);
+            // taps, w = k - delay in samples, e = exp(-a w^2):
+            //   KIND 0: q = k0 w e,          f = (k1 + k2 w) e
+            //   KIND 1: q = (k0 + k1 w) e,   f = (k2 + k3 w) e + k4 F(w dt)
+            if (KIND == 0) {
+              k0 = (float)(-p.aq * p.C * p.dts2 * i1);                 // p_p
+              k1 = (float)(p.af * p.C * cs * i2);                      // p_v
+              k2 = (float)(-p.af * p.C * p.dts2 / p.c0 * cs * i1);
+            } else {
+              const double cr =
+                  (p.rn[r] * dx + p.rn[r + p.nr] * dy + p.rn[r + 2 * p.nr] * dz) / d;
+              const double i3 = 1.0 / (4.0 * M_PI * (d * d * d));
+              const double qr = p.aq * cr * p.inv_rho, fr = p.af * cr * cs * p.inv_rho;
+              k0 = (float)(qr * p.C * i2);                              // v_p
+              k1 = (float)(-qr * p.C * p.dts2 / p.c0 * i1);
+              k2 = (float)(fr * p.C * 2.0 * i2 / p.c0);                 // v_v
+              k3 = (float)(-fr * p.C * p.dts2 / (p.c0 * p.c0) * i1);
+              k4 = (float)(fr * 2.0 * i3);                              // F term, pedestal
+            }
           }
         }
       }
@@ -182,9 +208,11 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
       pr_lo[pi] = lo;
       pr_n[pi] = n;
       pr_wb[pi] = wb;
-      pr_q[pi] = q;
-      pr_f1[pi] = f1;
-      pr_f2[pi] = f2;
+      pr_c[pi] = k0;
+      pr_c[npair + pi] = k1;
+      pr_c[2 * npair + pi] = k2;
+      pr_c[3 * npair + pi] = k3;
+      pr_c[4 * npair + pi] = k4;
     }
   };
 
@@ -211,15 +239,13 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     }
     const int nsc = min(p.sc, p.ns - c * p.sc);
     const float* win = smem + (c & 1) * wbuf + shift;
-    const float* pb = par0 + (c & 1) * 6 * npair;
+    const float* pb = par0 + (c & 1) * NPAR * npair;
     const int* pr_lo = reinterpret_cast<const int*>(pb);
     const int* pr_n = pr_lo + npair;
     const float* pr_wb = pb + 2 * npair;
-    const float* pr_q = pb + 3 * npair;
-    const float* pr_f1 = pb + 4 * npair;
-    const float* pr_f2 = pb + 5 * npair;
+    const float* pr_c = pb + 3 * npair;
     for (int sl = 0; ok && sl < nsc; ++sl) {
-      const float* wq = win + (size_t)(2 * sl) * p.rowpad;
+      const float* wq = win + (size_t)(NROW * sl) * p.rowpad;
       const float* wf = wq + p.rowpad;
       // taps of this warp's targets: lane-parallel, one exp per tap
 #pragma unroll
@@ -232,7 +258,15 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
           const int kp = kk % LM;
           const float w = wb + (float)kp;
           const float e = expf(-p.a * (w * w));
-          const float v = kk < LM ? pr_q[pi] * w * e : (pr_f1[pi] + pr_f2[pi] * w) * e;
+          float v;
+          if (KIND == 0) {
+            v = kk < LM ? pr_c[pi] * w * e : (pr_c[npair + pi] + pr_c[2 * npair + pi] * w) * e;
+          } else if (kk < LM) {
+            v = (pr_c[pi] + pr_c[npair + pi] * w) * e;
+          } else {
+            v = (pr_c[2 * npair + pi] + pr_c[3 * npair + pi] * w) * e +
+                pr_c[4 * npair + pi] * normcdff(w * p.dt_sigma);
+          }
           // interleaved {monopole, dipole} per tap for the paired FMA
           my_taps[rho * 2 * LM + 2 * kp + (kk >= LM)] = kp < n ? v : 0.f;
         }
@@ -258,6 +292,13 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
           for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(ta, x2[j + LM - 1 - 2 * k2], c2[j]);
 #pragma unroll
           for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(tb2, x2[j + LM - 2 - 2 * k2], c2[j]);
+        }
+        if (KIND == 1) {  // lags past the window: v_v's constant times the running sum
+          const float ped = pr_c[4 * npair + pi];
+          const float* wc = wq + 2 * p.rowpad;
+          const int cb = base + LM - 1 - pr_n[pi];
+#pragma unroll
+          for (int j = 0; j < KH_T; ++j) c2[j].y = __fmaf_rn(ped, wc[cb + j], c2[j].y);
         }
         // compensated accumulation over surface points
 #pragma unroll
@@ -322,10 +363,13 @@ struct DevBuf {
 
 using namespace adf;
 
-extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q,
-                               const float* in_f, float* out) {
+// kind 0: pressure, kind 1: normal velocity (adf_kh_pressure / adf_kh_velocity)
+static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const float* in_f,
+                  float* out, int kind) {
   if (!ctx || !d || !in_q || !in_f || !out || !d->s_pts || !d->s_nrm || !d->r_pts)
     return fail(ADF_E_ARG, "adf_kh_pressure: null argument");
+  if (kind == 1 && (!d->r_nrm || !(d->rho > 0)))
+    return fail(ADF_E_ARG, "adf_kh_velocity: target normals and a positive rho are required");
   if (d->ns < 1 || d->nr < 1 || d->nt < 1 || !(d->dt > 0) || !(d->sigma > 0) || !(d->c0 > 0))
     return fail(ADF_E_ARG, "adf_kh_pressure: ns, nr, nt, dt, sigma and c0 must be positive");
   if (d->ns > (1 << 30) || d->nr > (1 << 30) || d->nt > (1 << 28))
@@ -384,7 +428,9 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
   // multiple of 4 floats, so every bulk copy and the tap buffer stay aligned.
   const int rowpad = (wmax + 3 + 3) / 4 * 4;
   const size_t tap_bytes = (size_t)KH_WARPS * KH_RW * 2 * lm * 4;
-  const size_t per_s = 2 * ((size_t)2 * rowpad * 4 + (size_t)6 * KH_RT * 4);  // double-buffered
+  const int nrow = kind ? 3 : 2;  // staged rows per surface point
+  // double-buffered windows and pair parameters (lo, n, wb, 5 coefficients)
+  const size_t per_s = 2 * ((size_t)nrow * rowpad * 4 + (size_t)8 * KH_RT * 4);
   const size_t smem_cap = (size_t)ctx->smem_optin - 256;  // static mbarriers
   int sc = KH_SC_MAX;
   while (sc > 1 && per_s * sc + tap_bytes > smem_cap) --sc;
@@ -399,15 +445,27 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
     return fail(ADF_E_ARG, "adf_kh_pressure: the targets' delay spread needs a " +
                                std::to_string(wmax) + "-sample window, more than shared memory holds");
 
-  DevBuf<double> dsp, dsn, drp;
-  DevBuf<float> dq, df, dout;
+  DevBuf<double> dsp, dsn, drp, drn;
+  DevBuf<float> dq, df, dc, dout;
   DevBuf<int2> dtlo;
   DevBuf<int> derr;
   if (!dsp.alloc((size_t)3 * ns) || !dsn.alloc((size_t)3 * ns) || !drp.alloc((size_t)3 * nr) ||
       !dq.alloc((size_t)pitch * ns) || !df.alloc((size_t)pitch * ns) ||
       !dout.alloc((size_t)nt * nr) ||
-      !dtlo.alloc((size_t)ntiles) || !derr.alloc(1))
+      !dtlo.alloc((size_t)ntiles) || !derr.alloc(1) ||
+      (kind && (!drn.alloc((size_t)3 * nr) || !dc.alloc((size_t)pitch * ns))))
     return fail(ADF_E_NOMEM, "adf_kh_pressure: device allocation failed");
+  std::vector<float> csum;
+  if (kind) {  // running sum of in_f per surface point, in Float64, stored Float32
+    csum.resize((size_t)nt * ns);
+    for (int s = 0; s < ns; ++s) {
+      double a = 0.0;
+      for (int t = 0; t < nt; ++t) {
+        a += (double)in_f[(size_t)s * nt + t];
+        csum[(size_t)s * nt + t] = (float)a;
+      }
+    }
+  }
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(dsp.p, d->s_pts, (size_t)24 * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(dsn.p, d->s_nrm, (size_t)24 * ns, cudaMemcpyHostToDevice, st);
@@ -418,6 +476,12 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
                     cudaMemcpyHostToDevice, st);
   cudaMemcpy2DAsync(df.p + pad, (size_t)4 * pitch, in_f, (size_t)4 * nt, (size_t)4 * nt, ns,
                     cudaMemcpyHostToDevice, st);
+  if (kind) {
+    cudaMemcpyAsync(drn.p, d->r_nrm, (size_t)24 * nr, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(dc.p, 0, (size_t)4 * pitch * ns, st);
+    cudaMemcpy2DAsync(dc.p + pad, (size_t)4 * pitch, csum.data(), (size_t)4 * nt,
+                      (size_t)4 * nt, ns, cudaMemcpyHostToDevice, st);
+  }
   cudaMemcpyAsync(dtlo.p, tlo.data(), sizeof(int2) * ntiles, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(derr.p, 0, sizeof(int), st);
 
@@ -429,25 +493,35 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
   p.hw = hw;
   const double C = 1.0 / (std::sqrt(2.0 * M_PI) * d->sigma);
   const double s2 = d->sigma * d->sigma;
-  p.cq = -d->aq * C * d->dt / s2;
-  p.cf1 = d->af * C;
-  p.cf2 = -d->af * C * d->dt / (s2 * d->c0);
+  p.aq = d->aq;
+  p.af = d->af;
+  p.C = C;
+  p.dts2 = d->dt / s2;
+  p.c0 = d->c0;
+  p.inv_rho = kind ? 1.0 / d->rho : 0.0;
   p.a = (float)(d->dt * d->dt / (2.0 * s2));
-  p.sp = dsp.p; p.sn = dsn.p; p.rp = drp.p;
+  p.dt_sigma = (float)(d->dt / d->sigma);
+  p.sp = dsp.p; p.sn = dsn.p; p.rp = drp.p; p.rn = drn.p;
   p.tile_lo = dtlo.p;
-  p.in_q = dq.p; p.in_f = df.p; p.out = dout.p;
+  p.in_q = dq.p; p.in_f = df.p; p.cs_f = dc.p; p.out = dout.p;
   p.err = derr.p;
 
-  const void* fn = lm == 16 ? (const void*)adf_kh_pressure_kernel<16>
-                            : (const void*)adf_kh_pressure_kernel<32>;
+  const void* fn = lm == 16 ? (kind ? (const void*)adf_kh_pressure_kernel<16, 1>
+                                    : (const void*)adf_kh_pressure_kernel<16, 0>)
+                            : (kind ? (const void*)adf_kh_pressure_kernel<32, 1>
+                                    : (const void*)adf_kh_pressure_kernel<32, 0>);
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("kh smem: ") + cudaGetErrorString(e));
   const dim3 grid((unsigned)ntiles, (unsigned)((nt + KH_TB - 1) / KH_TB));
   cudaEventRecord(ctx->ev0, st);
-  if (lm == 16)
-    adf_kh_pressure_kernel<16><<<grid, KH_THREADS, smem, st>>>(p);
+  if (lm == 16 && !kind)
+    adf_kh_pressure_kernel<16, 0><<<grid, KH_THREADS, smem, st>>>(p);
+  else if (lm == 16)
+    adf_kh_pressure_kernel<16, 1><<<grid, KH_THREADS, smem, st>>>(p);
+  else if (!kind)
+    adf_kh_pressure_kernel<32, 0><<<grid, KH_THREADS, smem, st>>>(p);
   else
-    adf_kh_pressure_kernel<32><<<grid, KH_THREADS, smem, st>>>(p);
+    adf_kh_pressure_kernel<32, 1><<<grid, KH_THREADS, smem, st>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("kh launch: ") + cudaGetErrorString(e));
   cudaEventRecord(ctx->ev1, st);
@@ -460,10 +534,21 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_ms = ms;
   ctx->launches = 1;
-  ctx->h2d_bytes = (int64_t)48 * ns + 24 * (int64_t)nr + (int64_t)8 * nt * ns;
+  ctx->h2d_bytes = (int64_t)48 * ns + (kind ? 48 : 24) * (int64_t)nr +
+                   (int64_t)(kind ? 12 : 8) * nt * ns;
   ctx->d2h_bytes = (int64_t)4 * nt * nr;
   if (herr) return fail(ADF_E_STATE, "adf_kh_pressure: a pair's delay fell outside its tile bound");
   return ADF_OK;
+}
+
+extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q,
+                               const float* in_f, float* out) {
+  return kh_run(ctx, d, in_q, in_f, out, 0);
+}
+
+extern "C" int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q,
+                               const float* in_f, float* out) {
+  return kh_run(ctx, d, in_q, in_f, out, 1);
 }
 
 extern "C" int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms_out) {

@@ -288,8 +288,19 @@ typedef struct {
   const double* s_pts;
   const double* s_nrm;
   const double* r_pts;
+  const double* r_nrm;       /* (nr,3) target normals, adf_kh_velocity only */
 } adf_kh_desc;
 int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
+                    const float* in_f, float* out);
+/* Two-way KH normal velocity at targets (part3_kh_extrapolation.jl:151,
+ * 180-265): out[t,r] = aq * sum_s v_p(s,r) (*) in_q[:,s]
+ *                    + af * sum_s v_v(s,r) (*) in_f[:,s]
+ * with v_p, v_v of eval_one_kernel (kh_kernels.jl:106-157).  v_v's
+ * Gaussian-CDF term does not decay; beyond each pair's window it is added
+ * as its limit times the running sum of in_f (the K_dc pedestal of
+ * direct_kh_accumulate!, kh_kernels.jl:256-296), so the result is the
+ * convolution with the untruncated kernel.  Needs desc->r_nrm and rho.    */
+int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
                     const float* in_f, float* out);
 
 /* Measured FP32 FMA throughput of the device (TFLOP/s, 2 FLOP per FMA): the

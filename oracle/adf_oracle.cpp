@@ -1131,6 +1131,67 @@ int or_kh_pressure(int64_t ns, const double* sp, const double* sn, int64_t nr,
   return 0;
 }
 
+int or_kh_velocity(int64_t ns, const double* sp, const double* sn, int64_t nr,
+                   const double* rp, const double* rn, int64_t nt, double dt, double sg,
+                   double c0, double rho, const float* in_q, const float* in_f, double aq,
+                   double af, int64_t r0, int64_t r1, double* out, int nthreads) {
+  if (r0 < 0 || r1 > nr || r1 < r0 || nt < 1) return -1;
+  set_threads(nthreads);
+  const int64_t nrr = r1 - r0;
+  // running sums of in_f per surface point (FP64): cs[t] = sum_{j <= t} in_f[j]
+  std::vector<double> cs((size_t)(nt * ns));
+  for (int64_t s = 0; s < ns; ++s) {
+    double a = 0.0;
+    for (int64_t t = 0; t < nt; ++t) {
+      a += (double)in_f[t + nt * s];
+      cs[(size_t)(t + nt * s)] = a;
+    }
+  }
+  pfor(0, nrr, [&](int64_t rr) {
+    const int64_t ir = r0 + rr;
+    double* o = out + nt * rr;
+    for (int64_t t = 0; t < nt; ++t) o[t] = 0.0;
+    std::vector<double> kq, kf;
+    for (int64_t is = 0; is < ns; ++is) {
+      const double dx = rp[ir] - sp[is], dy = rp[ir + nr] - sp[is + ns],
+                   dz = rp[ir + 2 * nr] - sp[is + 2 * ns];
+      const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double ihx = dx / r, ihy = dy / r, ihz = dz / r;
+      const double cr = rn[ir] * ihx + rn[ir + nr] * ihy + rn[ir + 2 * nr] * ihz;
+      const double cs_ = sn[is] * ihx + sn[is + ns] * ihy + sn[is + 2 * ns] * ihz;
+      const double retard = r / c0;
+      const double i1 = 1 / (4 * M_PI * r), i2 = 1 / (4 * M_PI * (r * r)),
+                   i3 = 1 / (4 * M_PI * (r * r * r));
+      const int64_t lo = std::max<int64_t>(0, (int64_t)std::floor((retard - 12 * sg) / dt));
+      const int64_t hi = (int64_t)std::ceil((retard + 12 * sg) / dt);
+      kq.assign((size_t)(hi - lo + 1), 0.0);
+      kf.assign((size_t)(hi - lo + 1), 0.0);
+      for (int64_t k = lo; k <= hi; ++k) {
+        const double tau = (double)k * dt - retard;
+        const double f = kh_fg(tau, sg), df = kh_dfg(tau, sg), F = kh_Fg(tau, sg);
+        kq[(size_t)(k - lo)] = (cr / rho) * (f * i2 + df * i1 / c0);  // v_p
+        kf[(size_t)(k - lo)] =
+            (cr * cs_ / rho) * (2 * F * i3 + 2 * f * i2 / c0 + df * i1 / (c0 * c0));  // v_v
+      }
+      const double ped = (cr * cs_ / rho) * 2 * i3;  // v_v for tau -> inf
+      const float* q = in_q + nt * is;
+      const float* fs = in_f + nt * is;
+      for (int64_t t = 0; t < nt; ++t) {
+        double aq_s = 0.0, af_s = 0.0;
+        const int64_t kmax = std::min(hi, t);
+        for (int64_t k = lo; k <= kmax; ++k) {
+          aq_s += kq[(size_t)(k - lo)] * (double)q[t - k];
+          af_s += kf[(size_t)(k - lo)] * (double)fs[t - k];
+        }
+        // lags k > hi: the kernel is its tau -> inf value
+        if (t - hi - 1 >= 0) af_s += ped * cs[(size_t)(t - hi - 1 + nt * is)];
+        o[t] += aq * aq_s + af * af_s;
+      }
+    }
+  });
+  return 0;
+}
+
 // extrapolate_pv_from_pin! (extrapolation.jl:139-170)
 int or_extrapolate_pv_from_pin(const float* pin, int64_t nt, int64_t nrec, float* p_src,
                                float* v_src, int64_t nsrc, const float* pp, const float* vp,

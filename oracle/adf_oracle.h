@@ -165,6 +165,21 @@ int or_kh_pressure(int64_t ns, const double* s_pts, const double* s_nrm, int64_t
                    double c0, const float* in_q, const float* in_f, double aq, double af,
                    int mode, int64_t r_begin, int64_t r_end, double* out, int nthreads);
 
+/* Two-way KH normal velocity at targets (part3_kh_extrapolation.jl:151,
+ * 180-265): out[t, r] = aq*sum_s v_p(s,r) (*) in_q[., s]
+ *                    + af*sum_s v_v(s,r) (*) in_f[., s]
+ * with v_p, v_v of eval_one_kernel (kh_kernels.jl:106-157) in FP64: taps
+ * within +-12 sigma of the delay, plus, for the non-decaying F-term of v_v
+ * (its tau -> inf value (cos_r cos_s / rho) 2/(4 pi d^3)), that value times
+ * the running sum of in_f beyond the window, which makes the sum equal to
+ * the convolution with the full, untruncated kernel.  r_nrm (nr,3) are the
+ * target normals.  Targets [r_begin, r_end); out (nt, r_end-r_begin).     */
+int or_kh_velocity(int64_t ns, const double* s_pts, const double* s_nrm, int64_t nr,
+                   const double* r_pts, const double* r_nrm, int64_t nt, double dt,
+                   double sigma, double c0, double rho, const float* in_q, const float* in_f,
+                   double aq, double af, int64_t r_begin, int64_t r_end, double* out,
+                   int nthreads);
+
 /* extrapolate_pv_from_pin! (src/kernels/extrapolation.jl:139-170), 1-based it.
  * pin (nt, nrec), p_src/v_src (nt, nsrc), pp/vp (nt_gf, nsrc, nrec).      */
 int or_extrapolate_pv_from_pin(const float* pin, int64_t nt, int64_t nrec, float* p_src,

@@ -104,6 +104,10 @@ def lib():
                                      C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
                                      C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int,
                                      C.c_int64, C.c_int64, C.c_void_p, C.c_int]
+        L.or_kh_velocity.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                     C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                     C.c_int64, C.c_int64, C.c_void_p, C.c_int]
         L.or_extrapolate_pv_from_pin.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                                  C.c_int64, C.c_int64]
@@ -388,6 +392,22 @@ def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt, sigma, c0, aq, af, ntk=None
     _chk(lib().or_kh_pressure(ns, _p(f(s_pts)), _p(f(s_nrm)), nr, _p(f(r_pts)), nt, ntk, dt,
                               sigma, c0, _p(g(in_q)), _p(g(in_f)), aq, af, mode, r_begin, r_end,
                               _p(out), nthreads), "kh_pressure")
+    return out
+
+
+def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt, sigma, c0, rho, aq, af, r_begin=0,
+                r_end=None, nthreads=0):
+    """FP64 oracle of the two-way KH normal velocity (v_p, v_v kernels with the
+    v_v pedestal); in_q/in_f are (nt, ns) Float32."""
+    ns, nr = s_pts.shape[0], r_pts.shape[0]
+    nt = in_q.shape[0]
+    r_end = nr if r_end is None else r_end
+    out = np.zeros((nt, r_end - r_begin), np.float64, order="F")
+    f = lambda a: np.asfortranarray(a, np.float64)
+    g = lambda a: np.asfortranarray(a, np.float32)
+    _chk(lib().or_kh_velocity(ns, _p(f(s_pts)), _p(f(s_nrm)), nr, _p(f(r_pts)), _p(f(r_nrm)), nt,
+                              dt, sigma, c0, rho, _p(g(in_q)), _p(g(in_f)), aq, af, r_begin, r_end,
+                              _p(out), nthreads), "kh_velocity")
     return out
 
 

@@ -103,3 +103,30 @@ def test_fp32_fma_peak_is_plausible(adf, ctx):
     # 148 SMs x 128 FP32 lanes x 2 FLOP at 1-2 GHz
     assert 20.0 < tf < 90.0, tf
     assert ms > 0
+
+
+def run_velocity(adf, oracle, c, seed=9):
+    rng = np.random.default_rng(seed)
+    rn = rng.standard_normal(c["rp"].shape)
+    rn /= np.linalg.norm(rn, axis=1, keepdims=True)
+    aq, af = -RHO * 1e-9, -1e-9  # the two-way vn form's scales, up to dS dt
+    out = adf.kh_velocity(c["sp"], c["sn"], c["rp"], rn, c["q"], c["f"], c["dt"], c["sigma"], C0,
+                          aq, af, rho=RHO)
+    ref = oracle.kh_velocity(c["sp"], c["sn"], c["rp"], rn, c["q"], c["f"], c["dt"], c["sigma"],
+                             C0, RHO, aq, af)
+    return out, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ns,nr,nt,dt,r_surf,r_tgt", [
+    (256, 96, 1024, 5e-6, 0.25, 1.0),     # far field
+    (128, 64, 900, 5e-6, 0.25, 0.30),     # near field: the 1/r^3 pedestal of v_v is large
+    (45, 50, 1001, 5e-6, 0.25, 0.8),      # ragged sizes
+    (64, 40, 1500, 2.5e-6, 0.25, 0.6),    # 32-tap window
+])
+def test_kh_velocity_matches_fp64_oracle(adf, oracle, ctx, ns, nr, nt, dt, r_surf, r_tgt):
+    c = case(ns, nr, nt, dt, r_surf, r_tgt)
+    out, ref = run_velocity(adf, oracle, c)
+    assert np.isfinite(out).all()
+    assert np.abs(ref).max() > 0
+    assert rel_l2(out, ref) <= RTOL_L2

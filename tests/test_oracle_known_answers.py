@@ -149,3 +149,51 @@ def test_fibonacci_and_wavelets(oracle):
     tt = oracle.time_axis(d)
     i = np.argmax(r)
     assert abs(tt[i] - 1 / 2000.0) <= tt[1]
+
+
+def _ref_erf(x):
+    """_erf of src/kh_kernels.jl:19-25 (Abramowitz-Stegun 7.1.26), vectorised."""
+    s, ax = np.sign(x), np.abs(x)
+    t = 1.0 / (1.0 + 0.3275911 * ax)
+    y = 1.0 - (((((1.061405429 * t - 1.453152027) * t) + 1.421413741) * t - 0.284496736) * t +
+               0.254829592) * t * np.exp(-ax * ax)
+    return s * y
+
+
+def test_kh_velocity_pedestal_equals_full_kernel(oracle):
+    """The v_v kernel does not decay (its F term tends to a constant); the
+    oracle sums taps within +-12 sigma plus that constant times the running
+    input sum.  Brute force: the full kernel of eval_one_kernel
+    (kh_kernels.jl:106-157) at every lag, convolved directly."""
+    rng = np.random.default_rng(3)
+    ns, nr, nt, dt, c0, rho = 3, 2, 400, 5e-6, 343.0, 1.2
+    sg = np.sqrt(np.log(2.0)) / (2 * np.pi * 20e3)
+    sp = rng.standard_normal((ns, 3)) * 0.02
+    sn = rng.standard_normal((ns, 3))
+    sn /= np.linalg.norm(sn, axis=1, keepdims=True)
+    rp = rng.standard_normal((nr, 3)) * 0.02 + np.array([0.1, 0.0, 0.0])
+    rn = rng.standard_normal((nr, 3))
+    rn /= np.linalg.norm(rn, axis=1, keepdims=True)
+    q = rng.standard_normal((nt, ns)).astype(np.float32)
+    f = rng.standard_normal((nt, ns)).astype(np.float32)
+    aq, af = -0.7, 1.3
+    got = oracle.kh_velocity(sp, sn, rp, rn, q, f, dt, sg, c0, rho, aq, af)
+    want = np.zeros((nt, nr))
+    tg = np.arange(nt) * dt
+    for r in range(nr):
+        for s in range(ns):
+            d = rp[r] - sp[s]
+            dist = np.linalg.norm(d)
+            ih = d / dist
+            cr, cs = rn[r] @ ih, sn[s] @ ih
+            tau = tg - dist / c0
+            fg = np.exp(-tau ** 2 / (2 * sg ** 2)) / (np.sqrt(2 * np.pi) * sg)
+            dfg = -(tau / sg ** 2) * fg
+            Fg = 0.5 * (1 + _ref_erf(tau / (sg * np.sqrt(2))))
+            i1, i2, i3 = (1 / (4 * np.pi * dist ** k) for k in (1, 2, 3))
+            kq = (cr / rho) * (fg * i2 + dfg * i1 / c0)
+            kf = (cr * cs / rho) * (2 * Fg * i3 + 2 * fg * i2 / c0 + dfg * i1 / c0 ** 2)
+            want[:, r] += aq * np.convolve(kq, q[:, s].astype(np.float64))[:nt]
+            want[:, r] += af * np.convolve(kf, f[:, s].astype(np.float64))[:nt]
+    assert np.abs(got).max() > 0
+    assert np.linalg.norm(got - want) <= 1e-9 * np.linalg.norm(want)
