@@ -69,9 +69,11 @@ struct SolveDev {
   const int* gf_isrc;     // [n_out] 0-based transceiver columns driven
   const int* gf_irec;     // [n_in] 0-based transceiver columns read
   double* gf_pin;         // [n_in][nt] (p_rec - z0 vn_rec)/2 of recorded rows
+  double* gf_part;        // [n_out][gf_ks][2] partial sums of the split reduction
   double gf_z0;
   int gf_kind, gf_nt, gf_n1, gf_n2;
   int gf_nout, gf_nin;
+  int gf_ks, gf_pad_;     // receiver splits per driven source
 };
 
 constexpr int kTmaps = 9;
@@ -161,7 +163,8 @@ enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_
 cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
                         bool two_per_sm);
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
-cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_nsrc, cudaStream_t s);
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
+                                  cudaStream_t s);
 cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm);
 int consumer_threads();
 

@@ -1065,7 +1065,7 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 // Advances it_base of every solve by `by` steps: the last node of a captured
 // chunk of steps, so replaying the graph continues where it stopped.
 // In-loop GF extrapolation, extrapolate! (src/kernels/extrapolation.jl:204-249)
-// after v2vn! of step it < nt.  One block per driven source o:
+// after v2vn! of step it < nt, for every driven source o:
 //   PVFromPin (:139-170): pin[t, r] = (p_rec - z0 vn_rec)/2 (Float64);
 //     ps/vs = sum_r sum_tt p_pin/v_pin[T-tt+1, o, r] * pin[it-T+tt, r];
 //     p_src[it+1, iSrc[o]] = vs, vn_src[it+1, iSrc[o]] = ps.
@@ -1074,13 +1074,16 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 //   PVFromPV (:91-137, 204-218): ps += pv*p + pp*vn, vs += vv*p + vp*vn over
 //     the recorded p / v_n of the iRec columns (Float32 terms).
 // Sums are accumulated in Float64 (the Float32 zero of the reference is
-// promoted by the first Float64 add for the *FromPin kinds).  Rows before
+// promoted by the first Float64 add for the *FromPin kinds).  The receiver
+// range of each source is split over gf_ks blocks (blockIdx.x = o*ks + part)
+// whose partial sums the reduce kernel adds in a fixed order.  Rows before
 // `it` of pin come from gf_pin; row `it` is formed here and block 0 files it.
 __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it = S.it_base + p.step;
   if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
-  const int o = blockIdx.x;
+  const int ks = S.gf_ks;
+  const int o = blockIdx.x / ks, part = blockIdx.x - (blockIdx.x / ks) * ks;
   if (o >= S.gf_nout) return;
   const int nt = S.nt, ntx = S.ntx, ngf = S.gf_nt, n1 = S.gf_n1, nin = S.gf_nin;
   const int kind = S.gf_kind;
@@ -1091,14 +1094,16 @@ __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams
     const int col = S.gf_irec[r];
     return ((double)S.rec[0][cur + col] - (double)S.vn_rec[cur + col] * S.gf_z0) / 2.0;
   };
-  if (o == 0 && kind != ADF_GF_PV_FROM_PV_)
+  if (blockIdx.x == 0 && kind != ADF_GF_PV_FROM_PV_)
     for (int r = threadIdx.x; r < nin; r += blockDim.x)
       S.gf_pin[(long long)r * nt + (it - 1)] = pin_now(r);
+  const int rb = (int)((long long)nin * part / ks), re = (int)((long long)nin * (part + 1) / ks);
   double a = 0.0, b = 0.0;
-  const long long n = (long long)nin * T;
-  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
-    const int r = (int)(k / T);
-    const int tt = (int)(k - (long long)r * T);  // 0-based
+  // (r, tt) walk over this block's receivers, tt fastest: contiguous tensor
+  // and pin reads, the index stepped instead of divided
+  int r = rb + (int)threadIdx.x / T, tt = (int)threadIdx.x - ((int)threadIdx.x / T) * T;
+  const int step_r = (int)blockDim.x / T, step_t = (int)blockDim.x - step_r * T;
+  for (; r < re;) {
     const int row = t0 + tt;
     // tensor element [T-tt, ., .] (1-based lag) for this receiver and output
     const long long g = (long long)(T - 1 - tt) +
@@ -1116,6 +1121,12 @@ __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams
       const double pin = row == it - 1 ? pin_now(r) : S.gf_pin[(long long)r * nt + row];
       a = __dadd_rn(a, __dmul_rn((double)S.gf_t[0][g], pin));
       b = __dadd_rn(b, __dmul_rn((double)S.gf_t[1][g], pin));
+    }
+    r += step_r;
+    tt += step_t;
+    if (tt >= T) {
+      tt -= T;
+      ++r;
     }
   }
   __shared__ double red[2][8];
@@ -1136,19 +1147,38 @@ __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams
       sa = __dadd_rn(sa, red[0][k]);
       sb = __dadd_rn(sb, red[1][k]);
     }
-    const int col = S.gf_isrc[o];
-    float ps, vs;
-    if (kind == ADF_GF_P_FROM_PIN_) {
-      const float pos = (float)sa, neg = (float)sb;
-      ps = (float)((double)__fadd_rn(pos, neg) / S.gf_z0);  // vn_src
-      vs = __fsub_rn(pos, neg);                                            // p_src
-    } else {
-      ps = (float)sa;  // vn_src <- p_pin / (pv, pp)-derived
-      vs = (float)sb;  // p_src  <- v_pin / (vv, vp)-derived
-    }
-    S.src[0][(long long)it * S.src_ntx + col] = vs;
-    S.vn_src[(long long)it * ntx + col] = ps;
+    double* pp = S.gf_part + ((long long)o * ks + part) * 2;
+    pp[0] = sa;
+    pp[1] = sb;
   }
+}
+
+// Adds each source's partial sums in split order and writes its p_src and
+// vn_src samples of row it+1.
+__global__ void adf_gf_reduce_kernel(const EpiParams p) {
+  const SolveDev& S = p.solves[blockIdx.y];
+  const int it = S.it_base + p.step;
+  if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= S.gf_nout) return;
+  double sa = 0.0, sb = 0.0;
+  for (int k = 0; k < S.gf_ks; ++k) {
+    const double* pp = S.gf_part + ((long long)o * S.gf_ks + k) * 2;
+    sa = __dadd_rn(sa, pp[0]);
+    sb = __dadd_rn(sb, pp[1]);
+  }
+  const int col = S.gf_isrc[o];
+  float ps, vs;
+  if (S.gf_kind == ADF_GF_P_FROM_PIN_) {
+    const float pos = (float)sa, neg = (float)sb;
+    ps = (float)((double)__fadd_rn(pos, neg) / S.gf_z0);  // vn_src
+    vs = __fsub_rn(pos, neg);                              // p_src
+  } else {
+    ps = (float)sa;  // vn_src <- p_pin / (pv, pp)-derived
+    vs = (float)sb;  // p_src  <- v_pin / (vv, vp)-derived
+  }
+  S.src[0][(long long)it * S.src_ntx + col] = vs;
+  S.vn_src[(long long)it * S.ntx + col] = ps;
 }
 
 __global__ void adf_advance_kernel(SolveDev* solves, int n, int by) {
@@ -1179,10 +1209,14 @@ cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_nsrc, cudaStream_t s) {
-  // one block per driven source of the largest map in the batch
-  dim3 grid(max_nsrc > 0 ? max_nsrc : 1, p.n_solves);
-  adf_gf_extrapolate_kernel<<<grid, 256, 0, s>>>(p);
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
+                                  cudaStream_t s) {
+  // (source, receiver split) blocks of the largest map in the batch, then
+  // the fixed-order reduction of the splits
+  adf_gf_extrapolate_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), 256, 0, s>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  adf_gf_reduce_kernel<<<dim3((max_nsrc + 127) / 128, p.n_solves), 128, 0, s>>>(p);
   return cudaGetLastError();
 }
 

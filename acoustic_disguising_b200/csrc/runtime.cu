@@ -442,9 +442,13 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   int max_stage = 0, max_pn = 0;
   max_ntx = 0;
   max_gf_nsrc = 0;
+  max_gf_blocks = 0;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
-    if (sd[i].flags & SF_GF) max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
+    if (sd[i].flags & SF_GF) {
+      max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
+      max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
+    }
     for (int k = 0; k < kTmaps; ++k) tm[(size_t)kTmaps * i + k] = list[i]->tm[k];
     const SolveDev& d = list[i]->dev;
     const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
@@ -494,7 +498,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaStreamSynchronize(st);
   stage_floats = max_stage;
   pn_floats = max_pn;
-  per_step = max_gf_nsrc > 0 ? 4 : 2;
+  per_step = max_gf_nsrc > 0 ? 5 : 2;
   // pipeline depth: as many slots as fit two CTAs per SM, else one CTA.
   // The kernel's static shared memory counts against the same budget.
   cudaFuncAttributes fa{};
@@ -573,7 +577,7 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
   if (max_gf_nsrc > 0) {  // in-loop GF extrapolation, then vn2v! of those solves
-    if ((e2 = launch_gf_extrapolate(ep, max_gf_nsrc, ctx->stream)) != cudaSuccess)
+    if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
     ep.phase = 2;
     if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
@@ -1069,7 +1073,13 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_src, rc);
     int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_rec, rc);
     double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_rec * d->nt, rc);
+    // receiver splits: about eight 256-thread blocks per SM in all
+    const int ks = (int)std::max<int64_t>(
+        1, std::min<int64_t>(gf->n_rec, (int64_t)8 * ctx->nsm / std::max<int64_t>(1, gf->n_src)));
+    double* part = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_src * ks * 2, rc);
     if (rc) return rc;
+    sd.gf_part = part;
+    sd.gf_ks = ks;
     std::vector<int> cs((size_t)gf->n_src), cr((size_t)gf->n_rec);
     for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
     for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);

@@ -91,6 +91,7 @@ struct Batch {
   int n_items = 0, stages = 3, stage_floats = 0, pn_floats = 0, grid = 1, max_ntx = 0;
   bool two_per_sm = false;  // ring sized so two CTAs share an SM
   int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
+  int max_gf_blocks = 0;     // (source, receiver split) blocks of the GF kernel
   int per_step = 2;          // kernel launches per launch-step
   size_t smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
