@@ -9,7 +9,7 @@ from .api import (  # noqa: F401
     ricker_wavelet, fib_sphere_area, cpml_profiles, cpml_profiles_static, STATIC_CPML_MAX_NPML,
     split_profiles, Cpml, shape_params,
     build_update_mask, Transceiver, TransceiverGrid, transceivers_to_grid, p_src, p_rec, vn_src,
-    vn_rec, run_fdtd, GfMap, PVFromPin, PFromPin, PVFromPV, injection_coefficients, kh_pressure, kh_velocity, fp32_fma_peak, GfRequest,
+    vn_rec, run_fdtd, GfMap, PVFromPin, PFromPin, PVFromPV, injection_coefficients, kh_pressure, kh_velocity, gf_postprocess, gf_unit_factors, fp32_fma_peak, GfRequest,
     gf_solve_batch, autotune, Server,
 )
 

@@ -144,6 +144,9 @@ SIGNATURES = [
     ("adf_kh_velocity", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("adf_gf_postprocess", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                     C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                     C.c_double, C.c_int]),
     ("adf_injection_coefficients", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_double,
                                              C.c_int64, C.c_void_p]),
 ]

@@ -496,6 +496,27 @@ def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt: float, sigma: float,
     return out
 
 
+def gf_postprocess(a, t_in0: float, dt_in: float, nt_out: int, t_out0: float, dt_out: float,
+                   unit: float = 1.0, denoise: bool = True, ctx: Context | None = None):
+    """impulsive_gfs post-processing on the GPU (greens.jl:174-190): denoise,
+    cubic B-spline resampling onto t_out0 + k dt_out with the dt-ratio scale,
+    division by `unit` (gf_to_physical's C_p / C_v).  a: (nt_in, ncol)."""
+    ctx = ctx or default_context()
+    a = np.asfortranarray(a, np.float32)
+    out = np.zeros((nt_out, a.shape[1]), np.float32, order="F")
+    L.check(L.lib().adf_gf_postprocess(ctx.h, a.shape[1], a.shape[0], t_in0, dt_in, nt_out,
+                                       t_out0, dt_out, _p(a), _p(out), unit, int(bool(denoise))),
+            "gf_postprocess")
+    return out
+
+
+def gf_unit_factors(d: L.Domain, dt_save: float):
+    """gf_unit_factors (greens_io.jl:180-184): (C_p, C_v) of raw FDTD GFs."""
+    C_p = d.dx ** 3 * dt_save / (d.dt ** 2 * d.c0 ** 2)
+    C_v = -d.r0 * d.dx ** 3 * dt_save / d.dt ** 2
+    return C_p, C_v
+
+
 def fp32_fma_peak(ctx: Context | None = None):
     """Measured FP32 FMA throughput (TFLOP/s) and the probe's duration (ms)."""
     ctx = ctx or default_context()

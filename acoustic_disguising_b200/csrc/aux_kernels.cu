@@ -219,6 +219,77 @@ cudaError_t launch_scale_traces(const float* in, float* out, long long n, const 
   return cudaGetLastError();
 }
 
+// ---- impulsive_gfs post-processing (src/greens.jl:174-190, resample.jl:32-76,
+// greens_io.jl:195-205), one source's traces (nt_in, ncol) column-major.
+// Prefilter: one thread per column -- denoise at 1e-4 of the column's
+// (signed) maximum, then the natural cubic B-spline coefficients
+// c_0..c_{n+1} of Line(OnGrid()) ends: c_1 = y_1, c_n = y_n and
+// (c_{i-1} + 4 c_i + c_{i+1}) / 6 = y_i in between (Thomas algorithm; the
+// pivots cpv depend only on i and are shared by all columns).
+__global__ void adf_gf_prefilter_kernel(int ncol, int n, const float* __restrict__ in,
+                                        const double* __restrict__ cpv, double* coef,
+                                        int denoise) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const float* a = in + (long long)n * c;
+  double* cf = coef + (long long)(n + 2) * c;
+  float mx = a[0];
+  for (int t = 1; t < n; ++t) mx = fmaxf(mx, a[t]);
+  const double thr = 1e-4 * (double)mx;
+  auto y = [&](int t1) {  // 1-based sample, denoised
+    const float v = a[t1 - 1];
+    return (denoise && (double)fabsf(v) < thr) ? 0.0 : (double)v;
+  };
+  cf[1] = y(1);
+  cf[n] = y(n);
+  // forward sweep: cf[i] holds d'_i
+  for (int i = 2; i <= n - 1; ++i) {
+    double rhs = 6.0 * y(i);
+    if (i == 2) rhs -= cf[1];
+    if (i == n - 1) rhs -= cf[n];
+    const double b = 4.0 - (i > 2 ? cpv[i - 1] : 0.0);
+    cf[i] = (rhs - (i > 2 ? cf[i - 1] : 0.0)) / b;
+  }
+  for (int i = n - 2; i >= 2; --i) cf[i] = cf[i] - cpv[i] * cf[i + 1];
+  cf[0] = 2.0 * cf[1] - cf[2];
+  cf[n + 1] = 2.0 * cf[n] - cf[n - 1];
+}
+
+// Evaluation: one thread per output sample and column; Flat() outside the
+// input axis, times dt_out/dt_in, rounded to Float32, divided by unit32.
+__global__ void adf_gf_resample_kernel(int ncol, int n, int nt_out, double t_in0, double dt_in,
+                                       double t_out0, double dt_out, const double* coef,
+                                       float* out, float unit32) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= (long long)nt_out * ncol) return;
+  const int c = (int)(k / nt_out), j = (int)(k - (long long)c * nt_out);
+  const double* cf = coef + (long long)(n + 2) * c;
+  const double tt = t_out0 + (double)j * dt_out;
+  double x = (tt - t_in0) / dt_in + 1.0;
+  x = fmin(fmax(x, 1.0), (double)n);
+  int i = (int)floor(x);
+  if (i > n - 1) i = n - 1;
+  const double d = x - (double)i, e = 1.0 - d;
+  const double w0 = e * e * e / 6.0, w3 = d * d * d / 6.0;
+  const double w1 = (3.0 * d * d * d - 6.0 * d * d + 4.0) / 6.0;
+  const double w2 = (-3.0 * d * d * d + 3.0 * d * d + 3.0 * d + 1.0) / 6.0;
+  const double v = cf[i - 1] * w0 + cf[i] * w1 + cf[i + 1] * w2 + cf[i + 2] * w3;
+  out[k] = __fdiv_rn((float)(v * (dt_out / dt_in)), unit32);
+}
+
+cudaError_t launch_gf_postprocess(int ncol, int n, int nt_out, double t_in0, double dt_in,
+                                  double t_out0, double dt_out, const float* in,
+                                  const double* cpv, double* coef, float* out, float unit32,
+                                  int denoise, cudaStream_t s) {
+  adf_gf_prefilter_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(ncol, n, in, cpv, coef, denoise);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long tot = (long long)nt_out * ncol;
+  adf_gf_resample_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
+      ncol, n, nt_out, t_in0, dt_in, t_out0, dt_out, coef, out, unit32);
+  return cudaGetLastError();
+}
+
 // Fixed scratch for adf_cpml_profiles_static: room for the profiles of
 // npml <= kStaticCpmlMaxNpml (8*npml+4 values) in Float64 followed by Float32.
 // Nothing in it has to start at zero: the profile kernel writes every value

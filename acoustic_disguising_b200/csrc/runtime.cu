@@ -32,6 +32,10 @@ cudaError_t launch_pack_mask(const uint8_t* jl, int nx, int ny, int nz, int mw, 
                              cudaStream_t s);
 cudaError_t launch_injection_coef(double radius, long long n, double dt, double rho, double dx,
                                   double z0, double* out, cudaStream_t s);
+cudaError_t launch_gf_postprocess(int ncol, int n, int nt_out, double t_in0, double dt_in,
+                                  double t_out0, double dt_out, const float* in,
+                                  const double* cpv, double* coef, float* out, float unit32,
+                                  int denoise, cudaStream_t s);
 int static_cpml_max_npml();
 cudaError_t static_cpml_scratch(double** d64, float** d32);
 
@@ -1231,6 +1235,57 @@ int adf_kernel_timing(adf_ctx* ctx, double* ms, int64_t* n, int reset) {
     ctx->kernel_ms = 0.0;
     ctx->kernel_launches = 0;
   }
+  return ADF_OK;
+}
+
+int adf_gf_postprocess(adf_ctx* ctx, int64_t ncol, int64_t nt_in, double t_in0, double dt_in,
+                       int64_t nt_out, double t_out0, double dt_out, const float* in,
+                       float* out, double unit, int denoise) {
+  if (!ctx || !in || !out || ncol < 1 || nt_in < 4 || nt_out < 1 || !(dt_in > 0) ||
+      !(dt_out > 0) || !(unit != 0) || ncol > (1 << 28) || nt_in > (1 << 28) ||
+      nt_out > (1 << 28))
+    return fail(ADF_E_ARG, "adf_gf_postprocess: bad arguments");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  const int n = (int)nt_in;
+  std::vector<double> cpv((size_t)n + 1, 0.0);  // Thomas pivots of (1, 4, 1)
+  for (int i = 2; i <= n - 1; ++i) cpv[(size_t)i] = 1.0 / (4.0 - (i > 2 ? cpv[(size_t)i - 1] : 0.0));
+  float* din = nullptr;
+  float* dout = nullptr;
+  double* dcoef = nullptr;
+  double* dcp = nullptr;
+  auto release = [&]() {
+    cudaFree(din);
+    cudaFree(dout);
+    cudaFree(dcoef);
+    cudaFree(dcp);
+  };
+  if (cudaMalloc(&din, (size_t)4 * n * ncol) != cudaSuccess ||
+      cudaMalloc(&dout, (size_t)4 * nt_out * ncol) != cudaSuccess ||
+      cudaMalloc(&dcoef, (size_t)8 * (n + 2) * ncol) != cudaSuccess ||
+      cudaMalloc(&dcp, (size_t)8 * (n + 1)) != cudaSuccess) {
+    release();
+    cudaGetLastError();
+    return fail(ADF_E_NOMEM, "adf_gf_postprocess: device allocation failed");
+  }
+  cudaStream_t st = ctx->stream;
+  cudaMemcpyAsync(din, in, (size_t)4 * n * ncol, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dcp, cpv.data(), (size_t)8 * (n + 1), cudaMemcpyHostToDevice, st);
+  cudaEventRecord(ctx->ev0, st);
+  e = launch_gf_postprocess((int)ncol, n, (int)nt_out, t_in0, dt_in, t_out0, dt_out, din, dcp,
+                            dcoef, dout, (float)unit, denoise ? 1 : 0, st);
+  cudaEventRecord(ctx->ev1, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, (size_t)4 * nt_out * ncol, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  release();
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  ctx->last_ms = ms;
+  ctx->launches = 2;
+  ctx->h2d_bytes = (int64_t)4 * n * ncol;
+  ctx->d2h_bytes = (int64_t)4 * nt_out * ncol;
   return ADF_OK;
 }
 

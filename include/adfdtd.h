@@ -308,6 +308,19 @@ int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
  * reference counterpart; ms (optional) receives the probe's duration.      */
 int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms);
 
+/* impulsive_gfs post-processing of recorded GF traces (src/greens.jl:174-190,
+ * src/resample.jl:32-76, src/greens_io.jl:195-205), on the GPU, per column
+ * of in (nt_in, ncol) Float32: values below 1e-4 of the column maximum set
+ * to zero (denoise != 0); cubic B-spline resampling (Interpolations.jl
+ * BSpline(Cubic(Line(OnGrid()))), Flat() extrapolation) from the axis
+ * t_in0 + k dt_in to t_out0 + k dt_out, times dt_out/dt_in; rounded to
+ * Float32 and divided by Float32(unit) (gf_to_physical's C_p or C_v, 1 for
+ * raw units).  out (nt_out, ncol).  For impulsive_gfs: t_in0 = -timeshift,
+ * dt_in = dom.dt, t_out0 = 0, dt_out = tmax/(nt_gf-1).                    */
+int adf_gf_postprocess(adf_ctx* ctx, int64_t ncol, int64_t nt_in, double t_in0, double dt_in,
+                       int64_t nt_out, double t_out0, double dt_out, const float* in,
+                       float* out, double unit, int denoise);
+
 /* C_for_N (diagnostics/_check_inject_kh/injection_coefficients.jl:467-472)
  * with fib_sphere_area (src/io.jl:131), in FP64 on the GPU:
  * out[0]=C_f, out[1]=C_q, out[2]=dS.                                       */

@@ -1192,6 +1192,58 @@ int or_kh_velocity(int64_t ns, const double* sp, const double* sn, int64_t nr,
   return 0;
 }
 
+int or_gf_postprocess(int64_t ncol, int64_t n, double t_in0, double dt_in, int64_t nt_out,
+                      double t_out0, double dt_out, const float* in, float* out, double unit,
+                      int denoise) {
+  if (ncol < 0 || n < 4 || nt_out < 1 || !(dt_in > 0) || !(dt_out > 0) || !(unit != 0))
+    return -1;
+  const float unit32 = (float)unit;
+  const double amp = dt_out / dt_in;  // resample_time's scale_amplitude
+  pfor(0, ncol, [&](int64_t c) {
+    const float* a = in + n * c;
+    std::vector<double> y((size_t)n + 1), cf((size_t)n + 2), cp((size_t)n + 1), dp((size_t)n + 1);
+    // greens.jl:178-179: maximum over time (signed), threshold 1e-4 * max
+    float mx = a[0];
+    for (int64_t t = 1; t < n; ++t) mx = std::max(mx, a[t]);
+    for (int64_t t = 1; t <= n; ++t) {
+      const float v = a[t - 1];
+      y[(size_t)t] = (denoise && (double)std::fabs(v) < 1e-4 * (double)mx) ? 0.0 : (double)v;
+    }
+    // natural cubic B-spline coefficients c_0..c_{n+1}: c_1 = y_1, c_n = y_n,
+    // (c_{i-1} + 4 c_i + c_{i+1}) / 6 = y_i for i = 2..n-1, then the end rows
+    cf[1] = y[1];
+    cf[(size_t)n] = y[(size_t)n];
+    // Thomas algorithm on i = 2..n-1 with rhs 6 y_i and known c_1, c_n
+    for (int64_t i = 2; i <= n - 1; ++i) {
+      double rhs = 6.0 * y[(size_t)i];
+      if (i == 2) rhs -= cf[1];
+      if (i == n - 1) rhs -= cf[(size_t)n];
+      const double b = 4.0 - (i > 2 ? cp[(size_t)i - 1] : 0.0);
+      cp[(size_t)i] = 1.0 / b;
+      dp[(size_t)i] = (rhs - (i > 2 ? dp[(size_t)i - 1] : 0.0)) / b;
+    }
+    for (int64_t i = n - 1; i >= 2; --i)
+      cf[(size_t)i] = dp[(size_t)i] - (i < n - 1 ? cp[(size_t)i] * cf[(size_t)i + 1] : 0.0);
+    cf[0] = 2.0 * cf[1] - cf[2];
+    cf[(size_t)n + 1] = 2.0 * cf[(size_t)n] - cf[(size_t)n - 1];
+    for (int64_t k = 0; k < nt_out; ++k) {
+      const double tt = t_out0 + (double)k * dt_out;
+      double x = (tt - t_in0) / dt_in + 1.0;  // 1-based sample coordinate
+      x = std::min(std::max(x, 1.0), (double)n);  // Flat()
+      int64_t i = (int64_t)std::floor(x);
+      if (i > n - 1) i = n - 1;
+      const double d = x - (double)i, e = 1.0 - d;
+      const double w0 = e * e * e / 6.0, w3 = d * d * d / 6.0;
+      const double w1 = (3.0 * d * d * d - 6.0 * d * d + 4.0) / 6.0;
+      const double w2 = (-3.0 * d * d * d + 3.0 * d * d + 3.0 * d + 1.0) / 6.0;
+      const double v = cf[(size_t)i - 1] * w0 + cf[(size_t)i] * w1 + cf[(size_t)i + 1] * w2 +
+                       cf[(size_t)i + 2] * w3;
+      out[k + nt_out * c] = (float)(v * amp) / unit32;
+    }
+  });
+  return 0;
+}
+
 // extrapolate_pv_from_pin! (extrapolation.jl:139-170)
 int or_extrapolate_pv_from_pin(const float* pin, int64_t nt, int64_t nrec, float* p_src,
                                float* v_src, int64_t nsrc, const float* pp, const float* vp,

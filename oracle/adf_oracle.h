@@ -180,6 +180,22 @@ int or_kh_velocity(int64_t ns, const double* s_pts, const double* s_nrm, int64_t
                    double aq, double af, int64_t r_begin, int64_t r_end, double* out,
                    int nthreads);
 
+/* impulsive_gfs post-processing of one source's traces (src/greens.jl:
+ * 174-190, src/resample.jl:32-76, src/greens_io.jl:195-205), per column of
+ * in (nt_in, ncol) Float32:
+ *   denoise  (denoise != 0): values with |a| < 1e-4 * (column maximum) -> 0
+ *   resample : cubic B-spline, Line(OnGrid()) ends (zero second derivative),
+ *              Flat() extrapolation, from t_in0 + k dt_in to t_out0 + k
+ *              dt_out, times dt_out / dt_in, rounded to Float32
+ *   physical : divided by Float32(unit) (gf_to_physical's C_p or C_v; 1
+ *              leaves the raw units)
+ * into out (nt_out, ncol).  FP64 throughout before the final roundings.
+ * The B-spline prefilter follows Interpolations.jl 0.16.2's published
+ * algorithm, which is not part of the reference tree: parity unpinned.   */
+int or_gf_postprocess(int64_t ncol, int64_t nt_in, double t_in0, double dt_in, int64_t nt_out,
+                      double t_out0, double dt_out, const float* in, float* out, double unit,
+                      int denoise);
+
 /* extrapolate_pv_from_pin! (src/kernels/extrapolation.jl:139-170), 1-based it.
  * pin (nt, nrec), p_src/v_src (nt, nsrc), pp/vp (nt_gf, nsrc, nrec).      */
 int or_extrapolate_pv_from_pin(const float* pin, int64_t nt, int64_t nrec, float* p_src,

@@ -108,6 +108,9 @@ def lib():
                                      C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                      C.c_int64, C.c_int64, C.c_void_p, C.c_int]
+        L.or_gf_postprocess.argtypes = [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64,
+                                        C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_int]
         L.or_extrapolate_pv_from_pin.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                                  C.c_int64, C.c_int64]
@@ -408,6 +411,16 @@ def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt, sigma, c0, rho, aq, 
     _chk(lib().or_kh_velocity(ns, _p(f(s_pts)), _p(f(s_nrm)), nr, _p(f(r_pts)), _p(f(r_nrm)), nt,
                               dt, sigma, c0, rho, _p(g(in_q)), _p(g(in_f)), aq, af, r_begin, r_end,
                               _p(out), nthreads), "kh_velocity")
+    return out
+
+
+def gf_postprocess(a, t_in0, dt_in, nt_out, t_out0, dt_out, unit=1.0, denoise=True):
+    """impulsive_gfs post-processing (denoise, cubic B-spline resample,
+    physical units) of a (nt_in, ncol) float32 array -> (nt_out, ncol)."""
+    a = np.asfortranarray(a, np.float32)
+    out = np.zeros((nt_out, a.shape[1]), np.float32, order="F")
+    _chk(lib().or_gf_postprocess(a.shape[1], a.shape[0], t_in0, dt_in, nt_out, t_out0, dt_out,
+                                 _p(a), _p(out), unit, int(bool(denoise))), "gf_postprocess")
     return out
 
 
