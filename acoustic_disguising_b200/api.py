@@ -607,6 +607,53 @@ def autotune(nx: int, ny: int, nz: int, npml: int = 10, n_solves: int = 4, steps
     return ty.value, nzc.value, ms.value
 
 
+def impulsive_gfs(d: L.Domain, src_positions, src_normals, rec_positions, rec_normals,
+                  nt_gf: int, f_3db_hz: float, npml: int, pml_rcoef: float = 1e-4,
+                  pml_fc: float = 3e3, scatterer: str = "none", scatterer_kw: dict | None = None,
+                  arith: str = "promote", batch: int = 8, ctx: Context | None = None) -> dict:
+    """impulsive_gfs (src/greens.jl:48-234) on the GPU: for every source point
+    and source type (:p, direction [1,0,0,0]; :v, direction [0, normal]) one
+    FDTD solve recording p and v_n at the receivers (batched through the GF
+    engine), then per solve the post-processing of greens.jl:174-190 on the
+    GPU (denoise, cubic B-spline resampling from the shifted FDTD axis
+    range(-timeshift, tmax-timeshift, nt) onto range(0, tmax, nt_gf) with
+    the dt-ratio scale).  Returns the raw-unit tensors p_p, p_v, v_p, v_v
+    (nt_gf, n_rec, n_src) Float32 (first letter: receiver channel, second:
+    source type), t, src_positions, rec_positions; gf_file.save_impulsive_gfs
+    writes them in physical units."""
+    ctx = ctx or default_context()
+    sp = np.asarray(src_positions, np.float64).reshape(-1, 3)
+    sn = np.asarray(src_normals, np.float64).reshape(-1, 3)
+    rp = np.asarray(rec_positions, np.float64).reshape(-1, 3)
+    rn = np.asarray(rec_normals, np.float64).reshape(-1, 3)
+    n_src, n_rec, nt = sp.shape[0], rp.shape[0], int(d.nt)
+    tf, timeshift = impulsive_wavelet(d, f_3db_hz)
+    dt_in = float(d.tmax) / (nt - 1)       # step of range(-ts, tmax - ts; length = nt)
+    dt_gf = float(d.tmax) / (nt_gf - 1)    # step of range(0, tmax; length = nt_gf)
+    out = {k: np.zeros((nt_gf, n_rec, n_src), np.float32, order="F")
+           for k in ("p_p", "p_v", "v_p", "v_v")}
+    jobs = [(i, typ) for i in range(n_src) for typ in ("p", "v")]
+    for b0 in range(0, len(jobs), max(1, batch)):
+        chunk = jobs[b0:b0 + max(1, batch)]
+        reqs = []
+        for i, typ in chunk:
+            direction = [1.0, 0.0, 0.0, 0.0] if typ == "p" else [0.0, *sn[i]]
+            reqs.append(GfRequest(d, sp[i], direction, tf, rp, rn, npml=npml,
+                                  pml_rcoef=pml_rcoef, pml_fc=pml_fc, scatterer=scatterer,
+                                  scatterer_kw=dict(scatterer_kw or {}), arith=arith))
+        gf_solve_batch(reqs, batched=True, ctx=ctx)
+        for (i, typ), r in zip(chunk, reqs):
+            A = np.concatenate([r.p, r.vn], axis=1)  # (nt, 2 n_rec): p then v_n columns
+            R = gf_postprocess(A, -timeshift, dt_in, nt_gf, 0.0, dt_gf, unit=1.0, denoise=True,
+                               ctx=ctx)
+            out["p_" + typ][:, :, i] = R[:, :n_rec]
+            out["v_" + typ][:, :, i] = R[:, n_rec:]
+    out["t"] = np.linspace(0.0, float(d.tmax), nt_gf)
+    out["src_positions"] = sp
+    out["rec_positions"] = rp
+    return out
+
+
 class Server:
     """Continuous-batching serving loop (adf_server_*)."""
 

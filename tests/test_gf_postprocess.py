@@ -53,3 +53,38 @@ def test_gf_postprocess_matches_oracle(adf, oracle, ctx, denoise, unit):
     assert np.isfinite(out).all()
     err = np.linalg.norm(out.astype(np.float64) - ref) / np.linalg.norm(ref)
     assert err <= 1e-6, err
+
+
+@pytest.mark.gpu
+def test_impulsive_gfs_pipeline(adf, oracle, ctx):
+    """impulsive_gfs (greens.jl:48-234) end to end on the GPU against the
+    oracle's solve + post-processing for the same sources and receivers."""
+    DX, C0, RHO = 0.005, 343.0, 1.2
+    dt = 0.5 * DX / C0 / np.sqrt(3.0)
+    n, steps, nt_gf = 40, 140, 60
+    d = adf.Domain(tmax=(steps - 0.5) * dt, xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
+    sp, sn = adf.fibonacci_sphere(2, 0.35 * d.xmax)
+    rp, rn = adf.fibonacci_sphere(6, 0.2 * d.xmax)
+    res = adf.impulsive_gfs(d, sp, sn, rp, rn, nt_gf, 4000.0, npml=5, pml_fc=2000.0,
+                            scatterer="sphere", scatterer_kw=dict(radius=0.06 * d.xmax), batch=3)
+    o = oracle.domain(tmax=d.tmax, xmax=d.xmax, nx=n, c0=C0, r0=RHO, cf=0.5)
+    tf, ts = oracle.impulsive_wavelet(o, 4000.0)
+    mask = oracle.build_update_mask(o, "sphere", radius=0.06 * d.xmax)
+    for i in range(2):
+        for typ in ("p", "v"):
+            direction = [1.0, 0, 0, 0] if typ == "p" else [0.0, *sn[i]]
+            pts = np.vstack([sp[i], rp])
+            dirs = np.vstack([direction, np.hstack([np.zeros((6, 1)), rn])])
+            tfs = np.vstack([tf, np.zeros((6, d.nt))])
+            g = oracle.transceivers_to_grid(o, pts, dirs, tfs)
+            cp = oracle.CpmlState(o, 5, 1e-4, 2000.0)
+            f = np.zeros((n, n, n, 4), np.float32, order="F")
+            oracle.run_fdtd(o, f, g, cp, mask)
+            A = np.concatenate([g.rec[0][:, 1:], g.vn_rec[:, 1:]], axis=1)
+            R = oracle.gf_postprocess(A, -ts, d.tmax / (d.nt - 1), nt_gf, 0.0,
+                                      d.tmax / (nt_gf - 1), 1.0, True)
+            for ch, cols in (("p", slice(0, 6)), ("v", slice(6, 12))):
+                got = res[f"{ch}_{typ}"][:, :, i].astype(np.float64)
+                want = R[:, cols].astype(np.float64)
+                assert np.abs(want).max() > 0
+                assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want), (i, typ, ch)
