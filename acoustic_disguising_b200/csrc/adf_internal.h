@@ -21,7 +21,6 @@ enum : int {
   SF_PCPML = 2,     // p-side CPML active (npml>1, or npml>=1 with a mask)
   SF_VCPML = 4,     // v-side CPML active (npml>=1)
   SF_FP32 = 8,      // Float32 arithmetic instead of Float64 intermediates
-  SF_YZG = 16,      // y/z-slab CPML memory read from global memory, not staged
   SF_GF = 32,       // in-loop GF extrapolation between v2vn and vn2v
 };
 
@@ -62,6 +61,7 @@ struct SolveDev {
   float* vn_src;          // [nt][ntx] or NULL (no vn2v)
   float* vn_rec;
   const float* dir;       // [ntx][4]
+  const uint32_t* mask_bits;  // [nz][ny][mw] or NULL
   int* err;               // per-solve error word
   int pad_;
   // in-loop GF extrapolation, SF_GF only
@@ -76,20 +76,13 @@ struct SolveDev {
   int gf_ks, gf_pad_;     // receiver splits per driven source
 };
 
-constexpr int kTmaps = 9;
-
-// work item: {solve index, y tile, z0, z1}
+// work item: {solve index, y tile | x tile << 16, z0, z1}
 struct StepParams {
   SolveDev* solves;
-  const CUtensorMap* tmaps;  // kTmaps per solve: field, field(2 planes), mask, x-psi p/v,
-                             // y-psi p/v, z-psi p/v
   const int4* items;
   int n_items;
-  int step;          // launch-step index within the chunk
-  int stages;
-  int stage_floats;  // ring slot stride (floats)
-  int pn_floats;     // one Pn plane buffer (floats)
-  int* err;          // launch-wide error word
+  int step;  // launch-step index within the chunk
+  int* err;  // launch-wide error word
 };
 
 struct EpiParams {
@@ -99,73 +92,15 @@ struct EpiParams {
   int phase;  // 0: records, v2vn and vn2v; solves with SF_GF: 1 records + v2vn, 2 vn2v
 };
 
-// One ring slot (floats; every region 128-B aligned so TMA can land in it):
-//   P, Vx, Vy : rows j0-1 .. j0+ty of plane k            (3 x reg)
-//   Vz        : the same rows of planes k and k+1        (reg2)
-//   mask      : nibble words of those rows               (regm, 0 without a mask)
-//   xp, xv    : x-slab CPML memory of those rows, both   (regxp / regxv, 0 when
-//               sides, p side and v side                  that side is inactive)
-//   py,vy,pz,vz: y- and z-slab CPML memory of those rows (reg each when that side
-//               (one slab side each)                      is active, else 0)
-//   header    : 32 floats, the plane's entry-list offsets
-inline __host__ __device__ int round32(long long v) { return (int)((v + 31) / 32 * 32); }
-struct SlotLayout {
-  int reg, reg2, regm, regxp, regxv, regyz_p, regyz_v, total;
-  int off_vz, off_m, off_xp, off_xv, off_py, off_vy, off_pz, off_vz2;
-};
-// stage_yz = false leaves the y/z-slab boxes out (the kernel then reads that
-// CPML memory from global memory on slab planes), which makes room for
-// taller tiles.
-inline __host__ __device__ SlotLayout slot_layout(int ty, int nxp, int mw, int npp, int nvp,
-                                                  bool stage_yz) {
-  SlotLayout L;
-  const long long R = ty + 2;
-  L.reg = round32(R * nxp);
-  L.reg2 = round32(2 * R * nxp);
-  L.regm = round32(R * mw);
-  L.regxp = round32(2 * R * npp);
-  L.regxv = round32(2 * R * nvp);
-  L.regyz_p = (npp && stage_yz) ? L.reg : 0;
-  L.regyz_v = (nvp && stage_yz) ? L.reg : 0;
-  L.off_vz = 3 * L.reg;
-  L.off_m = L.off_vz + L.reg2;
-  L.off_xp = L.off_m + L.regm;
-  L.off_xv = L.off_xp + L.regxp;
-  L.off_py = L.off_xv + L.regxv;
-  L.off_vy = L.off_py + L.regyz_p;
-  L.off_pz = L.off_vy + L.regyz_v;
-  L.off_vz2 = L.off_pz + L.regyz_p;
-  L.total = L.off_vz2 + L.regyz_v + 32;
-  return L;
-}
-// y-slab side whose rows a tile's box holds (-1: tile outside both slabs):
-// the left slab if any row j0-1..j0+ty lies in [0, w), else the right slab
-// if any lies in [n-w, n).  w = npml (p side) or npml+1 (v side).
-inline __host__ __device__ int tile_yside(int j0, int ty, int n, int w) {
-  if (j0 - 1 < w) return 0;
-  if (j0 + ty >= n - w) return 1;
-  return -1;
-}
-// z-slab side of a plane (left slab has priority, as getBoundaryIndex)
-inline __host__ __device__ int plane_zside(int k, int n, int w) {
-  if (k < w) return 0;
-  if (k >= n - w) return 1;
-  return -1;
-}
-
-inline __host__ __device__ int pn_plane_floats(int ty, int nxp) { return round32((long long)(ty + 1) * nxp); }
-
 // error codes written by kernels
 enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_DRAIN_TIMEOUT = 3 };
 
 // launch helpers implemented in fdtd_kernels.cu
-// two_per_sm selects the build of the step kernel sized for two CTAs per SM
-cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
-                        bool two_per_sm);
+// one CTA per work item, blockDim (32, max_ty + 1); max_ty <= step_max_ty()
+cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s);
+int step_max_ty();
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
                                   cudaStream_t s);
-cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm);
-int consumer_threads();
 
 }  // namespace adf

@@ -5,24 +5,16 @@
 // buffer `rb` and writes buffer `wb`, so the pressure update, the q-channel
 // injection/recording, the three velocity updates, the f-channel
 // injection/recording and the rigid mirrors all happen in a single pass over
-// HBM: 16 B read + 16 B written per cell, plus psi traffic on CPML slabs and
-// half a byte of mask per cell.
+// HBM: 16 B read + 16 B written per cell, plus the CPML memory on the slabs
+// and half a byte of mask per cell.
 //
-// Work decomposition: a persistent CTA walks (solve, y tile, z chunk) items.
-// A tile spans the full x extent (nxp <= 512), `ty` rows and a run of
-// planes.  A producer warp streams planes into a ring of shared-memory slots
-// with TMA (cp.async.bulk.tensor, no multicast): each slot holds P, Vx, Vy
-// for rows j0-1 .. j0+ty and plane k, Vz for planes k and k+1, and the mask
-// nibbles.  Eight consumer warps compute, per plane:
-//   P phase : P_new on rows j0-1 .. j0+ty-1 (row j0-1 is the halo that the
-//             velocity update of row j0 needs; it is recomputed, not
-//             exchanged), into a triple-buffered shared plane;
-//   Q phase : q-channel inject/record entries of this (tile, plane), if any;
-//   V phase : Vx/Vy/Vz_new from P_new (x-1 and y-1 from shared memory, z-1
-//             from the previous plane still in shared memory);
-//   F phase : f-channel entries, if any;  then 128-bit stores of all four.
-// A z chunk starting at z0 > 0 first recomputes P_new on plane z0-1
-// (prologue plane: no stores, no records) for Vz at z0.
+// Work decomposition (2.5D): a CTA owns a tile of ty rows x 128 cells of one
+// solve and a run of planes; its warps are the tile's rows, its lanes 4-cell
+// quads, and it walks the planes in z keeping the z-neighbours in registers.
+// The new P of a plane goes through shared memory for the x-1 / y-1
+// neighbours of the velocity update; the halo row and column are
+// recomputed, not exchanged.  Grids of many such CTAs (two or more per SM)
+// keep HBM busy: the update is a short, memory-bound stencil.
 //
 // Arithmetic: Arith<double> reproduces Julia's promotion (Float32 storage,
 // Float64 Domain scalars, src/kernels/updates.jl) with explicit round-to-
@@ -31,56 +23,10 @@
 // variant.  Injection/recording (derivatives.jl:30-60) is pure Float32 with
 // separate multiply and add, as the reference computes it.
 #include "adf_internal.h"
-#include "ptx_util.h"
 
 namespace adf {
 
-#ifndef ADF_NCT
-#define ADF_NCT 256
-#endif
-constexpr int NCT = ADF_NCT;      // consumer threads
-constexpr int NCW = NCT / 32;     // consumer warps
-constexpr int NTHREADS = NCT + 32;
-constexpr int kMaxStages = 8;
-constexpr int kPnBufs = 3;
 constexpr int kMaxCoef = 8 * 63 + 4;  // CPML coefficients for npml <= 63
-
-int consumer_threads() { return NCT; }
-
-// ---------------------------------------------------------------------------
-// TMA tensor loads (no multicast)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
-                                            int c0, int c1, int c2, int c3, int c4) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
-                                            int c0, int c1, int c2, int c3) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
-                                            int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(mbar), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-__device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((uint64_t)map)
-               : "memory");
-}
-__device__ __forceinline__ void consumer_bar() {
-  asm volatile("bar.sync 1, %0;" ::"n"(NCT) : "memory");
-}
 
 // ---------------------------------------------------------------------------
 // Arithmetic policies
@@ -125,138 +71,48 @@ __device__ __forceinline__ void cpml_apply(R& dv, float& m, float a, float b) {
   dv = A::add(dv, A::cv(m));
 }
 
-struct PlaneCtx {
-  const float* sP;
-  const float* sVx;
-  const float* sVy;
-  const float* sVz;   // plane k rows, plane k+1 at + R*nxp
-  const uint32_t* sM;
-  const float* sXp;   // x-slab psi, p side: [side][R][npp]
-  const float* sXv;   // x-slab psi, v side: [side][R][nvp]
-  const float* yP;    // y-slab psi rows of side ysP (p) / ysV (v): [R][nxp]
-  const float* yV;
-  const float* zP;    // z-slab psi of this plane (p / v side): [R][nxp]
-  const float* zV;
-  int ysP, ysV;
-  const float* co;    // CPML coefficients staged in shared memory
-  float* pn_cur;
-  const float* pn_prev;
-  int j0, R, pl, rb, wb;
-  bool has_mask;
-};
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-__device__ __forceinline__ float f4get(const float4& v, int e) {
-  return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ void f4set(float4& v, int e, float x) {
-  if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
-}
+__device__ __forceinline__ float4 neg4(float4 v) { return make_float4(-v.x, -v.y, -v.z, -v.w); }
 
-// Per-item scalars held in registers for the fast paths (the descriptor
-// lives in shared memory; re-reading it per quad costs a load per field).
 template <typename R>
-struct Regs {
-  int nxp, R2;  // row pitch, rows per ring region (ty+2)
+struct Sc {  // per-solve update scalars in registers
   R fq, fv, rdx, rdy, rdz;
 };
 
-// ---------------------------------------------------------------------------
-// Boundary path, pressure: rigid planes, the i = nx plane, CPML slabs.  Row-
-// and plane-wide conditions are uniform branches; per-cell conditions (the x
-// slab, the last x cells) are selects, so the four cells' dependency chains
-// interleave.  CPML memory comes from the ring slot (x and staged y/z slabs).
-// ---------------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ float p_cell_slow(float P, float dx_in, float dy_in, float dz_in,
-                                             const Regs<R>& g, bool upd, bool open, bool xs,
-                                             float& mx, float ax, float bx, bool ys, float& my,
-                                             float ay, float by, bool zs, float& mz, float az,
-                                             float bz) {
-  using A = Arith<R>;
-  R dvx = A::mul(A::cv(dx_in), g.rdx);
-  R dvy = A::mul(A::cv(dy_in), g.rdy);
-  R dvz = A::mul(A::cv(dz_in), g.rdz);
-  {  // x slab: computed for every cell, kept where the cell is in the slab
-    R d2 = dvx;
-    float m2 = mx;
-    cpml_apply<R>(d2, m2, ax, bx);
-    if (xs) { dvx = d2; mx = m2; }
-  }
-  if (ys) cpml_apply<R>(dvy, my, ay, by);
-  if (zs) cpml_apply<R>(dvz, mz, az, bz);
-  const float n = A::rn(A::sub(A::cv(P), A::mul(g.fq, A::add(A::add(dvx, dvy), dvz))));
-  return (upd && open) ? n : P;
-}
+// Per-(row, plane) geometry shared by the cells of a quad, uniform across a warp.
+struct RowCtx {
+  int nx, ny, nz, npml, nxp, j, k, rb, wb;
+  bool pcpml, vcpml;
+};
 
+// ---------------------------------------------------------------------------
+// Pressure update of the quad x0..x0+3 of row j, plane k (update_p_cpml!,
+// update_p_mask!, update_p! on the rigid planes; updates.jl:21-136).
+// Inputs are the plane's P, Vx (x0..x0+4), Vy (rows j, j+1) and Vz (planes
+// k, k+1) from the input buffer.  Row- and plane-wide conditions (rigid
+// planes, y/z slabs) are warp-uniform branches; the x slab is a per-cell
+// block taken only by quads that touch it.  `owned` stores the new CPML
+// memory; recomputed halo cells and the prologue plane leave it alone.
+// ---------------------------------------------------------------------------
 template <typename R>
-__device__ __forceinline__ void p_quad(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
-                                       int r, int q, bool owned) {
-  const int nxp = g.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, npp = S.npp;
-  const int x0 = 4 * q;
-  const int j = c.j0 - 1 + r;
-  const int pl = c.pl;
-  const float* base = c.sP + r * nxp + x0;
-  const float4 P4 = ld4(base);
-  const float4 X4 = ld4(c.sVx + r * nxp + x0);
-  const float X5 = (x0 + 4 < nxp) ? c.sVx[r * nxp + x0 + 4] : 0.f;
-  const float4 Y0 = ld4(c.sVy + r * nxp + x0);
-  const float4 Y1 = ld4(c.sVy + (r + 1) * nxp + x0);
-  const float4 Z0 = ld4(c.sVz + r * nxp + x0);
-  const float4 Z1 = ld4(c.sVz + (c.R + r) * nxp + x0);
-  uint32_t nib = 0xFFFFu;
-  const bool rigid_y = (j == ny - 1), rigid_z = (pl == nz - 1);
-  // rigid planes use update_p! (updates.jl:122-136): -2V/d at the wall, no
-  // CPML, no mask; the (ny, nz) corner is not updated at all
+__device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
+                                                const float* co, int x0, bool owned, float4 P4,
+                                                float4 X4, float X5, float4 Y0, float4 Y1,
+                                                float4 Z0, float4 Z1, uint32_t nib) {
+  using A = Arith<R>;
+  const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, j = rc.j, k = rc.k;
+  const bool rigid_y = j == ny - 1, rigid_z = k == nz - 1;
+  // rigid planes use update_p! (-2V/d at the wall, no CPML, no mask); the
+  // (ny, nz) corner is not updated at all
   const bool plain_rigid = rigid_y || rigid_z;
-  if (c.has_mask && !plain_rigid) nib = (c.sM[r * S.mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-  const bool pc = (S.flags & SF_PCPML) != 0 && !plain_rigid;
-  const float* co = c.co;
-  int ysd = -1, yl = 0, zsd = -1, zl = 0;
-  if (pc) {
-    if (j < npml) { ysd = 0; yl = j; }
-    else if (j >= ny - npml) { ysd = 1; yl = j - (ny - npml); }
-    if (pl < npml) { zsd = 0; zl = pl; }
-    else if (pl >= nz - npml) { zsd = 1; zl = pl - (nz - npml); }
-  }
-  long long oy = 0, oz = 0;
-  float4 my = make_float4(0.f, 0.f, 0.f, 0.f), mz = my;
-  float ay = 0.f, by = 0.f, az = 0.f, bz = 0.f;
-  if (ysd >= 0) {  // staged with the plane unless the tile straddles both y slabs
-    oy = (long long)ysd * S.psi_p_side[1] + ((long long)pl * npml + yl) * nxp + x0;
-    my = ysd == c.ysP ? ld4(c.yP + r * nxp + x0) : ldg4(S.psi_p[1] + c.rb * S.psi_p_buf[1] + oy);
-    ay = co[ysd * npml + yl];
-    by = co[4 * npml + 2 + ysd * npml + yl];
-  }
-  if (zsd >= 0) {
-    oz = (long long)zsd * S.psi_p_side[2] + ((long long)zl * ny + j) * nxp + x0;
-    mz = (S.flags & SF_YZG) ? ldg4(S.psi_p[2] + c.rb * S.psi_p_buf[2] + oz)
-                            : ld4(c.zP + r * nxp + x0);
-    az = co[zsd * npml + zl];
-    bz = co[4 * npml + 2 + zsd * npml + zl];
-  }
-  // x slab: side and depth of each cell, memory from the slot
-  float mx[4], ax[4], bx[4];
-  bool xs[4];
-  int xside[4], xl[4];
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const int x = x0 + e;
-    int side = -1, l = 0;
-    if (pc) {
-      side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
-      l = side == 0 ? x : x - (nx - npml);
-    }
-    xs[e] = side >= 0;
-    const int sd = xs[e] ? side : 0, ll = xs[e] ? l : 0;
-    xside[e] = sd;
-    xl[e] = ll;
-    mx[e] = c.sXp[(sd * c.R + r) * npp + ll];
-    ax[e] = xs[e] ? co[sd * npml + ll] : 0.f;
-    bx[e] = xs[e] ? co[4 * npml + 2 + sd * npml + ll] : 0.f;
-  }
+  const bool corner = rigid_y && rigid_z;
+  if (plain_rigid) nib = 0xFFFFu;
+  const float Pv[4] = {P4.x, P4.y, P4.z, P4.w};
+  const float dxv[4] = {__fsub_rn(X4.y, X4.x), __fsub_rn(X4.z, X4.y), __fsub_rn(X4.w, X4.z),
+                        __fsub_rn(X5, X4.w)};
   const float dyv[4] = {rigid_y ? __fmul_rn(-2.0f, Y0.x) : __fsub_rn(Y1.x, Y0.x),
                         rigid_y ? __fmul_rn(-2.0f, Y0.y) : __fsub_rn(Y1.y, Y0.y),
                         rigid_y ? __fmul_rn(-2.0f, Y0.z) : __fsub_rn(Y1.z, Y0.z),
@@ -265,94 +121,129 @@ __device__ __forceinline__ void p_quad(const SolveDev& S, const Regs<R>& g, cons
                         rigid_z ? __fmul_rn(-2.0f, Z0.y) : __fsub_rn(Z1.y, Z0.y),
                         rigid_z ? __fmul_rn(-2.0f, Z0.z) : __fsub_rn(Z1.z, Z0.z),
                         rigid_z ? __fmul_rn(-2.0f, Z0.w) : __fsub_rn(Z1.w, Z0.w)};
-  const float dxv[4] = {__fsub_rn(X4.y, X4.x), __fsub_rn(X4.z, X4.y), __fsub_rn(X4.w, X4.z),
-                        __fsub_rn(X5, X4.w)};
-  const bool corner = rigid_y && rigid_z;
-  const float Pv[4] = {P4.x, P4.y, P4.z, P4.w};
-  float myv[4] = {my.x, my.y, my.z, my.w}, mzv[4] = {mz.x, mz.y, mz.z, mz.w};
+  R dvx[4], dvy[4], dvz[4];
+  bool upd[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    dvx[e] = A::mul(A::cv(dxv[e]), g.rdx);
+    dvy[e] = A::mul(A::cv(dyv[e]), g.rdy);
+    dvz[e] = A::mul(A::cv(dzv[e]), g.rdz);
+    upd[e] = x0 + e <= nx - 2 && !corner;
+  }
+  if (rc.pcpml && !plain_rigid) {
+    if (x0 < npml || x0 + 3 >= nx - npml) {  // x slab
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int x = x0 + e;
+        const int side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
+        if (side >= 0 && upd[e]) {
+          const int l = side == 0 ? x : x - (nx - npml);
+          const long long o = side * S.psi_p_side[0] + ((long long)k * ny + j) * S.npp + l;
+          float m = S.psi_p[0][rc.rb * S.psi_p_buf[0] + o];
+          cpml_apply<R>(dvx[e], m, co[side * npml + l], co[4 * npml + 2 + side * npml + l]);
+          if (owned) S.psi_p[0][rc.wb * S.psi_p_buf[0] + o] = m;
+        }
+      }
+    }
+    const int ysd = j < npml ? 0 : (j >= ny - npml ? 1 : -1);
+    if (ysd >= 0) {  // y slab: the whole quad, cells that are not updated keep their memory
+      const int yl = ysd == 0 ? j : j - (ny - npml);
+      const long long o = ysd * S.psi_p_side[1] + ((long long)k * npml + yl) * rc.nxp + x0;
+      const float4 m4 = ld4(S.psi_p[1] + rc.rb * S.psi_p_buf[1] + o);
+      float m[4] = {m4.x, m4.y, m4.z, m4.w};
+      const float a = co[ysd * npml + yl], b = co[4 * npml + 2 + ysd * npml + yl];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (upd[e]) cpml_apply<R>(dvy[e], m[e], a, b);
+      if (owned) st4(S.psi_p[1] + rc.wb * S.psi_p_buf[1] + o, make_float4(m[0], m[1], m[2], m[3]));
+    }
+    const int zsd = k < npml ? 0 : (k >= nz - npml ? 1 : -1);
+    if (zsd >= 0) {
+      const int zl = zsd == 0 ? k : k - (nz - npml);
+      const long long o = zsd * S.psi_p_side[2] + ((long long)zl * ny + j) * rc.nxp + x0;
+      const float4 m4 = ld4(S.psi_p[2] + rc.rb * S.psi_p_buf[2] + o);
+      float m[4] = {m4.x, m4.y, m4.z, m4.w};
+      const float a = co[zsd * npml + zl], b = co[4 * npml + 2 + zsd * npml + zl];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (upd[e]) cpml_apply<R>(dvz[e], m[e], a, b);
+      if (owned) st4(S.psi_p[2] + rc.wb * S.psi_p_buf[2] + o, make_float4(m[0], m[1], m[2], m[3]));
+    }
+  }
   float o[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    const bool upd = (x0 + e <= nx - 2) && !corner;
-    float myc = myv[e], mzc = mzv[e], mxc = mx[e];
-    o[e] = p_cell_slow<R>(Pv[e], dxv[e], dyv[e], dzv[e], g, upd, (nib >> (4 * e)) & 1u,
-                          xs[e] && upd, mxc, ax[e], bx[e], ysd >= 0, myc, ay, by, zsd >= 0, mzc,
-                          az, bz);
-    if (upd) { myv[e] = myc; mzv[e] = mzc; mx[e] = mxc; }
+    const float n =
+        A::rn(A::sub(A::cv(Pv[e]), A::mul(g.fq, A::add(A::add(dvx[e], dvy[e]), dvz[e]))));
+    o[e] = (upd[e] && ((nib >> (4 * e)) & 1u)) ? n : Pv[e];
   }
-  st4(c.pn_cur + r * nxp + x0, make_float4(o[0], o[1], o[2], o[3]));
-  if (owned) {  // cells of the quad that were not updated keep their loaded value
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-      if (xs[e] && (x0 + e <= nx - 2) && !corner)
-        S.psi_p[0][c.wb * S.psi_p_buf[0] + xside[e] * S.psi_p_side[0] +
-                   ((long long)pl * ny + j) * npp + xl[e]] = mx[e];
-    if (ysd >= 0)
-      st4(S.psi_p[1] + c.wb * S.psi_p_buf[1] + oy, make_float4(myv[0], myv[1], myv[2], myv[3]));
-    if (zsd >= 0)
-      st4(S.psi_p[2] + c.wb * S.psi_p_buf[2] + oz, make_float4(mzv[0], mzv[1], mzv[2], mzv[3]));
-  }
+  return make_float4(o[0], o[1], o[2], o[3]);
 }
 
-// Boundary path, velocities: grid edges (Vx at i=1, Vy at j=1, Vz at k=1 are
-// not updated) and CPML slabs with the half-grid coefficients (npml+1).
+// The same update for one cell (the halo column x = xb-1 of an x tile).
 template <typename R>
-__device__ __forceinline__ float v_cell_slow(float V, float dp_in, R fv, R rd, bool upd,
-                                             bool open, bool sl, float& m, float a, float b) {
+__device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
+                                               const float* co, const float* fld, int x) {
   using A = Arith<R>;
-  R dp = A::mul(A::cv(dp_in), rd);
-  R d2 = dp;
-  float m2 = m;
-  cpml_apply<R>(d2, m2, a, b);
-  if (sl) { dp = d2; m = m2; }
-  const float n = A::rn(A::sub(A::cv(V), A::mul(fv, dp)));
-  return (upd && open) ? n : V;
+  const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, j = rc.j, k = rc.k, nxp = rc.nxp;
+  const long long cs = S.chan_stride, plane = (long long)ny * nxp;
+  const float* b = fld + ((long long)k * ny + j) * nxp + x;
+  const bool rigid_y = j == ny - 1, rigid_z = k == nz - 1;
+  const bool plain_rigid = rigid_y || rigid_z;
+  const bool upd = x <= nx - 2 && !(rigid_y && rigid_z);
+  const float P = __ldg(b);
+  if (!upd) return P;
+  const float X0 = __ldg(b + cs), X1 = __ldg(b + cs + 1);
+  const float Y0 = __ldg(b + 2 * cs), Z0 = __ldg(b + 3 * cs);
+  const float dy = rigid_y ? __fmul_rn(-2.0f, Y0) : __fsub_rn(__ldg(b + 2 * cs + nxp), Y0);
+  const float dz = rigid_z ? __fmul_rn(-2.0f, Z0) : __fsub_rn(__ldg(b + 3 * cs + plane), Z0);
+  R dvx = A::mul(A::cv(__fsub_rn(X1, X0)), g.rdx);
+  R dvy = A::mul(A::cv(dy), g.rdy);
+  R dvz = A::mul(A::cv(dz), g.rdz);
+  bool open = true;
+  if (!plain_rigid) {
+    if (S.flags & SF_MASK) open = (S.mask_bits[((long long)k * ny + j) * S.mw + (x >> 3)] >> (4 * (x & 7))) & 1u;
+    if (rc.pcpml) {
+      const int xs = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
+      if (xs >= 0) {
+        const int l = xs == 0 ? x : x - (nx - npml);
+        float m = S.psi_p[0][rc.rb * S.psi_p_buf[0] + xs * S.psi_p_side[0] +
+                             ((long long)k * ny + j) * S.npp + l];
+        cpml_apply<R>(dvx, m, co[xs * npml + l], co[4 * npml + 2 + xs * npml + l]);
+      }
+      const int ysd = j < npml ? 0 : (j >= ny - npml ? 1 : -1);
+      if (ysd >= 0) {
+        const int yl = ysd == 0 ? j : j - (ny - npml);
+        float m = S.psi_p[1][rc.rb * S.psi_p_buf[1] + ysd * S.psi_p_side[1] +
+                             ((long long)k * npml + yl) * nxp + x];
+        cpml_apply<R>(dvy, m, co[ysd * npml + yl], co[4 * npml + 2 + ysd * npml + yl]);
+      }
+      const int zsd = k < npml ? 0 : (k >= nz - npml ? 1 : -1);
+      if (zsd >= 0) {
+        const int zl = zsd == 0 ? k : k - (nz - npml);
+        float m = S.psi_p[2][rc.rb * S.psi_p_buf[2] + zsd * S.psi_p_side[2] +
+                             ((long long)zl * ny + j) * nxp + x];
+        cpml_apply<R>(dvz, m, co[zsd * npml + zl], co[4 * npml + 2 + zsd * npml + zl]);
+      }
+    }
+  }
+  const float n = A::rn(A::sub(A::cv(P), A::mul(g.fq, A::add(A::add(dvx, dvy), dvz))));
+  return open ? n : P;
 }
 
+// ---------------------------------------------------------------------------
+// Velocity updates of the quad (update_vx!/vy!/vz! and their masked forms,
+// updates.jl:192-274, 380-500): Vx over x >= 1, Vy over j >= 1, Vz over k >= 1,
+// x < nx; CPML with the half-grid coefficients (npml+1 layers).
+// ---------------------------------------------------------------------------
 template <typename R>
-__device__ __forceinline__ void v_quad(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
-                                       int r, int q, float4& vxo, float4& vyo, float4& vzo) {
-  const int nxp = g.nxp, nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, nvp = S.nvp;
-  const int nm = npml + 1;
-  const int x0 = 4 * q;
-  const int j = c.j0 - 1 + r;
-  const int pl = c.pl;
-  const float4 Pc = ld4(c.pn_cur + r * nxp + x0);
-  const float Pxm = x0 > 0 ? c.pn_cur[r * nxp + x0 - 1] : 0.f;
-  const float4 Pym = ld4(c.pn_cur + (r - 1) * nxp + x0);
-  const float4 Pzm = ld4(c.pn_prev + r * nxp + x0);
-  const float4 VX = ld4(c.sVx + r * nxp + x0);
-  const float4 VY = ld4(c.sVy + r * nxp + x0);
-  const float4 VZ = ld4(c.sVz + r * nxp + x0);
-  uint32_t nib = 0xFFFFu;
-  if (c.has_mask) nib = (c.sM[r * S.mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-  const bool vc = (S.flags & SF_VCPML) != 0;
-  const float* co = c.co;
-  int ysd = -1, yl = 0, zsd = -1, zl = 0;
-  if (vc && j >= 1) {
-    if (j <= npml) { ysd = 0; yl = j; }
-    else if (j >= ny - npml - 1) { ysd = 1; yl = j - (ny - npml - 1); }
-  }
-  if (vc && pl >= 1) {
-    if (pl <= npml) { zsd = 0; zl = pl; }
-    else if (pl >= nz - npml - 1) { zsd = 1; zl = pl - (nz - npml - 1); }
-  }
-  long long oy = 0, oz = 0;
-  float4 my = make_float4(0.f, 0.f, 0.f, 0.f), mz = my;
-  float ay = 0.f, by = 0.f, az = 0.f, bz = 0.f;
-  if (ysd >= 0) {
-    oy = (long long)ysd * S.psi_v_side[1] + ((long long)pl * nm + yl) * nxp + x0;
-    my = ysd == c.ysV ? ld4(c.yV + r * nxp + x0) : ldg4(S.psi_v[1] + c.rb * S.psi_v_buf[1] + oy);
-    ay = co[2 * npml + ysd * nm + yl];
-    by = co[6 * npml + 2 + ysd * nm + yl];
-  }
-  if (zsd >= 0) {
-    oz = (long long)zsd * S.psi_v_side[2] + ((long long)zl * ny + j) * nxp + x0;
-    mz = (S.flags & SF_YZG) ? ldg4(S.psi_v[2] + c.rb * S.psi_v_buf[2] + oz)
-                            : ld4(c.zV + r * nxp + x0);
-    az = co[2 * npml + zsd * nm + zl];
-    bz = co[6 * npml + 2 + zsd * nm + zl];
-  }
+__device__ __forceinline__ void v_update_quad(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
+                                              const float* co, int x0, float4 Pc, float Pxm,
+                                              float4 Pym, float4 Pzm, float4 VX, float4 VY,
+                                              float4 VZ, uint32_t nib, float4& vxo, float4& vyo,
+                                              float4& vzo) {
+  using A = Arith<R>;
+  const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, nm = npml + 1, j = rc.j, k = rc.k;
   const float Pv[4] = {Pc.x, Pc.y, Pc.z, Pc.w};
   const float Pl[4] = {Pxm, Pc.x, Pc.y, Pc.z};
   const float Py[4] = {Pym.x, Pym.y, Pym.z, Pym.w};
@@ -360,660 +251,399 @@ __device__ __forceinline__ void v_quad(const SolveDev& S, const Regs<R>& g, cons
   const float Vx[4] = {VX.x, VX.y, VX.z, VX.w};
   const float Vy[4] = {VY.x, VY.y, VY.z, VY.w};
   const float Vz[4] = {VZ.x, VZ.y, VZ.z, VZ.w};
-  float myv[4] = {my.x, my.y, my.z, my.w}, mzv[4] = {mz.x, mz.y, mz.z, mz.w};
-  float ox[4], oy4[4], oz4[4], mx[4];
-  bool xs[4];
-  int xside[4], xl[4];
+  R dx[4], dy[4], dz[4];
+  bool in[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    const int x = x0 + e;
-    const bool in = x < nx;
-    // Vx over i = 2..nx (update_vx!, updates.jl:192-218), x slab with npml+1
-    int side = -1, l = 0;
-    if (vc) {
-      side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
-      l = side == 0 ? x : x - (nx - npml - 1);
+    dx[e] = A::mul(A::cv(__fsub_rn(Pv[e], Pl[e])), g.rdx);
+    dy[e] = A::mul(A::cv(__fsub_rn(Pv[e], Py[e])), g.rdy);
+    dz[e] = A::mul(A::cv(__fsub_rn(Pv[e], Pz[e])), g.rdz);
+    in[e] = x0 + e < nx;
+  }
+  if (rc.vcpml) {
+    if (x0 <= npml || x0 + 3 >= nx - npml - 1) {  // x slab
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int x = x0 + e;
+        const int side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
+        if (side >= 0 && in[e] && x >= 1) {
+          const int l = side == 0 ? x : x - (nx - npml - 1);
+          const long long o = side * S.psi_v_side[0] + ((long long)k * ny + j) * S.nvp + l;
+          float m = S.psi_v[0][rc.rb * S.psi_v_buf[0] + o];
+          cpml_apply<R>(dx[e], m, co[2 * npml + side * nm + l], co[6 * npml + 2 + side * nm + l]);
+          S.psi_v[0][rc.wb * S.psi_v_buf[0] + o] = m;
+        }
+      }
     }
-    const bool updx = in && x >= 1;
-    xs[e] = side >= 0 && updx;
-    const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
-    xside[e] = sd;
-    xl[e] = ll;
-    mx[e] = c.sXv[(sd * c.R + r) * nvp + ll];
-    const float axe = side >= 0 ? co[2 * npml + sd * nm + ll] : 0.f;
-    const float bxe = side >= 0 ? co[6 * npml + 2 + sd * nm + ll] : 0.f;
-    ox[e] = v_cell_slow<R>(Vx[e], __fsub_rn(Pv[e], Pl[e]), g.fv, g.rdx, updx,
-                           (nib >> (4 * e + 1)) & 1u, xs[e], mx[e], axe, bxe);
-    // Vy over j = 2..ny
-    float myc = myv[e];
-    oy4[e] = v_cell_slow<R>(Vy[e], __fsub_rn(Pv[e], Py[e]), g.fv, g.rdy, in && j >= 1,
-                            (nib >> (4 * e + 2)) & 1u, ysd >= 0 && in, myc, ay, by);
-    if (in) myv[e] = myc;
-    // Vz over k = 2..nz
-    float mzc = mzv[e];
-    oz4[e] = v_cell_slow<R>(Vz[e], __fsub_rn(Pv[e], Pz[e]), g.fv, g.rdz, in && pl >= 1,
-                            (nib >> (4 * e + 3)) & 1u, zsd >= 0 && in, mzc, az, bz);
-    if (in) mzv[e] = mzc;
+    const int ysd = j < 1 ? -1 : (j <= npml ? 0 : (j >= ny - npml - 1 ? 1 : -1));
+    if (ysd >= 0) {
+      const int yl = ysd == 0 ? j : j - (ny - npml - 1);
+      const long long o = ysd * S.psi_v_side[1] + ((long long)k * nm + yl) * rc.nxp + x0;
+      const float4 m4 = ld4(S.psi_v[1] + rc.rb * S.psi_v_buf[1] + o);
+      float m[4] = {m4.x, m4.y, m4.z, m4.w};
+      const float a = co[2 * npml + ysd * nm + yl], b = co[6 * npml + 2 + ysd * nm + yl];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (in[e]) cpml_apply<R>(dy[e], m[e], a, b);
+      st4(S.psi_v[1] + rc.wb * S.psi_v_buf[1] + o, make_float4(m[0], m[1], m[2], m[3]));
+    }
+    const int zsd = k < 1 ? -1 : (k <= npml ? 0 : (k >= nz - npml - 1 ? 1 : -1));
+    if (zsd >= 0) {
+      const int zl = zsd == 0 ? k : k - (nz - npml - 1);
+      const long long o = zsd * S.psi_v_side[2] + ((long long)zl * ny + j) * rc.nxp + x0;
+      const float4 m4 = ld4(S.psi_v[2] + rc.rb * S.psi_v_buf[2] + o);
+      float m[4] = {m4.x, m4.y, m4.z, m4.w};
+      const float a = co[2 * npml + zsd * nm + zl], b = co[6 * npml + 2 + zsd * nm + zl];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (in[e]) cpml_apply<R>(dz[e], m[e], a, b);
+      st4(S.psi_v[2] + rc.wb * S.psi_v_buf[2] + o, make_float4(m[0], m[1], m[2], m[3]));
+    }
+  }
+  float ox[4], oy[4], oz[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const bool ux = in[e] && x0 + e >= 1 && ((nib >> (4 * e + 1)) & 1u);
+    const bool uy = in[e] && j >= 1 && ((nib >> (4 * e + 2)) & 1u);
+    const bool uz = in[e] && k >= 1 && ((nib >> (4 * e + 3)) & 1u);
+    const float nxv = A::rn(A::sub(A::cv(Vx[e]), A::mul(g.fv, dx[e])));
+    const float nyv = A::rn(A::sub(A::cv(Vy[e]), A::mul(g.fv, dy[e])));
+    const float nzv = A::rn(A::sub(A::cv(Vz[e]), A::mul(g.fv, dz[e])));
+    ox[e] = ux ? nxv : Vx[e];
+    oy[e] = uy ? nyv : Vy[e];
+    oz[e] = uz ? nzv : Vz[e];
   }
   vxo = make_float4(ox[0], ox[1], ox[2], ox[3]);
-  vyo = make_float4(oy4[0], oy4[1], oy4[2], oy4[3]);
-  vzo = make_float4(oz4[0], oz4[1], oz4[2], oz4[3]);
-#pragma unroll
-  for (int e = 0; e < 4; ++e)
-    if (xs[e])
-      S.psi_v[0][c.wb * S.psi_v_buf[0] + xside[e] * S.psi_v_side[0] +
-                 ((long long)pl * ny + j) * nvp + xl[e]] = mx[e];
-  if (ysd >= 0)
-    st4(S.psi_v[1] + c.wb * S.psi_v_buf[1] + oy, make_float4(myv[0], myv[1], myv[2], myv[3]));
-  if (zsd >= 0)
-    st4(S.psi_v[2] + c.wb * S.psi_v_buf[2] + oz, make_float4(mzv[0], mzv[1], mzv[2], mzv[3]));
+  vyo = make_float4(oy[0], oy[1], oy[2], oy[3]);
+  vzo = make_float4(oz[0], oz[1], oz[2], oz[3]);
 }
 
-// ---- one cell of a boundary quad on an ordinary tile-plane: no rigid plane
-// and no y/z slab here, only the x slab and the last x cells.  Same
-// arithmetic as p_quad / v_quad for that cell.
-template <typename R>
-__device__ __forceinline__ void p_xcell(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
-                                        int r, int x, bool owned) {
-  const int nxp = g.nxp, nx = S.nx, npml = S.npml;
-  const int o = r * nxp + x;
-  const float P = c.sP[o];
-  const float X0 = c.sVx[o];
-  const float X1 = (x + 1 < nxp) ? c.sVx[o + 1] : 0.f;
-  const float dy = __fsub_rn(c.sVy[o + nxp], c.sVy[o]);
-  const float dz = __fsub_rn(c.sVz[o + c.R * nxp], c.sVz[o]);
-  uint32_t open = 1u;
-  if (c.has_mask) open = (c.sM[r * S.mw + (x >> 3)] >> (4 * (x & 7))) & 1u;
-  const bool upd = x <= nx - 2;
-  int side = -1, l = 0;
-  if (S.flags & SF_PCPML) {
-    side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
-    l = side == 0 ? x : x - (nx - npml);
-  }
-  const bool xs = side >= 0 && upd;
-  const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
-  float mx = c.sXp[(sd * c.R + r) * S.npp + ll];
-  const float ax = side >= 0 ? c.co[sd * npml + ll] : 0.f;
-  const float bx = side >= 0 ? c.co[4 * npml + 2 + sd * npml + ll] : 0.f;
-  float my = 0.f, mz = 0.f;
-  c.pn_cur[o] = p_cell_slow<R>(P, __fsub_rn(X1, X0), dy, dz, g, upd, open, xs, mx, ax, bx, false,
-                               my, 0.f, 0.f, false, mz, 0.f, 0.f);
-  if (owned && xs) {
-    const int j = c.j0 - 1 + r;
-    S.psi_p[0][c.wb * S.psi_p_buf[0] + sd * S.psi_p_side[0] +
-               ((long long)c.pl * S.ny + j) * S.npp + ll] = mx;
-  }
-}
-
-template <typename R>
-__device__ __forceinline__ void v_xcell(const SolveDev& S, const Regs<R>& g, const PlaneCtx& c,
-                                        int r, int x, float& vx, float& vy, float& vz) {
-  const int nxp = g.nxp, nx = S.nx, npml = S.npml, nm = npml + 1;
-  const int j = c.j0 - 1 + r;
-  const int o = r * nxp + x;
-  const float Pc = c.pn_cur[o];
-  const float Pxm = x > 0 ? c.pn_cur[o - 1] : 0.f;
-  const float Pym = c.pn_cur[o - nxp];
-  const float Pzm = c.pn_prev[o];
-  uint32_t nib = 0xFu;
-  if (c.has_mask) nib = (c.sM[r * S.mw + (x >> 3)] >> (4 * (x & 7))) & 0xFu;
-  const bool in = x < nx;
-  int side = -1, l = 0;
-  if (S.flags & SF_VCPML) {
-    side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
-    l = side == 0 ? x : x - (nx - npml - 1);
-  }
-  const bool updx = in && x >= 1;
-  const bool xs = side >= 0 && updx;
-  const int sd = side >= 0 ? side : 0, ll = side >= 0 ? l : 0;
-  float mx = c.sXv[(sd * c.R + r) * S.nvp + ll];
-  const float axe = side >= 0 ? c.co[2 * npml + sd * nm + ll] : 0.f;
-  const float bxe = side >= 0 ? c.co[6 * npml + 2 + sd * nm + ll] : 0.f;
-  vx = v_cell_slow<R>(c.sVx[o], __fsub_rn(Pc, Pxm), g.fv, g.rdx, updx, (nib >> 1) & 1u, xs, mx,
-                      axe, bxe);
-  float dm = 0.f;
-  vy = v_cell_slow<R>(c.sVy[o], __fsub_rn(Pc, Pym), g.fv, g.rdy, in && j >= 1, (nib >> 2) & 1u,
-                      false, dm, 0.f, 0.f);
-  vz = v_cell_slow<R>(c.sVz[o], __fsub_rn(Pc, Pzm), g.fv, g.rdz, in && c.pl >= 1,
-                      (nib >> 3) & 1u, false, dm, 0.f, 0.f);
-  if (xs)
-    S.psi_v[0][c.wb * S.psi_v_buf[0] + sd * S.psi_v_side[0] +
-               ((long long)c.pl * S.ny + j) * S.nvp + ll] = mx;
-}
-
-// ---- fast paths: every cell of the quad is an interior cell of its update
-// (no rigid plane, no CPML slab, no grid edge); branch-free 4-wide code.
-template <typename R>
-__device__ __forceinline__ float p_cell(float P, float dvx, float dvy, float dvz, R fq, R rdx,
-                                        R rdy, R rdz, uint32_t open) {
-  using A = Arith<R>;
-  const R s = A::add(A::add(A::mul(A::cv(dvx), rdx), A::mul(A::cv(dvy), rdy)),
-                     A::mul(A::cv(dvz), rdz));
-  const float n = A::rn(A::sub(A::cv(P), A::mul(fq, s)));
-  return open ? n : P;
-}
-
-template <typename R>
-__device__ __forceinline__ float v_cell(float V, float dp, R fv, R rd, uint32_t open) {
-  using A = Arith<R>;
-  const float n = A::rn(A::sub(A::cv(V), A::mul(fv, A::mul(A::cv(dp), rd))));
-  return open ? n : V;
-}
-
-template <typename R>
-__device__ __forceinline__ void p_quad_fast(const Regs<R>& g, const float* __restrict__ sp,
-                                            const float* __restrict__ sx,
-                                            const float* __restrict__ sy,
-                                            const float* __restrict__ sz,
-                                            float* __restrict__ out, uint32_t nib) {
-  const int nxp = g.nxp;
-  const float4 P4 = ld4(sp), X4 = ld4(sx), Y0 = ld4(sy), Y1 = ld4(sy + nxp), Z0 = ld4(sz),
-               Z1 = ld4(sz + g.R2 * nxp);
-  const float X5 = sx[4];
-  float4 o;
-  o.x = p_cell<R>(P4.x, __fsub_rn(X4.y, X4.x), __fsub_rn(Y1.x, Y0.x), __fsub_rn(Z1.x, Z0.x),
-                  g.fq, g.rdx, g.rdy, g.rdz, nib & 1u);
-  o.y = p_cell<R>(P4.y, __fsub_rn(X4.z, X4.y), __fsub_rn(Y1.y, Y0.y), __fsub_rn(Z1.y, Z0.y),
-                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x10u);
-  o.z = p_cell<R>(P4.z, __fsub_rn(X4.w, X4.z), __fsub_rn(Y1.z, Y0.z), __fsub_rn(Z1.z, Z0.z),
-                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x100u);
-  o.w = p_cell<R>(P4.w, __fsub_rn(X5, X4.w), __fsub_rn(Y1.w, Y0.w), __fsub_rn(Z1.w, Z0.w),
-                  g.fq, g.rdx, g.rdy, g.rdz, nib & 0x1000u);
-  st4(out, o);
-}
-
-template <typename R>
-__device__ __forceinline__ void v_quad_fast(const Regs<R>& g, const float* __restrict__ pc,
-                                            const float* __restrict__ pz,
-                                            const float* __restrict__ sx,
-                                            const float* __restrict__ sy,
-                                            const float* __restrict__ sz, uint32_t nib,
-                                            float4& vx, float4& vy, float4& vz) {
-  const float4 Pc = ld4(pc), Pym = ld4(pc - g.nxp), Pzm = ld4(pz);
-  const float Pxm = pc[-1];
-  const float4 VX = ld4(sx), VY = ld4(sy), VZ = ld4(sz);
-  vx.x = v_cell<R>(VX.x, __fsub_rn(Pc.x, Pxm), g.fv, g.rdx, nib & 0x2u);
-  vx.y = v_cell<R>(VX.y, __fsub_rn(Pc.y, Pc.x), g.fv, g.rdx, nib & 0x20u);
-  vx.z = v_cell<R>(VX.z, __fsub_rn(Pc.z, Pc.y), g.fv, g.rdx, nib & 0x200u);
-  vx.w = v_cell<R>(VX.w, __fsub_rn(Pc.w, Pc.z), g.fv, g.rdx, nib & 0x2000u);
-  vy.x = v_cell<R>(VY.x, __fsub_rn(Pc.x, Pym.x), g.fv, g.rdy, nib & 0x4u);
-  vy.y = v_cell<R>(VY.y, __fsub_rn(Pc.y, Pym.y), g.fv, g.rdy, nib & 0x40u);
-  vy.z = v_cell<R>(VY.z, __fsub_rn(Pc.z, Pym.z), g.fv, g.rdy, nib & 0x400u);
-  vy.w = v_cell<R>(VY.w, __fsub_rn(Pc.w, Pym.w), g.fv, g.rdy, nib & 0x4000u);
-  vz.x = v_cell<R>(VZ.x, __fsub_rn(Pc.x, Pzm.x), g.fv, g.rdz, nib & 0x8u);
-  vz.y = v_cell<R>(VZ.y, __fsub_rn(Pc.y, Pzm.y), g.fv, g.rdz, nib & 0x80u);
-  vz.z = v_cell<R>(VZ.z, __fsub_rn(Pc.z, Pzm.z), g.fv, g.rdz, nib & 0x800u);
-  vz.w = v_cell<R>(VZ.w, __fsub_rn(Pc.w, Pzm.w), g.fv, g.rdz, nib & 0x8000u);
-}
-
-// interp_trilinear! entries of one (tile, plane, channel) in transceiver
-// order per cell: rec += w*f (stored per entry, summed by the epilogue in
-// corner order), then f += w*src[it].  A segment with one entry carries it
-// inline {cell | 1<<16, w, slot, src column}; longer ones point at the
-// entry arrays {cell | n<<16, first entry, 0, 0}.
-__device__ __forceinline__ void process_entries(const SolveDev& S, int b, int e, int chan,
-                                                float* cells, bool records, int it) {
+// ---------------------------------------------------------------------------
+// interp_trilinear! entries of one (y tile, plane, channel) bucket
+// (derivatives.jl:30-60).  Segments are cells {cell = r*nxp + x | n << 16};
+// inside a cell the entries are in transceiver order: rec += w*f (stored per
+// entry, summed by the epilogue in corner order), then f += w*src[it].  The
+// CTA handles the cells of its x range [x_lo, x_hi) and records only those
+// it owns (row >= 1, x >= xb; the P bucket also carries the tile's halo row
+// with slot -1).  `cells` maps (r, x) -> shared memory.
+// ---------------------------------------------------------------------------
+template <typename CellAt>
+__device__ __forceinline__ void apply_entries(const SolveDev& S, int b, int e, int chan, int nxp,
+                                              int x_lo, int x_hi, int xb, bool records, int it,
+                                              int tid, int nthr, CellAt cell_at) {
   const float* src = S.src[chan] + (long long)(it - 1) * S.src_ntx;
-  for (int si = b + (int)threadIdx.x; si < e; si += NCT) {
+  for (int si = b + tid; si < e; si += nthr) {
     const int4 sg = __ldg(S.seg + si);
     const int cell = sg.x & 0xFFFF, cnt = (int)((unsigned)sg.x >> 16);
-    float v = cells[cell];
+    const int r = cell / nxp, x = cell - r * nxp;
+    if (x < x_lo || x >= x_hi) continue;
+    const bool rec = records && r >= 1 && x >= xb;
+    float* c = cell_at(r, x);
+    float v = *c;
     if (cnt == 1) {
       const float w = __int_as_float(sg.y);
-      if (records && sg.z >= 0) S.contrib[sg.z] = __fmul_rn(w, v);
+      if (rec && sg.z >= 0) S.contrib[sg.z] = __fmul_rn(w, v);
       if (sg.w >= 0) v = __fadd_rn(v, __fmul_rn(w, __ldg(src + sg.w)));
     } else {
-      for (int k = sg.y; k < sg.y + cnt; ++k) {
-        const float w = __ldg(S.ent_w + k);
-        const int slot = __ldg(S.ent_slot + k);
-        if (records && slot >= 0) S.contrib[slot] = __fmul_rn(w, v);
-        const int col = __ldg(S.ent_tx + k);
+      for (int kk = sg.y; kk < sg.y + cnt; ++kk) {
+        const float w = __ldg(S.ent_w + kk);
+        const int slot = __ldg(S.ent_slot + kk);
+        if (rec && slot >= 0) S.contrib[slot] = __fmul_rn(w, v);
+        const int col = __ldg(S.ent_tx + kk);
         if (col >= 0) v = __fadd_rn(v, __fmul_rn(w, __ldg(src + col)));  // receivers: src == 0
       }
     }
-    cells[cell] = v;
+    *c = v;
   }
 }
 
-__device__ __forceinline__ void store_outputs(const SolveDev& S, const PlaneCtx& c, int r, int q,
-                                              float4 P4, float4 vx, float4 vy, float4 vz) {
-  const int j = c.j0 - 1 + r;
-  const int pl = c.pl;
-  float* out = S.field + (long long)c.wb * S.buf_stride;
-  const long long row = ((long long)pl * S.ny + j) * S.nxp + 4 * q;
-  st4(out + row, P4);
-  st4(out + S.chan_stride + row, vx);
-  // rigid mirrors (forward.jl:134-137): Vy[:,1,:] = -Vy[:,2,:], Vz[:,:,1] = -Vz[:,:,2]
-  if (j != 0) st4(out + 2 * S.chan_stride + row, vy);
-  if (j == 1)
-    st4(out + 2 * S.chan_stride + row - S.nxp, make_float4(-vy.x, -vy.y, -vy.z, -vy.w));
-  if (pl != 0) st4(out + 3 * S.chan_stride + row, vz);
-  if (pl == 1)
-    st4(out + 3 * S.chan_stride + row - (long long)S.ny * S.nxp,
-        make_float4(-vz.x, -vz.y, -vz.z, -vz.w));
+// ---- plain quads: every cell interior for its update (no rigid plane, no
+// CPML slab, no grid edge); the same arithmetic as the general functions
+// for such cells, without their conditions.
+template <typename R>
+__device__ __forceinline__ float p_plain(float P, float dx, float dy, float dz, const Sc<R>& g) {
+  using A = Arith<R>;
+  const R s = A::add(A::add(A::mul(A::cv(dx), g.rdx), A::mul(A::cv(dy), g.rdy)),
+                     A::mul(A::cv(dz), g.rdz));
+  return A::rn(A::sub(A::cv(P), A::mul(g.fq, s)));
 }
-
-__device__ __forceinline__ void store_cell(const SolveDev& S, const PlaneCtx& c, int r, int x,
-                                           float P, float vx, float vy, float vz) {
-  const int j = c.j0 - 1 + r;
-  const int pl = c.pl;
-  float* out = S.field + (long long)c.wb * S.buf_stride;
-  const long long cell = ((long long)pl * S.ny + j) * S.nxp + x;
-  out[cell] = P;
-  out[S.chan_stride + cell] = vx;
-  if (j != 0) out[2 * S.chan_stride + cell] = vy;
-  if (j == 1) out[2 * S.chan_stride + cell - S.nxp] = -vy;
-  if (pl != 0) out[3 * S.chan_stride + cell] = vz;
-  if (pl == 1) out[3 * S.chan_stride + cell - (long long)S.ny * S.nxp] = -vz;
+template <typename R>
+__device__ __forceinline__ float v_plain(float V, float dp, R rd, const Sc<R>& g) {
+  using A = Arith<R>;
+  return A::rn(A::sub(A::cv(V), A::mul(g.fv, A::mul(A::cv(dp), rd))));
 }
-
-// Work index -> (row, quad, cell) for an ordinary tile-plane.  Boundary quads
-// (the first nl and the last nb-nl quads of a row) are split into their four
-// cells, one cell per thread, so that the longer boundary update is spread
-// over several warps instead of making one warp the critical path of the
-// plane.  Work units: the interior quads of every row, then the boundary
-// cells.  Division by the per-row counts uses a 32.32 reciprocal (exact for
-// u, divisor < 2^16).
-struct XSplit {
-  int nl, ni, nb, na, na_pad, total;
-  unsigned long long mb, mi;
-  // u -> (row, quad, cell); cell = -1 for an interior quad (all four cells).
-  // Interior quads come first, so the threads whose unit is a boundary cell
-  // are the ones without a second unit in phases with more units than
-  // threads.
-  __device__ __forceinline__ void map(int u, int& row, int& q, int& e) const {
-    const int nint = total - na_pad;
-    if (u < nint) {
-      row = (int)(((unsigned long long)u * mi) >> 32);
-      q = nl + u - row * ni;
-      e = -1;
-      return;
-    }
-    u -= nint;
-    if (u >= na) { row = -1; e = 0; return; }
-    row = (int)(((unsigned long long)u * mb) >> 32);
-    const int k = u - row * 4 * nb;
-    const int kq = k >> 2;
-    q = kq < nl ? kq : kq + ni;
-    e = k & 3;
+template <typename R, bool MASK>
+__device__ __forceinline__ float4 p_plain_quad(const Sc<R>& g, float4 P4, float4 X4, float X5,
+                                               float4 Y0, float4 Y1, float4 Z0, float4 Z1,
+                                               uint32_t nib) {
+  float4 n;
+  n.x = p_plain<R>(P4.x, __fsub_rn(X4.y, X4.x), __fsub_rn(Y1.x, Y0.x), __fsub_rn(Z1.x, Z0.x), g);
+  n.y = p_plain<R>(P4.y, __fsub_rn(X4.z, X4.y), __fsub_rn(Y1.y, Y0.y), __fsub_rn(Z1.y, Z0.y), g);
+  n.z = p_plain<R>(P4.z, __fsub_rn(X4.w, X4.z), __fsub_rn(Y1.z, Y0.z), __fsub_rn(Z1.z, Z0.z), g);
+  n.w = p_plain<R>(P4.w, __fsub_rn(X5, X4.w), __fsub_rn(Y1.w, Y0.w), __fsub_rn(Z1.w, Z0.w), g);
+  if (MASK) {
+    n.x = (nib & 1u) ? n.x : P4.x;
+    n.y = (nib & 0x10u) ? n.y : P4.y;
+    n.z = (nib & 0x100u) ? n.z : P4.z;
+    n.w = (nib & 0x1000u) ? n.w : P4.w;
   }
-};
-__device__ __forceinline__ XSplit make_split(int xmin, int xmax, int nq, int nrows) {
-  XSplit s;
-  s.nl = (xmin + 3) / 4;                     // quads with x0 < xmin
-  const int qhi = xmax >= 3 ? (xmax - 3) / 4 : -1;  // last quad with x0+3 <= xmax
-  s.ni = max(0, min(qhi, nq - 1) - s.nl + 1);
-  s.nb = nq - s.ni;
-  s.na = nrows * s.nb * 4;
-  s.na_pad = (s.na + 31) / 32 * 32;
-  s.total = s.na_pad + nrows * s.ni;
-  s.mb = s.nb ? ((1ull << 32) + 4 * s.nb - 1) / (4 * s.nb) : 0;
-  s.mi = s.ni ? ((1ull << 32) + s.ni - 1) / s.ni : 0;
-  return s;
+  return n;
 }
+template <typename R, bool MASK>
+__device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Pxm, float4 Pym,
+                                             float4 Pzm, float4 VX, float4 VY, float4 VZ,
+                                             uint32_t nib, float4& vx, float4& vy, float4& vz) {
+  vx.x = v_plain<R>(VX.x, __fsub_rn(Pc.x, Pxm), g.rdx, g);
+  vx.y = v_plain<R>(VX.y, __fsub_rn(Pc.y, Pc.x), g.rdx, g);
+  vx.z = v_plain<R>(VX.z, __fsub_rn(Pc.z, Pc.y), g.rdx, g);
+  vx.w = v_plain<R>(VX.w, __fsub_rn(Pc.w, Pc.z), g.rdx, g);
+  vy.x = v_plain<R>(VY.x, __fsub_rn(Pc.x, Pym.x), g.rdy, g);
+  vy.y = v_plain<R>(VY.y, __fsub_rn(Pc.y, Pym.y), g.rdy, g);
+  vy.z = v_plain<R>(VY.z, __fsub_rn(Pc.z, Pym.z), g.rdy, g);
+  vy.w = v_plain<R>(VY.w, __fsub_rn(Pc.w, Pym.w), g.rdy, g);
+  vz.x = v_plain<R>(VZ.x, __fsub_rn(Pc.x, Pzm.x), g.rdz, g);
+  vz.y = v_plain<R>(VZ.y, __fsub_rn(Pc.y, Pzm.y), g.rdz, g);
+  vz.z = v_plain<R>(VZ.z, __fsub_rn(Pc.z, Pzm.z), g.rdz, g);
+  vz.w = v_plain<R>(VZ.w, __fsub_rn(Pc.w, Pzm.w), g.rdz, g);
+  if (MASK) {
+    vx.x = (nib & 0x2u) ? vx.x : VX.x;
+    vx.y = (nib & 0x20u) ? vx.y : VX.y;
+    vx.z = (nib & 0x200u) ? vx.z : VX.z;
+    vx.w = (nib & 0x2000u) ? vx.w : VX.w;
+    vy.x = (nib & 0x4u) ? vy.x : VY.x;
+    vy.y = (nib & 0x40u) ? vy.y : VY.y;
+    vy.z = (nib & 0x400u) ? vy.z : VY.z;
+    vy.w = (nib & 0x4000u) ? vy.w : VY.w;
+    vz.x = (nib & 0x8u) ? vz.x : VZ.x;
+    vz.y = (nib & 0x80u) ? vz.y : VZ.y;
+    vz.z = (nib & 0x800u) ? vz.z : VZ.z;
+    vz.w = (nib & 0x8000u) ? vz.w : VZ.w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The step kernel.  One CTA per work item {solve, y tile | x tile << 16, z0,
+// z1}: a tile of ty <= 8 rows j0..j0+ty-1 and the 128 cells xb..xb+127 of
+// one solve, and the planes z0..z1-1.  blockDim = (32, 9).  Warps 0-7 each
+// hold 8 quads x 4 rows of the tile (warp w: quads 8(w%4)..+7, rows
+// 1+4(w/4)..+3 in tile-row numbering, row r = j - j0 + 1); warp 8 holds the
+// halo row r = 0 (j0-1), whose new P the Vy update of row j0 needs: it is
+// recomputed, not exchanged.  The lanes of quad 0 also recompute the halo
+// column x = xb-1 (for Vx at xb).  With this shape the x-slab quads of a
+// tile sit in one warp column, so only those warps take the CPML branch.
+// Per plane, after a prologue plane z0-1 (new P only, for Vz at z0) when
+// z0 > 0:
+//   loads  : P, Vx, Vy of plane k and Vz of plane k+1 (Vz of plane k and the
+//            new P of plane k-1 are carried in registers), 128-bit, coalesced;
+//   P      : new P into a double-buffered shared plane; barrier;
+//   q      : injection/recording on P (only planes with entries; barrier);
+//   V      : Vx/Vy/Vz from the new P (x-1 and y-1 neighbours from shared
+//            memory);
+//   f      : injection/recording on V (only planes with entries: staged in
+//            shared memory between two barriers);
+//   stores : 128-bit stores of the four channels and the rigid mirrors.
+// A warp whose quads are all plain for this plane (the bulk of the grid)
+// takes the plain functions (warp-uniform branch); the rest the general
+// ones.  Several CTAs per SM keep enough independent warps in flight to
+// cover the latency of the float/double chains and of HBM.
+// ---------------------------------------------------------------------------
+constexpr int kMaxTy = 8;           // rows per tile
+constexpr int kXT = 128;            // cells per x tile
+constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..131] = cells
+constexpr int kStepThreads = 32 * (kMaxTy + 1);
 
 template <typename R>
-__device__ bool consume_item(const StepParams& p, const SolveDev& S, int4 item, int it,
-                             uint64_t* full, uint64_t* empty, float* ring, float* pn, int& n,
-                             volatile int* s_fail, const float* s_co) {
-  using A = Arith<R>;
-  const int rb = (it - S.it_first) & 1;
-  const int ty = S.ty, nxp = S.nxp, nq = nxp / 4;
-  const int j0 = item.y * ty;
-  const int Rr = ty + 2;
+__device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
+                                          float* sPn, float* sV, const float* co) {
+  const int lane = threadIdx.x, wid = threadIdx.y;
+  const int tid = wid * 32 + lane, nthr = blockDim.x * blockDim.y;
+  const int nx = S.nx, ny = S.ny, nz = S.nz, nxp = S.nxp, ty = S.ty, npml = S.npml;
+  const int T = item.y & 0xFFFF, X = item.y >> 16;
+  const int j0 = T * ty, xb = X * kXT;
+  int r, qx, wr0, wnr, wq0, wnq;  // this thread's row and quad; its warp's rows and quads
+  if (wid < 8) {
+    const int wx = wid & 3, wy = wid >> 2;
+    qx = 8 * wx + (lane & 7);
+    r = 1 + 4 * wy + (lane >> 3);
+    wq0 = 8 * wx;
+    wnq = 8;
+    wr0 = 1 + 4 * wy;
+    wnr = 4;
+  } else {
+    qx = lane;
+    r = 0;
+    wq0 = 0;
+    wnq = 32;
+    wr0 = 0;
+    wnr = 1;
+  }
+  const int j = j0 - 1 + r, x0 = xb + 4 * qx;
+  const bool row_ok = r <= ty && j >= 0 && j < ny;
+  const bool act = row_ok && x0 < nxp;  // this thread updates a quad
+  const bool vrow = act && r >= 1;      // ... and owns it (velocity update, stores)
+  const int rb = (it - S.it_first) & 1, wb = rb ^ 1;
+  const long long cs = S.chan_stride, plane = (long long)ny * nxp;
+  const float* fin = S.field + rb * S.buf_stride;
+  float* fout = S.field + wb * S.buf_stride;
   const bool has_mask = (S.flags & SF_MASK) != 0;
-  const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
-  const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
-                                   vcpml ? S.nvp : 0, !(S.flags & SF_YZG));
-  const int pz0 = item.z > 0 ? item.z - 1 : 0;
-  const int tid = threadIdx.x;
-  Regs<R> g;
-  g.nxp = nxp;
-  g.R2 = Rr;
-  g.fq = A::fq(S);
-  g.fv = A::fv(S);
-  g.rdx = A::rdx(S);
-  g.rdy = A::rdy(S);
-  g.rdz = A::rdz(S);
-  const int nx = S.nx, ny = S.ny, nz = S.nz, npml = S.npml, mw = S.mw;
-  // thread -> (row, quad) walk: stride NCT over rows of nq quads
-  const int dr = NCT / nq, dq = NCT - (NCT / nq) * nq;
-  const int r_first = tid / nq, q_first = tid - r_first * nq;
-  // x ranges where every cell of a quad takes the plain update
-  const int p_xmin = pcpml ? npml : 0;
-  const int p_xmax = pcpml ? min(nx - 2, nx - npml - 1) : nx - 2;
-  const int v_xmin = vcpml ? npml + 1 : 1;
-  const int v_xmax = vcpml ? nx - npml - 2 : nx - 1;
-  // Ordinary tile-planes: boundary quads (x slab / x edges) are packed into
-  // whole warps ahead of the interior quads, so interior warps never diverge
-  // into the boundary path.  Row range and x classes per phase:
-  const int rP0 = j0 == 0 ? 1 : 0, rP1 = min(ty, ny - j0);
-  const int rV1 = min(ty, ny - j0);
-  bool tileP = rP1 >= rP0, tileV = rV1 >= 1;
-  for (int r = rP0; r <= rP1; ++r) {
-    const int j = j0 - 1 + r;
-    tileP = tileP && (j != ny - 1) && (!pcpml || (j >= npml && j < ny - npml));
-  }
-  for (int r = 1; r <= rV1; ++r) {
-    const int j = j0 - 1 + r;
-    tileV = tileV && j >= 1 && (!vcpml || (j > npml && j < ny - npml - 1));
-  }
-  const XSplit sP = make_split(p_xmin, p_xmax, nq, rP1 - rP0 + 1);
-  const XSplit sV = make_split(v_xmin, v_xmax, nq, rV1);
-  tileP = tileP && sP.ni > 0;
-  tileV = tileV && sV.ni > 0;
-  for (int pl = pz0; pl < item.w; ++pl, ++n) {
-    const int slot = n % p.stages;
-    const int round = n / p.stages;
-    // every consumer thread waits; a thread that gives up skips the P phase
-    // and the abort is decided uniformly after the barrier below, so no
-    // thread is ever left alone in bar.sync
-    const bool landed = mbar_wait(smem_u32(&full[slot]), round & 1);
-    if (!landed) *s_fail = 1;
-    const bool prologue = pl < item.z;
-    float* base = ring + (long long)slot * p.stage_floats;
-    PlaneCtx c;
-    c.sP = base;
-    c.sVx = base + L.reg;
-    c.sVy = base + 2 * L.reg;
-    c.sVz = base + L.off_vz;
-    c.sM = reinterpret_cast<const uint32_t*>(base + L.off_m);
-    c.sXp = base + L.off_xp;
-    c.sXv = base + L.off_xv;
-    c.yP = base + L.off_py;
-    c.yV = base + L.off_vy;
-    c.zP = base + L.off_pz;
-    c.zV = base + L.off_vz2;
-    c.co = s_co;
-    c.ysP = (pcpml && !(S.flags & SF_YZG)) ? tile_yside(j0, ty, ny, npml) : -1;
-    c.ysV = (vcpml && !(S.flags & SF_YZG)) ? tile_yside(j0, ty, ny, npml + 1) : -1;
-    c.pn_cur = pn + (n % kPnBufs) * p.pn_floats;
-    c.pn_prev = pn + ((n + kPnBufs - 1) % kPnBufs) * p.pn_floats;
-    c.j0 = j0;
-    c.R = Rr;
-    c.pl = pl;
-    c.rb = rb;
-    c.wb = rb ^ 1;
-    c.has_mask = has_mask;
-    // ---- P phase: rows j0-1 .. j0+ty-1 ----
-    if (landed) {
-      const bool pl_plain = !(pl == nz - 1) && (!pcpml || (pl >= npml && pl < nz - npml));
-      auto p_work = [&](int r, int q, bool fast) {
-        if (fast) {
-          uint32_t nib = 0xFFFFu;
-          if (has_mask) nib = (c.sM[r * mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-          const int o = r * nxp + 4 * q;
-          p_quad_fast<R>(g, c.sP + o, c.sVx + o, c.sVy + o, c.sVz + o, c.pn_cur + o, nib);
-        } else {
-          p_quad<R>(S, g, c, r, q, !prologue && r >= 1);
-        }
-      };
-      if (pl_plain && tileP) {
-        for (int u = tid; u < sP.total; u += NCT) {
-          int row, q, e;
-          sP.map(u, row, q, e);
-          if (row < 0) continue;
-          if (e < 0)
-            p_work(rP0 + row, q, true);
-          else
-            p_xcell<R>(S, g, c, rP0 + row, 4 * q + e, !prologue && rP0 + row >= 1);
-        }
-      } else {
-        for (int r = r_first, q = q_first; r <= ty; q += dq, r += dr) {
-          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
-          const int j = j0 - 1 + r;
-          if (j < 0 || j >= ny) continue;
-          const int x0 = 4 * q;
-          const bool row_plain = (j != ny - 1) && (!pcpml || (j >= npml && j < ny - npml));
-          p_work(r, q, pl_plain && row_plain && x0 + 3 <= p_xmax && x0 >= p_xmin);
-        }
-      }
+  const bool pcp = (S.flags & SF_PCPML) != 0, vcp = (S.flags & SF_VCPML) != 0;
+  Sc<R> g;
+  g.fq = Arith<R>::fq(S);
+  g.fv = Arith<R>::fv(S);
+  g.rdx = Arith<R>::rdx(S);
+  g.rdy = Arith<R>::rdy(S);
+  g.rdz = Arith<R>::rdz(S);
+  RowCtx rc;
+  rc.nx = nx;
+  rc.ny = ny;
+  rc.nz = nz;
+  rc.npml = npml;
+  rc.nxp = nxp;
+  rc.j = j;
+  rc.rb = rb;
+  rc.wb = wb;
+  rc.pcpml = pcp;
+  rc.vcpml = vcp;
+  // warp-uniform: do all of the warp's rows and x cells take the plain P
+  // (and, rows >= 1, V) updates?  The plane is checked per plane below.
+  bool wplain_rx;
+  {
+    const int wj0 = j0 - 1 + wr0, wj1 = wj0 + wnr - 1;
+    const int wx0 = xb + 4 * wq0, wx1 = wx0 + 4 * wnq - 1;
+    const int p_xmin = pcp ? npml : 0, p_xmax = pcp ? min(nx - 2, nx - npml - 1) : nx - 2;
+    const int v_xmin = vcp ? npml + 1 : 1, v_xmax = vcp ? nx - npml - 2 : nx - 1;
+    bool ok = wr0 + wnr - 1 <= ty && wj0 >= 0 && wx1 < nxp;
+    ok = ok && wj1 < ny - 1 && (!pcp || (wj0 >= npml && wj1 < ny - npml));
+    ok = ok && wx0 >= p_xmin && wx1 <= p_xmax;
+    if (wr0 >= 1) {
+      ok = ok && wj0 >= 1 && (!vcp || (wj0 > npml && wj1 < ny - npml - 1));
+      ok = ok && wx0 >= v_xmin && wx1 <= v_xmax;
     }
-    consumer_bar();
-    if (*s_fail) {
-      if (tid == 0) atomicExch(p.err, KERR_FULL_TIMEOUT);
-      return false;
+    wplain_rx = ok;
+  }
+  const long long rowoff = (long long)(row_ok ? j : 0) * nxp + x0;
+  const int pq = r * kPnPitch + 4 + 4 * qx;  // this quad in a shared new-P plane
+  const int z0 = item.z, z1 = item.w;
+  const int kfirst = z0 > 0 ? z0 - 1 : z0;
+  float4 Z0 = make_float4(0.f, 0.f, 0.f, 0.f), Pzm = Z0;
+  if (act) Z0 = ldg4(fin + 3 * cs + kfirst * plane + rowoff);
+  const int* tp = S.tp_off + (long long)T * nz * 4;
+  for (int k = kfirst; k < z1; ++k) {
+    const bool prologue = k < z0;
+    rc.k = k;
+    float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
+    const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
+    const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
+    const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
+    const bool wplain = wplain_rx && pplane && (wr0 == 0 || prologue || vplane);
+    float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), X4 = Pn, Y0 = Pn, Z1 = Pn;
+    uint32_t nib = 0xFFFFu;
+    if (act) {
+      const float* b = fin + k * plane + rowoff;
+      const float4 P4 = ldg4(b);
+      X4 = ldg4(b + cs);
+      Y0 = ldg4(b + 2 * cs);
+      const float X5 = x0 + 4 < nxp ? __ldg(b + cs + 4) : 0.f;
+      const float4 Y1 = j + 1 < ny ? ldg4(b + 2 * cs + nxp) : Pn;
+      Z1 = k + 1 < nz ? ldg4(b + 3 * cs + plane) : Pn;
+      if (has_mask)
+        nib = (__ldg(S.mask_bits + ((long long)k * ny + j) * S.mw + (x0 >> 3)) >> ((x0 & 4) * 4)) &
+              0xFFFFu;
+      if (wplain)
+        Pn = has_mask ? p_plain_quad<R, true>(g, P4, X4, X5, Y0, Y1, Z0, Z1, nib)
+                      : p_plain_quad<R, false>(g, P4, X4, X5, Y0, Y1, Z0, Z1, nib);
+      else
+        Pn = p_update_quad<R>(S, rc, g, co, x0, vrow && !prologue, P4, X4, X5, Y0, Y1, Z0, Z1, nib);
+      st4(pn + pq, Pn);
     }
-    // ---- Q phase: q-channel inject/record on P (forward.jl:92) ----
-    const int* hdr = reinterpret_cast<const int*>(base + p.stage_floats - 32);
-    const int off0 = hdr[0], off1 = hdr[1], off2 = hdr[2], off3 = hdr[3], off4 = hdr[4];
+    if (qx == 0 && r >= 1 && row_ok && xb > 0) pn[pq - 1] = p_update_cell<R>(S, rc, g, co, fin, xb - 1);
+    __syncthreads();
+    // ---- q channel: inject/record on the new P (forward.jl:92) ----
     if (off0 < off1) {
-      process_entries(S, off0, off1, 0, c.pn_cur, !prologue, it);
-      consumer_bar();
+      apply_entries(S, off0, off1, 0, nxp, xb - 1, xb + kXT, xb, !prologue, it, tid, nthr,
+                    [&](int rr, int x) { return pn + rr * kPnPitch + (x - xb + 4); });
+      __syncthreads();
+      if (act) Pn = ld4(pn + pq);
     }
     if (!prologue) {
-      const bool has_f = off1 < off4;
-      const bool pl_vplain = pl >= 1 && (!vcpml || (pl > npml && pl < nz - npml - 1));
-      auto v_work = [&](int r, int q, bool fast) {
-        float4 vx, vy, vz;
-        const int o = r * nxp + 4 * q;
-        if (fast) {
-          uint32_t nib = 0xFFFFu;
-          if (has_mask) nib = (c.sM[r * mw + (q >> 1)] >> ((q & 1) * 16)) & 0xFFFFu;
-          v_quad_fast<R>(g, c.pn_cur + o, c.pn_prev + o, c.sVx + o, c.sVy + o, c.sVz + o, nib,
-                         vx, vy, vz);
+      float4 vx = Pn, vy = Pn, vz = Pn;
+      if (vrow) {
+        const float Pxm = pn[pq - 1];
+        const float4 Pym = ld4(pn + pq - kPnPitch);
+        if (wplain) {
+          if (has_mask)
+            v_plain_quad<R, true>(g, Pn, Pxm, Pym, Pzm, X4, Y0, Z0, nib, vx, vy, vz);
+          else
+            v_plain_quad<R, false>(g, Pn, Pxm, Pym, Pzm, X4, Y0, Z0, nib, vx, vy, vz);
         } else {
-          v_quad<R>(S, g, c, r, q, vx, vy, vz);
-        }
-        if (has_f) {  // stage into this slot's own rows (only this thread reads them)
-          st4(const_cast<float*>(c.sVx) + o, vx);
-          st4(const_cast<float*>(c.sVy) + o, vy);
-          st4(const_cast<float*>(c.sVz) + o, vz);
-        } else {
-          store_outputs(S, c, r, q, ld4(c.pn_cur + o), vx, vy, vz);
-        }
-      };
-      if (pl_vplain && tileV) {
-        for (int u = tid; u < sV.total; u += NCT) {
-          int row, q, e;
-          sV.map(u, row, q, e);
-          if (row < 0) continue;
-          if (e < 0) {
-            v_work(1 + row, q, true);
-          } else {
-            const int r = 1 + row, x = 4 * q + e, o = r * nxp + x;
-            float vx, vy, vz;
-            v_xcell<R>(S, g, c, r, x, vx, vy, vz);
-            if (has_f) {  // stage into this slot's own row cells (only this thread reads them)
-              const_cast<float*>(c.sVx)[o] = vx;
-              const_cast<float*>(c.sVy)[o] = vy;
-              const_cast<float*>(c.sVz)[o] = vz;
-            } else {
-              store_cell(S, c, r, x, c.pn_cur[o], vx, vy, vz);
-            }
-          }
-        }
-      } else {
-        for (int r = 1 + r_first, q = q_first; r <= ty; q += dq, r += dr) {
-          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
-          const int j = j0 - 1 + r;
-          if (j >= ny) continue;
-          const int x0 = 4 * q;
-          const bool row_vplain = j >= 1 && (!vcpml || (j > npml && j < ny - npml - 1));
-          v_work(r, q, pl_vplain && row_vplain && x0 >= v_xmin && x0 + 3 <= v_xmax);
+          v_update_quad<R>(S, rc, g, co, x0, Pn, Pxm, Pym, Pzm, X4, Y0, Z0, nib, vx, vy, vz);
         }
       }
-      if (has_f) {
-        consumer_bar();
-        // ---- F phase: f-channel inject/record (forward.jl:111-115) ----
-        if (off1 < off2) process_entries(S, off1, off2, 1, const_cast<float*>(c.sVx), true, it);
-        if (off2 < off3) process_entries(S, off2, off3, 2, const_cast<float*>(c.sVy), true, it);
-        if (off3 < off4) process_entries(S, off3, off4, 3, const_cast<float*>(c.sVz), true, it);
-        consumer_bar();
-        for (int r = 1 + r_first, q = q_first; r <= ty; q += dq, r += dr) {
-          if (q >= nq) { q -= nq; ++r; if (r > ty) break; }
-          const int j = j0 - 1 + r;
-          if (j >= ny) continue;
-          const int o = r * nxp + 4 * q;
-          store_outputs(S, c, r, q, ld4(c.pn_cur + o), ld4(c.sVx + o), ld4(c.sVy + o),
-                        ld4(c.sVz + o));
+      // ---- f channel: inject/record on the new V (forward.jl:111-115) ----
+      if (off1 < off4) {
+        float* sVx = sV;
+        float* sVy = sV + kMaxTy * kXT;
+        float* sVz = sV + 2 * kMaxTy * kXT;
+        const int so = (r - 1) * kXT + 4 * qx;
+        if (vrow) {
+          st4(sVx + so, vx);
+          st4(sVy + so, vy);
+          st4(sVz + so, vz);
         }
-        // generic-proxy writes to the slot must be ordered before the next
-        // TMA write into it
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        for (int c = 1; c <= 3; ++c) {
+          const int b = __ldg(tp + 4 * k + c), e = __ldg(tp + 4 * k + c + 1);
+          if (b < e)
+            apply_entries(S, b, e, c, nxp, xb, xb + kXT, xb, true, it, tid, nthr,
+                          [&](int rr, int x) {
+                            return sV + (c - 1) * kMaxTy * kXT + (rr - 1) * kXT + (x - xb);
+                          });
+        }
+        __syncthreads();
+        if (vrow) {
+          vx = ld4(sVx + so);
+          vy = ld4(sVy + so);
+          vz = ld4(sVz + so);
+        }
+      }
+      if (vrow) {
+        float* o = fout + k * plane + rowoff;
+        st4(o, Pn);
+        st4(o + cs, vx);
+        // rigid mirrors (forward.jl:134-137): Vy[:,1,:] = -Vy[:,2,:], Vz[:,:,1] = -Vz[:,:,2]
+        if (j != 0) st4(o + 2 * cs, vy);
+        if (j == 1) st4(o + 2 * cs - nxp, neg4(vy));
+        if (k != 0) st4(o + 3 * cs, vz);
+        if (k == 1) st4(o + 3 * cs - plane, neg4(vz));
       }
     }
-    __syncwarp();
-    if ((tid & 31) == 0) mbar_arrive(smem_u32(&empty[slot]));
+    Pzm = Pn;
+    Z0 = Z1;
   }
-  return true;
 }
 
-// MINB = CTAs per SM the launch is sized for: 2 caps registers so two CTAs
-// fit, 1 gives the kernel the registers it needs without spilling.
-template <int MINB>
-__global__ void __launch_bounds__(NTHREADS, MINB) adf_fdtd_step_kernel(const StepParams p) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
-  uint64_t* empty = full + kMaxStages;
-  float* ring = reinterpret_cast<float*>(smem_raw + 256);
-  float* pn = ring + (long long)p.stages * p.stage_floats;
-  __shared__ int s_fail;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    s_fail = 0;
-    for (int s = 0; s < p.stages; ++s) {
-      mbar_init(smem_u32(&full[s]), 1);
-      mbar_init(smem_u32(&empty[s]), NCW);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+__global__ void __launch_bounds__(kStepThreads, 3) adf_fdtd_step_kernel(const StepParams p) {
+  __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
+  __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
+  __shared__ float s_co[kMaxCoef];
+  __shared__ __align__(16) SolveDev S;  // the solve descriptor, read in the hot loop
+  const int4 item = p.items[blockIdx.x];
+  const SolveDev& G = p.solves[item.x];
+  const int it = G.it_base + p.step;
+  if (it > G.it_stop) return;
+  const int tid = threadIdx.y * 32 + threadIdx.x, nthr = blockDim.x * blockDim.y;
+  {
+    const int* src = reinterpret_cast<const int*>(&G);
+    int* dst = reinterpret_cast<int*>(&S);
+    for (int w = tid; w < (int)(sizeof(SolveDev) / 4); w += nthr) dst[w] = src[w];
+    const int ncoef = 8 * G.npml + 4;
+    for (int w = tid; w < ncoef; w += nthr) s_co[w] = G.coef[w];
   }
   __syncthreads();
-
-  if (tid >= NCT) {
-    // ---------------- producer warp: TMA loads into the ring ----------------
-    if (tid != NCT) return;
-    int n = 0;
-    int last_round[kMaxStages];
-    for (int s = 0; s < kMaxStages; ++s) last_round[s] = -1;
-    int cur = -1;
-    for (int i = blockIdx.x; i < p.n_items; i += gridDim.x) {
-      if (*(volatile int*)p.err) break;
-      const int4 item = p.items[i];
-      const SolveDev& S = p.solves[item.x];
-      const int it = S.it_base + p.step;
-      if (it > S.it_stop) continue;
-      const int rb = (it - S.it_first) & 1;
-      const CUtensorMap* tm = p.tmaps + kTmaps * item.x;
-      if (item.x != cur) {
-        for (int k = 0; k < kTmaps; ++k) tmap_acquire(tm + k);
-        cur = item.x;
-      }
-      const int ty = S.ty, nxp = S.nxp, Rr = ty + 2;
-      const int j0 = item.y * ty;
-      const bool has_mask = (S.flags & SF_MASK) != 0;
-      const bool pcpml = (S.flags & SF_PCPML) != 0, vcpml = (S.flags & SF_VCPML) != 0;
-      const bool stage_yz = !(S.flags & SF_YZG);
-      const SlotLayout L = slot_layout(ty, nxp, has_mask ? S.mw : 0, pcpml ? S.npp : 0,
-                                       vcpml ? S.nvp : 0, stage_yz);
-      const uint32_t bytes0 =
-          (uint32_t)(5 * Rr * nxp * 4 + (has_mask ? Rr * S.mw * 4 : 0) +
-                     (pcpml ? 2 * Rr * S.npp * 4 : 0) + (vcpml ? 2 * Rr * S.nvp * 4 : 0));
-      const uint32_t box_bytes = (uint32_t)(Rr * nxp * 4);
-      const int ny = S.ny, nz = S.nz, npml = S.npml;
-      const int ysP = (pcpml && stage_yz) ? tile_yside(j0, ty, ny, npml) : -1;
-      const int ysV = (vcpml && stage_yz) ? tile_yside(j0, ty, ny, npml + 1) : -1;
-      const int pz0 = item.z > 0 ? item.z - 1 : 0;
-      bool ok = true;
-      for (int pl = pz0; pl < item.w; ++pl, ++n) {
-        const int slot = n % p.stages, round = n / p.stages;
-        if (!mbar_wait(smem_u32(&empty[slot]), (round & 1) ^ 1)) {
-          atomicExch(p.err, KERR_EMPTY_TIMEOUT);
-          ok = false;
-          break;
-        }
-        const uint32_t mb = smem_u32(&full[slot]);
-        float* base = ring + (long long)slot * p.stage_floats;
-        // bulk copies first (the transaction count may dip below zero until
-        // the arrive below adds the expected bytes; the phase cannot complete
-        // before that arrive)
-        tma_load_5d(smem_u32(base), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 0);
-        tma_load_5d(smem_u32(base + L.reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 1);
-        tma_load_5d(smem_u32(base + 2 * L.reg), tm, mb, 0, 0, j0 - 1, pl, 4 * rb + 2);
-        tma_load_5d(smem_u32(base + L.off_vz), tm + 1, mb, 0, 0, j0 - 1, pl, 4 * rb + 3);
-        if (has_mask) tma_load_3d(smem_u32(base + L.off_m), tm + 2, mb, 0, j0 - 1, pl);
-        // x-slab CPML memory of both sides: box (np, R, 1, 2) at (0, j0-1, pl, 2*rb)
-        if (pcpml) tma_load_4d(smem_u32(base + L.off_xp), tm + 3, mb, 0, j0 - 1, pl, 2 * rb);
-        if (vcpml) tma_load_4d(smem_u32(base + L.off_xv), tm + 4, mb, 0, j0 - 1, pl, 2 * rb);
-        // y-slab rows of the tile (rows outside the slab arrive as zeros) and
-        // the z-slab plane, p and v sides
-        uint32_t bytes = bytes0;
-        if (ysP >= 0) {
-          const int l0 = ysP == 0 ? j0 - 1 : j0 - 1 - (ny - npml);
-          tma_load_5d(smem_u32(base + L.off_py), tm + 5, mb, 0, 0, l0, pl, 2 * rb + ysP);
-          bytes += box_bytes;
-        }
-        if (ysV >= 0) {
-          const int l0 = ysV == 0 ? j0 - 1 : j0 - 1 - (ny - npml - 1);
-          tma_load_5d(smem_u32(base + L.off_vy), tm + 6, mb, 0, 0, l0, pl, 2 * rb + ysV);
-          bytes += box_bytes;
-        }
-        if (pcpml && stage_yz) {
-          const int zs = plane_zside(pl, nz, npml);
-          if (zs >= 0) {
-            const int l = zs == 0 ? pl : pl - (nz - npml);
-            tma_load_5d(smem_u32(base + L.off_pz), tm + 7, mb, 0, 0, j0 - 1, l, 2 * rb + zs);
-            bytes += box_bytes;
-          }
-        }
-        if (vcpml && stage_yz) {
-          const int zs = plane_zside(pl, nz, npml + 1);
-          if (zs >= 0) {
-            const int l = zs == 0 ? pl : pl - (nz - npml - 1);
-            tma_load_5d(smem_u32(base + L.off_vz2), tm + 8, mb, 0, 0, j0 - 1, l, 2 * rb + zs);
-            bytes += box_bytes;
-          }
-        }
-        {  // entry-list offsets of this (tile, plane), staged for the consumers
-          int* hdr = reinterpret_cast<int*>(base + p.stage_floats - 32);
-          const int tb = (item.y * S.nz + pl) * 4;
-          const int4 o4 = *reinterpret_cast<const int4*>(S.tp_off + tb);
-          hdr[0] = o4.x; hdr[1] = o4.y; hdr[2] = o4.z; hdr[3] = o4.w;
-          hdr[4] = S.tp_off[tb + 4];
-        }
-        mbar_expect_tx(mb, bytes);  // release: the header is visible after the wait
-        last_round[slot] = round;
-      }
-      if (!ok) break;
-    }
-    // never leave while a bulk copy into this CTA's shared memory is in flight
-    for (int s = 0; s < p.stages; ++s)
-      if (last_round[s] >= 0 && !mbar_wait(smem_u32(&full[s]), last_round[s] & 1))
-        atomicExch(p.err, KERR_DRAIN_TIMEOUT);
-    return;
-  }
-
-  // ---------------- consumer warps ----------------
-  // the solve descriptor is read from shared memory inside the hot loops
-  __shared__ __align__(16) SolveDev s_desc[2];
-  __shared__ float s_coef[2][kMaxCoef];
-  int n = 0, k_item = 0;
-  for (int i = blockIdx.x; i < p.n_items; i += gridDim.x) {
-    const int4 item = p.items[i];
-    const SolveDev& G = p.solves[item.x];
-    const int it = G.it_base + p.step;
-    if (it > G.it_stop) continue;
-    SolveDev& S = s_desc[k_item & 1];
-    float* co = s_coef[k_item & 1];
-    ++k_item;
-    {
-      const int* src = reinterpret_cast<const int*>(&G);
-      int* dst = reinterpret_cast<int*>(&S);
-      for (int w = tid; w < (int)(sizeof(SolveDev) / 4); w += NCT) dst[w] = src[w];
-      const int ncoef = 8 * G.npml + 4;
-      for (int w = tid; w < ncoef; w += NCT) co[w] = G.coef[w];
-      consumer_bar();
-    }
-    bool ok;
-    if (S.flags & SF_FP32)
-      ok = consume_item<float>(p, S, item, it, full, empty, ring, pn, n, &s_fail, co);
-    else
-      ok = consume_item<double>(p, S, item, it, full, empty, ring, pn, n, &s_fail, co);
-    if (!ok) return;
-    // items run in lock-step with the producer; if it stopped on an error
-    // flag the next full-barrier wait times out and returns here
-  }
+  if (S.flags & SF_FP32)
+    step_item<float>(p, S, item, it, sPn, sV, s_co);
+  else
+    step_item<double>(p, S, item, it, sPn, sV, s_co);
 }
 
 // Per-step trace assembly (derivatives.jl:51-56 record sums in corner order,
@@ -1191,23 +821,13 @@ cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-const void* step_kernel_ptr(bool two_per_sm) {
-  return two_per_sm ? (const void*)adf_fdtd_step_kernel<2> : (const void*)adf_fdtd_step_kernel<1>;
-}
-
-cudaError_t step_kernel_attributes(size_t smem, bool two_per_sm) {
-  return cudaFuncSetAttribute(step_kernel_ptr(two_per_sm),
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-
-cudaError_t launch_step(const StepParams& p, int grid, int block, size_t smem, cudaStream_t s,
-                        bool two_per_sm) {
-  if (two_per_sm)
-    adf_fdtd_step_kernel<2><<<grid, block, smem, s>>>(p);
-  else
-    adf_fdtd_step_kernel<1><<<grid, block, smem, s>>>(p);
+cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s) {
+  (void)max_ty;  // the block always holds kMaxTy rows; shorter tiles idle the rest
+  adf_fdtd_step_kernel<<<grid, dim3(32, kMaxTy + 1), 0, s>>>(p);
   return cudaGetLastError();
 }
+
+int step_max_ty() { return kMaxTy; }
 
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
                                   cudaStream_t s) {

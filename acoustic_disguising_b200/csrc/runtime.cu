@@ -79,14 +79,14 @@ static T* dalloc(Solve& s, size_t n, int& rc) {
 }
 
 void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, int& mw) {
-  xh = (nx + 255) / 256;
-  int q = 4 * xh;
-  nxp = (nx + q - 1) / q * q;
+  xh = 1;
+  nxp = (nx + 3) / 4 * 4;
   mw = ((nx + 7) / 8 + 3) / 4 * 4;
   const Tune t = tune_lookup(nx, ny, nz);
   ty = t.ty;
   nzc = t.nzc;
   if (ty < 2) ty = 2;
+  if (ty > step_max_ty()) ty = step_max_ty();
   if (ty > ny) ty = ny;
   if (nzc < 2) nzc = 2;
   if (nzc > nz) nzc = nz;
@@ -105,76 +105,6 @@ size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, in
   b += (size_t)ntx * 4 * 8 * 4 * 3;  // contributions + entries
   b += (size_t)((ny + ty - 1) / ty) * nz * 4 * 4;
   return b + (1 << 20);
-}
-
-static int encode_tmaps(adf_ctx* ctx, Solve& s, int xh) {
-  SolveDev& d = s.dev;
-  const int bx = d.nxp / xh;
-  cuuint64_t dims[5] = {(cuuint64_t)(xh == 1 ? d.nx : bx), (cuuint64_t)xh, (cuuint64_t)d.ny,
-                        (cuuint64_t)d.nz, 8};
-  cuuint64_t strides[4] = {(cuuint64_t)bx * 4, (cuuint64_t)d.nxp * 4,
-                           (cuuint64_t)d.nxp * d.ny * 4, (cuuint64_t)d.nxp * d.ny * d.nz * 4};
-  cuuint32_t box[5] = {(cuuint32_t)bx, (cuuint32_t)xh, (cuuint32_t)(d.ty + 2), 1, 1};
-  cuuint32_t es[5] = {1, 1, 1, 1, 1};
-  CUresult r = ctx->encode(&s.tm[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, d.field, dims, strides,
-                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(field) failed: " + std::to_string((int)r));
-  box[3] = 2;
-  r = ctx->encode(&s.tm[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, d.field, dims, strides, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(vz) failed: " + std::to_string((int)r));
-  for (int k = 2; k < kTmaps; ++k) std::memset(&s.tm[k], 0, sizeof(CUtensorMap));
-  if (d.npml > 0) {  // x-slab CPML memory, [buf][side][nz][ny][np]: box (np, ty+2, 1, 2)
-    for (int v = 0; v < 2; ++v) {
-      const int np = v ? d.nvp : d.npp;
-      cuuint64_t xd[4] = {(cuuint64_t)np, (cuuint64_t)d.ny, (cuuint64_t)d.nz, 4};
-      cuuint64_t xs[3] = {(cuuint64_t)np * 4, (cuuint64_t)np * d.ny * 4,
-                          (cuuint64_t)np * d.ny * d.nz * 4};
-      cuuint32_t xb[4] = {(cuuint32_t)np, (cuuint32_t)(d.ty + 2), 1, 2};
-      r = ctx->encode(&s.tm[3 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
-                      v ? (void*)d.psi_v[0] : (void*)d.psi_p[0], xd, xs, xb, es,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(x psi) failed: " + std::to_string((int)r));
-    }
-    // y slab [buf][side][nz][n][nxp] and z slab [buf][side][n][ny][nxp], n = npml (p) or
-    // npml+1 (v): 5-D like the field, box (bx, xh, ty+2, 1, 1)
-    for (int v = 0; v < 2; ++v) {
-      const int n = v ? d.npml + 1 : d.npml;
-      float* base_y = v ? d.psi_v[1] : d.psi_p[1];
-      float* base_z = v ? d.psi_v[2] : d.psi_p[2];
-      cuuint64_t yd[5] = {dims[0], dims[1], (cuuint64_t)n, (cuuint64_t)d.nz, 4};
-      cuuint64_t ys[4] = {strides[0], (cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * n * 4,
-                          (cuuint64_t)d.nxp * n * d.nz * 4};
-      cuuint64_t zd[5] = {dims[0], dims[1], (cuuint64_t)d.ny, (cuuint64_t)n, 4};
-      cuuint64_t zs[4] = {strides[0], (cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * d.ny * 4,
-                          (cuuint64_t)d.nxp * d.ny * n * 4};
-      cuuint32_t b5[5] = {(cuuint32_t)bx, (cuuint32_t)xh, (cuuint32_t)(d.ty + 2), 1, 1};
-      r = ctx->encode(&s.tm[5 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base_y, yd, ys, b5, es,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(y psi) failed: " + std::to_string((int)r));
-      r = ctx->encode(&s.tm[7 + v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base_z, zd, zs, b5, es,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(z psi) failed: " + std::to_string((int)r));
-    }
-  }
-  if (d.flags & SF_MASK) {
-    cuuint64_t md[3] = {(cuuint64_t)d.mw, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
-    cuuint64_t ms[2] = {(cuuint64_t)d.mw * 4, (cuuint64_t)d.mw * d.ny * 4};
-    cuuint32_t mb[3] = {(cuuint32_t)d.mw, (cuuint32_t)(d.ty + 2), 1};
-    r = ctx->encode(&s.tm[2], CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, (void*)s.mask_bits, md, ms, mb,
-                    es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled(mask) failed: " + std::to_string((int)r));
-  }
-  return ADF_OK;
 }
 
 // Entry lists for interp_trilinear! (derivatives.jl:30-60): every in-bounds
@@ -320,12 +250,6 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   d.ntx = ntx;
   d.flags = (has_mask ? SF_MASK : 0) | ((npml > 1 || (has_mask && npml >= 1)) ? SF_PCPML : 0) |
             (npml >= 1 ? SF_VCPML : 0) | (arith == ADF_ARITH_FP32 ? SF_FP32 : 0);
-  // tiles taller than 8 rows only fit the ring without the y/z-slab boxes
-  if (d.ty > 8) d.flags |= SF_YZG;
-  if (const char* env = std::getenv("ADF_YZG")) {  // sweep override
-    if (std::atoi(env) == 1) d.flags |= SF_YZG;
-    else if (d.ty <= 8) d.flags &= ~SF_YZG;
-  }
   d.fq = dom.fact_m0;
   d.fv = dom.fact_m1;
   d.rdx = 1.0 / dom.dx;
@@ -345,6 +269,7 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   if (has_mask) {
     s.mask_bits = dalloc<uint32_t>(s, (size_t)d.mw * d.ny * d.nz, rc);
     if (rc) return rc;
+    d.mask_bits = s.mask_bits;
   }
   const long long n = npml, nm = npml + 1, nxp = d.nxp, ny = d.ny, nz = d.nz;
   d.npp = (npml + 3) / 4 * 4;
@@ -407,14 +332,15 @@ int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const floa
                    const int* src_col) {
   int rc = build_entries(s, idx, w, src_col);
   if (rc) return rc;
-  rc = encode_tmaps(ctx, s, s.xh);
-  if (rc) return rc;
-  // work items: z chunks outer, y tiles inner (neighbouring tiles run
-  // together so halo rows hit L2)
+  // work items {solve, y tile | x tile << 16, z0, z1}: z chunks outer, then
+  // y tiles, x tiles inner, so that tiles sharing halo rows run together and
+  // the halo hits L2
   s.items.clear();
+  const int nxt = (s.dev.nxp + 127) / 128;
   for (int z0 = 0; z0 < s.dev.nz; z0 += s.nzc)
     for (int t = 0; t < s.dev.nty; ++t)
-      s.items.push_back(make_int4(0, t, z0, std::min(z0 + s.nzc, s.dev.nz)));
+      for (int x = 0; x < nxt; ++x)
+        s.items.push_back(make_int4(0, t | (x << 16), z0, std::min(z0 + s.nzc, s.dev.nz)));
   return ADF_OK;
 }
 
@@ -427,11 +353,9 @@ void Batch::release() {
   graph_exec = nullptr;
   graph_steps = 0;
   if (d_solves) cudaFree(d_solves);
-  if (d_tmaps) cudaFree(d_tmaps);
   if (d_items) cudaFree(d_items);
   if (d_err) cudaFree(d_err);
   d_solves = nullptr;
-  d_tmaps = nullptr;
   d_items = nullptr;
   d_err = nullptr;
   cap_solves = cap_items = 0;
@@ -441,9 +365,8 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   solves = list;
   const int ns = (int)list.size();
   std::vector<SolveDev> sd(ns);
-  std::vector<CUtensorMap> tm((size_t)kTmaps * ns);
   std::vector<int4> items;
-  int max_stage = 0, max_pn = 0;
+  max_ty = 1;
   max_ntx = 0;
   max_gf_nsrc = 0;
   max_gf_blocks = 0;
@@ -453,13 +376,8 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
       max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
       max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
     }
-    for (int k = 0; k < kTmaps; ++k) tm[(size_t)kTmaps * i + k] = list[i]->tm[k];
     const SolveDev& d = list[i]->dev;
-    const SlotLayout L = slot_layout(d.ty, d.nxp, (d.flags & SF_MASK) ? d.mw : 0,
-                                     (d.flags & SF_PCPML) ? d.npp : 0,
-                                     (d.flags & SF_VCPML) ? d.nvp : 0, !(d.flags & SF_YZG));
-    max_stage = std::max(max_stage, L.total);
-    max_pn = std::max(max_pn, pn_plane_floats(d.ty, d.nxp));
+    max_ty = std::max(max_ty, d.ty);
     max_ntx = std::max(max_ntx, d.ntx);
   }
   // interleave items of different solves so the batch stays balanced
@@ -485,7 +403,6 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
     cap_solves = std::max(ns, 1);
     cap_items = std::max(n_items, 1);
     if (cudaMalloc(&d_solves, sizeof(SolveDev) * cap_solves) != cudaSuccess ||
-        cudaMalloc(&d_tmaps, sizeof(CUtensorMap) * kTmaps * cap_solves) != cudaSuccess ||
         cudaMalloc(&d_items, sizeof(int4) * cap_items) != cudaSuccess ||
         cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
@@ -495,47 +412,12 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   host_solves = sd;
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_tmaps, tm.data(), sizeof(CUtensorMap) * kTmaps * ns, cudaMemcpyHostToDevice,
-                  st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_err, 0, sizeof(int), st);
   cudaStreamSynchronize(st);
-  stage_floats = max_stage;
-  pn_floats = max_pn;
   per_step = max_gf_nsrc > 0 ? 5 : 2;
-  // pipeline depth: as many slots as fit two CTAs per SM, else one CTA.
-  // The kernel's static shared memory counts against the same budget.
-  cudaFuncAttributes fa{};
-  cudaFuncGetAttributes(&fa, step_kernel_ptr(false));
-  const size_t fixed = 256 + (size_t)3 * pn_floats * 4 + fa.sharedSizeBytes;
-  const size_t per_cta2 = (size_t)ctx->smem_per_sm / 2 - 1024;
-  int stages = (int)((per_cta2 > fixed ? per_cta2 - fixed : 0) / ((size_t)stage_floats * 4));
-  two_per_sm = stages >= 2;
-  if (stages < 2) {
-    const size_t per_cta1 = std::min((size_t)ctx->smem_optin, (size_t)ctx->smem_per_sm - 1024);
-    stages = (int)((per_cta1 - fixed) / ((size_t)stage_floats * 4));
-  }
-  stages = std::min(std::max(stages, 2), 8);
-  if (const char* env = std::getenv("ADF_STAGES")) {  // sweep override
-    const int v = std::atoi(env);
-    if (v >= 2 && v <= 8) {
-      stages = v;
-      two_per_sm = fixed + (size_t)v * stage_floats * 4 <= per_cta2;
-    }
-  }
-  this->stages = stages;
-  smem = fixed - fa.sharedSizeBytes + (size_t)stages * stage_floats * 4;  // dynamic part
-  if (smem + fa.sharedSizeBytes > (size_t)ctx->smem_optin)
-    return fail(ADF_E_ARG, "grid too wide for shared memory");
-  if (cudaError_t ea = step_kernel_attributes(smem, two_per_sm); ea != cudaSuccess)
-    return fail(ADF_E_DEVICE, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(ea));
-  int bps = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, step_kernel_ptr(two_per_sm),
-                                                consumer_threads() + 32,
-                                                smem);
-  if (bps < 1) bps = 1;
-  grid = std::min(n_items, ctx->nsm * bps);
-  if (grid < 1) grid = 1;
+  if (max_ty > step_max_ty()) return fail(ADF_E_ARG, "tile taller than the step kernel's rows");
+  grid = n_items;
   if (graph_exec) {
     cudaGraphExecDestroy(graph_exec);
     graph_exec = nullptr;
@@ -547,13 +429,9 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
 int Batch::launch_step(adf_ctx* ctx, int step) {
   StepParams p;
   p.solves = d_solves;
-  p.tmaps = d_tmaps;
   p.items = d_items;
   p.n_items = n_items;
   p.step = step;
-  p.stages = stages;
-  p.stage_floats = stage_floats;
-  p.pn_floats = pn_floats;
   p.err = d_err;
   const bool timed = ctx->kernel_timing && 2 * step + 1 < (int)ctx->kev.size();
   // inside stream capture an event record must be an external node to be
@@ -564,12 +442,10 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
       cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (timed && cudaEventRecordWithFlags(ctx->kev[2 * step], ctx->stream, evf) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("event record: ") + cudaGetErrorString(cudaGetLastError()));
-  cudaError_t e =
-      adf::launch_step(p, grid, consumer_threads() + 32, smem, ctx->stream, two_per_sm);
+  cudaError_t e = adf::launch_step(p, grid, max_ty, ctx->stream);
   if (e != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("step launch failed: ") + cudaGetErrorString(e) +
-                                  " (grid " + std::to_string(grid) + ", smem " +
-                                  std::to_string(smem) + ")");
+                                  " (grid " + std::to_string(grid) + ")");
   if (timed && cudaEventRecordWithFlags(ctx->kev[2 * step + 1], ctx->stream, evf) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("event record: ") + cudaGetErrorString(cudaGetLastError()));
   EpiParams ep;
@@ -839,16 +715,6 @@ int adf_ctx_create(int device, size_t hbm_budget, adf_ctx** out) {
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   c->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
-  cudaDriverEntryPointQueryResult q;
-  void* fn = nullptr;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-          cudaSuccess ||
-      !fn) {
-    cudaStreamDestroy(c->stream);
-    delete c;
-    return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled unavailable");
-  }
-  c->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   *out = c;
   return ADF_OK;
 }

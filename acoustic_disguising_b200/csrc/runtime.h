@@ -21,7 +21,6 @@ struct adf_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   size_t budget = 0;
-  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   struct adf::Solve* cur = nullptr;  // solve whose field adf_read_field reads
   int64_t cur_it = 0;
   double last_ms = 0.0;
@@ -64,7 +63,6 @@ struct Solve {
   SolveDev dev;
   std::vector<void*> allocs;
   size_t bytes = 0;
-  CUtensorMap tm[kTmaps];
   int nzc = 32;
   int xh = 1;
   uint32_t* mask_bits = nullptr;
@@ -75,7 +73,7 @@ struct Solve {
   long long n_entries = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation when set
-  std::vector<int4> items;  // {0, y tile, z0, z1}
+  std::vector<int4> items;  // {0, y tile | x tile << 16, z0, z1}
   ~Solve();
   void release();
 };
@@ -84,16 +82,14 @@ struct Batch {
   std::vector<Solve*> solves;
   std::vector<SolveDev> host_solves;
   SolveDev* d_solves = nullptr;
-  CUtensorMap* d_tmaps = nullptr;
   int4* d_items = nullptr;
   int* d_err = nullptr;
   int cap_solves = 0, cap_items = 0;
-  int n_items = 0, stages = 3, stage_floats = 0, pn_floats = 0, grid = 1, max_ntx = 0;
-  bool two_per_sm = false;  // ring sized so two CTAs share an SM
+  int n_items = 0, grid = 1, max_ntx = 0;
+  int max_ty = 1;            // tallest tile in the batch: the block is (32, max_ty + 1)
   int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
   int max_gf_blocks = 0;     // (source, receiver split) blocks of the GF kernel
   int per_step = 2;          // kernel launches per launch-step
-  size_t smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;
   ~Batch();
@@ -127,6 +123,5 @@ int pack_transceivers_host(const hm::Dom& d, const double* points, const double*
 
 // kernels (fdtd_kernels.cu)
 cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s);
-const void* step_kernel_ptr(bool two_per_sm);
 
 }  // namespace adf
