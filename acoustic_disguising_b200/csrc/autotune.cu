@@ -65,11 +65,11 @@ extern "C" int adf_autotune(adf_ctx* ctx, int64_t nx, int64_t ny, int64_t nz, in
     r.out_vn = out_vn.data() + (size_t)k * steps * nrec;
   }
   std::vector<std::pair<int, int>> cand;
-  const int tys[] = {2, 3, 4, 6, 8};
+  const int tys[] = {3, 5, 7};
   const int nzcs[] = {8, 16, 32};
   for (int ty : tys)
     for (int nzc : nzcs)
-      if (ty <= ny && nzc <= nz && (nx <= 256 || ty <= 3)) cand.push_back({ty, nzc});
+      if (ty <= ny && nzc <= nz) cand.push_back({ty, nzc});
   const bool timing_was = ctx->kernel_timing;
   adf_set_kernel_timing(ctx, 1);
   double best = 1e300;

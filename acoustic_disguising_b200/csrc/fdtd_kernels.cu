@@ -423,14 +423,14 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 
 // ---------------------------------------------------------------------------
 // The step kernel.  One CTA per work item {solve, y tile | x tile << 16, z0,
-// z1}: a tile of ty <= 8 rows j0..j0+ty-1 and the 128 cells xb..xb+127 of
-// one solve, and the planes z0..z1-1.  blockDim = (32, 9).  Warps 0-7 each
-// hold 8 quads x 4 rows of the tile (warp w: quads 8(w%4)..+7, rows
-// 1+4(w/4)..+3 in tile-row numbering, row r = j - j0 + 1); warp 8 holds the
-// halo row r = 0 (j0-1), whose new P the Vy update of row j0 needs: it is
-// recomputed, not exchanged.  The lanes of quad 0 also recompute the halo
-// column x = xb-1 (for Vx at xb).  With this shape the x-slab quads of a
-// tile sit in one warp column, so only those warps take the CPML branch.
+// z1}: a tile of ty <= 7 rows j0..j0+ty-1 and the 128 cells xb..xb+127 of
+// one solve, and the planes z0..z1-1.  blockDim = (32, 8): warp w holds the
+// 4 quads 4w..4w+3 (16 cells) of all 8 tile rows r = j - j0 + 1 = 0..7 (lane
+// = 4r + quad).  Row r = 0 is the halo row j0-1, whose new P the Vy update
+// of row j0 needs: it is recomputed, not exchanged.  The lanes of quad 0
+// also recompute the halo column x = xb-1 (for Vx at xb).  With this shape
+// the x-slab quads of a grid sit in one warp per x-edge tile, so only those
+// warps take the CPML branch.
 // Per plane, after a prologue plane z0-1 (new P only, for Vz at z0) when
 // z0 > 0:
 //   loads  : P, Vx, Vy of plane k and Vz of plane k+1 (Vz of plane k and the
@@ -447,10 +447,10 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 // ones.  Several CTAs per SM keep enough independent warps in flight to
 // cover the latency of the float/double chains and of HBM.
 // ---------------------------------------------------------------------------
-constexpr int kMaxTy = 8;           // rows per tile
+constexpr int kMaxTy = 7;           // rows per tile (plus the halo row: 8 per warp)
 constexpr int kXT = 128;            // cells per x tile
 constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..131] = cells
-constexpr int kStepThreads = 32 * (kMaxTy + 1);
+constexpr int kStepThreads = 256;  // 8 warps of 4 quads x 8 rows
 
 template <typename R>
 __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
@@ -460,23 +460,9 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxp = S.nxp, ty = S.ty, npml = S.npml;
   const int T = item.y & 0xFFFF, X = item.y >> 16;
   const int j0 = T * ty, xb = X * kXT;
-  int r, qx, wr0, wnr, wq0, wnq;  // this thread's row and quad; its warp's rows and quads
-  if (wid < 8) {
-    const int wx = wid & 3, wy = wid >> 2;
-    qx = 8 * wx + (lane & 7);
-    r = 1 + 4 * wy + (lane >> 3);
-    wq0 = 8 * wx;
-    wnq = 8;
-    wr0 = 1 + 4 * wy;
-    wnr = 4;
-  } else {
-    qx = lane;
-    r = 0;
-    wq0 = 0;
-    wnq = 32;
-    wr0 = 0;
-    wnr = 1;
-  }
+  // this thread's tile row r (0 = halo row) and quad qx; its warp's quads
+  const int qx = 4 * wid + (lane & 3), r = lane >> 2;
+  const int wq0 = 4 * wid, wnq = 4, wr0 = 0, wnr = kMaxTy + 1;
   const int j = j0 - 1 + r, x0 = xb + 4 * qx;
   const bool row_ok = r <= ty && j >= 0 && j < ny;
   const bool act = row_ok && x0 < nxp;  // this thread updates a quad
@@ -508,17 +494,15 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   // (and, rows >= 1, V) updates?  The plane is checked per plane below.
   bool wplain_rx;
   {
-    const int wj0 = j0 - 1 + wr0, wj1 = wj0 + wnr - 1;
+    const int wj0 = j0 - 1 + wr0, wj1 = wj0 + wnr - 1;  // rows: P on all, V from wj0 + 1
     const int wx0 = xb + 4 * wq0, wx1 = wx0 + 4 * wnq - 1;
     const int p_xmin = pcp ? npml : 0, p_xmax = pcp ? min(nx - 2, nx - npml - 1) : nx - 2;
     const int v_xmin = vcp ? npml + 1 : 1, v_xmax = vcp ? nx - npml - 2 : nx - 1;
     bool ok = wr0 + wnr - 1 <= ty && wj0 >= 0 && wx1 < nxp;
     ok = ok && wj1 < ny - 1 && (!pcp || (wj0 >= npml && wj1 < ny - npml));
     ok = ok && wx0 >= p_xmin && wx1 <= p_xmax;
-    if (wr0 >= 1) {
-      ok = ok && wj0 >= 1 && (!vcp || (wj0 > npml && wj1 < ny - npml - 1));
-      ok = ok && wx0 >= v_xmin && wx1 <= v_xmax;
-    }
+    ok = ok && wj0 + 1 >= 1 && (!vcp || (wj0 + 1 > npml && wj1 < ny - npml - 1));
+    ok = ok && wx0 >= v_xmin && wx1 <= v_xmax;
     wplain_rx = ok;
   }
   const long long rowoff = (long long)(row_ok ? j : 0) * nxp + x0;
@@ -535,7 +519,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
     const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
     const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
-    const bool wplain = wplain_rx && pplane && (wr0 == 0 || prologue || vplane);
+    const bool wplain = wplain_rx && pplane && (prologue || vplane);
     float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), X4 = Pn, Y0 = Pn, Z1 = Pn;
     uint32_t nib = 0xFFFFu;
     if (act) {
@@ -622,7 +606,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   }
 }
 
-__global__ void __launch_bounds__(kStepThreads, 3) adf_fdtd_step_kernel(const StepParams p) {
+__global__ void __launch_bounds__(kStepThreads, 4) adf_fdtd_step_kernel(const StepParams p) {
   __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
   __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
   __shared__ float s_co[kMaxCoef];
@@ -823,7 +807,7 @@ cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s) {
 
 cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s) {
   (void)max_ty;  // the block always holds kMaxTy rows; shorter tiles idle the rest
-  adf_fdtd_step_kernel<<<grid, dim3(32, kMaxTy + 1), 0, s>>>(p);
+  adf_fdtd_step_kernel<<<grid, dim3(32, 8), 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -52,11 +52,10 @@ static void load_locked() {
 
 static Tune default_tune(int nx, int ny, int nz) {
   Tune t;
-  // Large grids: 8-row tiles (one CTA per SM, more work per thread and less
-  // halo recomputation) still give every SM several items per solve.  Small
-  // grids keep 3-row tiles so that a single solve fills the GPU.  Rows wider
-  // than 256 cells take two x boxes and 3-row tiles (autotuned at 512^3).
-  t.ty = nx > 256 ? 3 : ((ny >= 224 && nz >= 224) ? 8 : 3);
+  // 7-row tiles fill every lane of the step kernel's 8-row warps (tile rows
+  // plus the recomputed halo row) and recompute the fewest halo rows.
+  t.ty = 7;
+  (void)nx;
   t.nzc = 16;
   (void)ny;
   return t;

@@ -148,6 +148,6 @@ def test_autotune_stores_a_shape_that_later_solves_use(adf, ctx, tmp_path, monke
     monkeypatch.setenv("ADF_TUNE_TABLE", str(table))
     monkeypatch.delenv("ADF_TILE", raising=False)
     ty, nzc, ms = adf.autotune(72, 64, 60, npml=6, n_solves=2, steps=12, ctx=ctx)
-    assert ty in (2, 3, 4, 6, 8) and nzc in (8, 16, 32) and ms > 0
+    assert ty in (3, 5, 7) and nzc in (8, 16, 32) and ms > 0
     txt = table.read_text()
     assert f'"72,64,60": [{ty}, {nzc}]' in txt
