@@ -5,8 +5,8 @@ steps per solve), batched through the C-ABI on B200.
 
 One bench step = one call of adf_gf_solve_batch over `--batch` complete
 solves (B sources of the 512-point Fibonacci source sphere): set-up, 2000
-time steps for all B solves advanced together (one persistent launch per
-time step, graph-captured), and the p / v_n traces copied back.
+time steps for all B solves advanced together (one step-kernel launch per
+time step over all of their tiles, graph-captured), and the p / v_n traces copied back.
 
   value : GF solves/s from device time (CUDA events on the library's
           stream around the stepping of each batch; inputs resident)
