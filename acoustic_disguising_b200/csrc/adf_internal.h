@@ -99,6 +99,7 @@ enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_
 // one CTA per work item, blockDim (32, max_ty + 1); max_ty <= step_max_ty()
 cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s);
 int step_max_ty();
+int step_x_tile();  // cells per x tile of a step work item
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
                                   cudaStream_t s);

@@ -8,13 +8,14 @@
 // HBM: 16 B read + 16 B written per cell, plus the CPML memory on the slabs
 // and half a byte of mask per cell.
 //
-// Work decomposition (2.5D): a CTA owns a tile of ty rows x 128 cells of one
-// solve and a run of planes; its warps are the tile's rows, its lanes 4-cell
-// quads, and it walks the planes in z keeping the z-neighbours in registers.
-// The new P of a plane goes through shared memory for the x-1 / y-1
-// neighbours of the velocity update; the halo row and column are
-// recomputed, not exchanged.  Grids of many such CTAs (two or more per SM)
-// keep HBM busy: the update is a short, memory-bound stencil.
+// Work decomposition (2.5D): a CTA owns a tile of 7 rows x 64 cells of one
+// solve and a run of planes; each warp holds 16 cells of all the tile's rows
+// (plus the halo row), its lanes 4-cell quads, and the CTA walks the planes
+// in z keeping the z-neighbours in registers.  The new P of a plane goes
+// through shared memory for the x-1 / y-1 neighbours of the velocity update;
+// the halo row and column are recomputed, not exchanged.  Grids of many
+// such CTAs (eight per SM) keep HBM busy: the update is a short,
+// memory-bound stencil.
 //
 // Arithmetic: Arith<double> reproduces Julia's promotion (Float32 storage,
 // Float64 Domain scalars, src/kernels/updates.jl) with explicit round-to-
@@ -423,14 +424,15 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 
 // ---------------------------------------------------------------------------
 // The step kernel.  One CTA per work item {solve, y tile | x tile << 16, z0,
-// z1}: a tile of ty <= 7 rows j0..j0+ty-1 and the 128 cells xb..xb+127 of
-// one solve, and the planes z0..z1-1.  blockDim = (32, 8): warp w holds the
-// 4 quads 4w..4w+3 (16 cells) of all 8 tile rows r = j - j0 + 1 = 0..7 (lane
-// = 4r + quad).  Row r = 0 is the halo row j0-1, whose new P the Vy update
-// of row j0 needs: it is recomputed, not exchanged.  The lanes of quad 0
-// also recompute the halo column x = xb-1 (for Vx at xb).  With this shape
-// the x-slab quads of a grid sit in one warp per x-edge tile, so only those
-// warps take the CPML branch.
+// z1}: a tile of ty <= 7 rows j0..j0+ty-1 and the kXT = 64 cells
+// xb..xb+63 of one solve, and the planes z0..z1-1.  blockDim = (32, 4): warp
+// w holds the 4 quads 4w..4w+3 (16 cells) of all 8 tile rows
+// r = j - j0 + 1 = 0..7 (lane = 4r + quad).  Row r = 0 is the halo row
+// j0-1, whose new P the Vy update of row j0 needs: it is recomputed, not
+// exchanged.  The lanes of quad 0 also recompute the halo column x = xb-1
+// (for Vx at xb).  With this shape the x-slab quads of a grid sit in one
+// warp of each x-edge tile and the tiles between hold none, so few warps
+// take the CPML branch and few CTAs wait for such a warp at their barrier.
 // Per plane, after a prologue plane z0-1 (new P only, for Vz at z0) when
 // z0 > 0:
 //   loads  : P, Vx, Vy of plane k and Vz of plane k+1 (Vz of plane k and the
@@ -448,9 +450,9 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 // cover the latency of the float/double chains and of HBM.
 // ---------------------------------------------------------------------------
 constexpr int kMaxTy = 7;           // rows per tile (plus the halo row: 8 per warp)
-constexpr int kXT = 128;            // cells per x tile
-constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..131] = cells
-constexpr int kStepThreads = 256;  // 8 warps of 4 quads x 8 rows
+constexpr int kXT = 64;             // cells per x tile (4 warps)
+constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..] = cells
+constexpr int kStepThreads = 32 * kXT / 16;  // warps of 4 quads x 8 rows
 
 template <typename R>
 __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
@@ -606,7 +608,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   }
 }
 
-__global__ void __launch_bounds__(kStepThreads, 4) adf_fdtd_step_kernel(const StepParams p) {
+__global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) adf_fdtd_step_kernel(const StepParams p) {
   __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
   __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
   __shared__ float s_co[kMaxCoef];
@@ -807,11 +809,12 @@ cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s) {
 
 cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s) {
   (void)max_ty;  // the block always holds kMaxTy rows; shorter tiles idle the rest
-  adf_fdtd_step_kernel<<<grid, dim3(32, 8), 0, s>>>(p);
+  adf_fdtd_step_kernel<<<grid, dim3(32, kXT / 16), 0, s>>>(p);
   return cudaGetLastError();
 }
 
 int step_max_ty() { return kMaxTy; }
+int step_x_tile() { return kXT; }
 
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
                                   cudaStream_t s) {

@@ -336,7 +336,7 @@ int solve_finalize(adf_ctx* ctx, Solve& s, const float* const idx[4], const floa
   // y tiles, x tiles inner, so that tiles sharing halo rows run together and
   // the halo hits L2
   s.items.clear();
-  const int nxt = (s.dev.nxp + 127) / 128;
+  const int xt = step_x_tile(), nxt = (s.dev.nxp + xt - 1) / xt;
   for (int z0 = 0; z0 < s.dev.nz; z0 += s.nzc)
     for (int t = 0; t < s.dev.nty; ++t)
       for (int x = 0; x < nxt; ++x)
