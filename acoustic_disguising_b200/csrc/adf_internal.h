@@ -82,7 +82,6 @@ struct StepParams {
   const int4* items;
   int n_items;
   int step;  // launch-step index within the chunk
-  int* err;  // launch-wide error word
 };
 
 struct EpiParams {
@@ -92,8 +91,6 @@ struct EpiParams {
   int phase;  // 0: records, v2vn and vn2v; solves with SF_GF: 1 records + v2vn, 2 vn2v
 };
 
-// error codes written by kernels
-enum : int { KERR_NONE = 0, KERR_FULL_TIMEOUT = 1, KERR_EMPTY_TIMEOUT = 2, KERR_DRAIN_TIMEOUT = 3 };
 
 // launch helpers implemented in fdtd_kernels.cu
 // one CTA per work item, blockDim (32, max_ty + 1); max_ty <= step_max_ty()

@@ -537,7 +537,8 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   ctx->h2d_bytes = (int64_t)48 * ns + (kind ? 48 : 24) * (int64_t)nr +
                    (int64_t)(kind ? 12 : 8) * nt * ns;
   ctx->d2h_bytes = (int64_t)4 * nt * nr;
-  if (herr) return fail(ADF_E_STATE, "adf_kh_pressure: a pair's delay fell outside its tile bound");
+  if (herr & 2) return fail(ADF_E_TIMEOUT, "KH: a bounded wait for a staged chunk gave up");
+  if (herr) return fail(ADF_E_STATE, "KH: a pair's delay fell outside its tile bound");
   return ADF_OK;
 }
 

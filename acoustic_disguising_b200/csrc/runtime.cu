@@ -78,8 +78,7 @@ static T* dalloc(Solve& s, size_t n, int& rc) {
   return static_cast<T*>(p);
 }
 
-void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, int& mw) {
-  xh = 1;
+void choose_tiles(int nx, int ny, int nz, int& nxp, int& ty, int& nzc, int& mw) {
   nxp = (nx + 3) / 4 * 4;
   mw = ((nx + 7) / 8 + 3) / 4 * 4;
   const Tune t = tune_lookup(nx, ny, nz);
@@ -94,8 +93,8 @@ void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, 
 
 size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, int64_t ntx,
                             int64_t nt, bool mask) {
-  int nxp, xh, ty, nzc, mw;
-  choose_tiles((int)nx, (int)ny, (int)nz, nxp, xh, ty, nzc, mw);
+  int nxp, ty, nzc, mw;
+  choose_tiles((int)nx, (int)ny, (int)nz, nxp, ty, nzc, mw);
   size_t b = 2ull * 4 * nz * ny * nxp * 4;
   if (mask) b += (size_t)mw * ny * nz * 4;
   size_t n = npml;
@@ -238,9 +237,7 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   SolveDev& d = s.dev;
   std::memset(&d, 0, sizeof(d));
   s.stream = ctx->stream;
-  int xh;
-  choose_tiles((int)dom.nx, (int)dom.ny, (int)dom.nz, d.nxp, xh, d.ty, s.nzc, d.mw);
-  s.xh = xh;
+  choose_tiles((int)dom.nx, (int)dom.ny, (int)dom.nz, d.nxp, d.ty, s.nzc, d.mw);
   d.nx = (int)dom.nx;
   d.ny = (int)dom.ny;
   d.nz = (int)dom.nz;
@@ -354,10 +351,8 @@ void Batch::release() {
   graph_steps = 0;
   if (d_solves) cudaFree(d_solves);
   if (d_items) cudaFree(d_items);
-  if (d_err) cudaFree(d_err);
   d_solves = nullptr;
   d_items = nullptr;
-  d_err = nullptr;
   cap_solves = cap_items = 0;
 }
 
@@ -403,8 +398,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
     cap_solves = std::max(ns, 1);
     cap_items = std::max(n_items, 1);
     if (cudaMalloc(&d_solves, sizeof(SolveDev) * cap_solves) != cudaSuccess ||
-        cudaMalloc(&d_items, sizeof(int4) * cap_items) != cudaSuccess ||
-        cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&d_items, sizeof(int4) * cap_items) != cudaSuccess) {
       cudaGetLastError();
       return fail(ADF_E_NOMEM, "batch descriptor allocation failed");
     }
@@ -413,7 +407,6 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(d_err, 0, sizeof(int), st);
   cudaStreamSynchronize(st);
   per_step = max_gf_nsrc > 0 ? 5 : 2;
   if (max_ty > step_max_ty()) return fail(ADF_E_ARG, "tile taller than the step kernel's rows");
@@ -432,7 +425,6 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   p.items = d_items;
   p.n_items = n_items;
   p.step = step;
-  p.err = d_err;
   const bool timed = ctx->kernel_timing && 2 * step + 1 < (int)ctx->kev.size();
   // inside stream capture an event record must be an external node to be
   // a timing point on every replay
@@ -564,12 +556,11 @@ void Batch::collect_kernel_times(adf_ctx* ctx, int n) {
   }
 }
 
+// Waits for the batch's work and reports any device error it raised.
 int Batch::check_error(adf_ctx* ctx) {
-  int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
-  if (h) return fail(ADF_E_TIMEOUT, "a bounded device-side wait gave up (code " + std::to_string(h) + ")");
   return ADF_OK;
 }
 

@@ -64,7 +64,6 @@ struct Solve {
   std::vector<void*> allocs;
   size_t bytes = 0;
   int nzc = 32;
-  int xh = 1;
   uint32_t* mask_bits = nullptr;
   float* coef_dev = nullptr;
   float* dir_dev = nullptr;
@@ -83,7 +82,6 @@ struct Batch {
   std::vector<SolveDev> host_solves;
   SolveDev* d_solves = nullptr;
   int4* d_items = nullptr;
-  int* d_err = nullptr;
   int cap_solves = 0, cap_items = 0;
   int n_items = 0, grid = 1, max_ntx = 0;
   int max_ty = 1;            // tallest tile in the batch: the block is (32, max_ty + 1)
@@ -104,7 +102,7 @@ struct Batch {
   int check_error(adf_ctx* ctx);
 };
 
-void choose_tiles(int nx, int ny, int nz, int& nxp, int& xh, int& ty, int& nzc, int& mw);
+void choose_tiles(int nx, int ny, int nz, int& nxp, int& ty, int& nzc, int& mw);
 size_t solve_bytes_estimate(int64_t nx, int64_t ny, int64_t nz, int64_t npml, int64_t ntx,
                             int64_t nt, bool mask);
 int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,

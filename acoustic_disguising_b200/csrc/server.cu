@@ -66,8 +66,8 @@ struct GfJob {
 };
 
 static size_t gf_bytes(const adf_gf_request& r) {
-  int nxp, xh, ty, nzc, mw;
-  choose_tiles((int)r.dom.nx, (int)r.dom.ny, (int)r.dom.nz, nxp, xh, ty, nzc, mw);
+  int nxp, ty, nzc, mw;
+  choose_tiles((int)r.dom.nx, (int)r.dom.ny, (int)r.dom.nz, nxp, ty, nzc, mw);
   const size_t nx = r.dom.nx, ny = r.dom.ny, nz = r.dom.nz, n = r.npml, nt = r.dom.nt;
   const size_t ntx = 1 + r.n_rec;
   size_t b = 2ull * 4 * nz * ny * nxp * 4;
