@@ -66,8 +66,9 @@ template <typename T>
 static T* dalloc(Solve& s, size_t n, int& rc) {
   void* p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = s.alloc_stream ? cudaMallocAsync(&p, n * sizeof(T), s.alloc_stream)
-                                 : cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = s.alloc_stream
+                      ? cudaMallocFromPoolAsync(&p, n * sizeof(T), s.alloc_pool, s.alloc_stream)
+                      : cudaMalloc(&p, n * sizeof(T));
   if (e != cudaSuccess) {
     cudaGetLastError();
     rc = fail(ADF_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
@@ -706,6 +707,24 @@ int adf_ctx_create(int device, size_t hbm_budget, adf_ctx** out) {
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   c->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+  {  // the context's own pool (device memory, no release back to the driver
+     // while the context lives); admission keeps its size within the budget
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+      cudaGetLastError();
+      if (c->pool) cudaMemPoolDestroy(c->pool);
+      cudaEventDestroy(c->ev0);
+      cudaEventDestroy(c->ev1);
+      cudaStreamDestroy(c->stream);
+      delete c;
+      return fail(ADF_E_DEVICE, "memory pool creation failed");
+    }
+  }
   *out = c;
   return ADF_OK;
 }
@@ -718,6 +737,7 @@ int adf_ctx_destroy(adf_ctx* c) {
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaStreamDestroy(c->stream);
+  if (c->pool) cudaMemPoolDestroy(c->pool);
   delete c;
   return ADF_OK;
 }

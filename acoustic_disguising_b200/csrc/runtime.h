@@ -20,6 +20,10 @@ struct adf_ctx {
   int smem_optin = 232448;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // stream-ordered pool of the GF engine's solve memory; it keeps freed
+  // blocks mapped, so a solve admitted after another one retires reuses its
+  // memory instead of mapping fresh gigabytes
+  cudaMemPool_t pool = nullptr;
   size_t budget = 0;
   struct adf::Solve* cur = nullptr;  // solve whose field adf_read_field reads
   int64_t cur_it = 0;
@@ -71,7 +75,8 @@ struct Solve {
   int64_t h2d = 0;         // bytes uploaded while setting this solve up
   long long n_entries = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation when set
+  cudaStream_t alloc_stream = nullptr;  // stream-ordered allocation from alloc_pool when set
+  cudaMemPool_t alloc_pool = nullptr;
   std::vector<int4> items;  // {0, y tile | x tile << 16, z0, z1}
   ~Solve();
   void release();

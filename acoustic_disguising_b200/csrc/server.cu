@@ -92,6 +92,7 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
     return fail(ADF_E_ARG, "bad GF request");
   auto s = std::make_unique<Solve>();
   s->alloc_stream = ctx->stream;
+  s->alloc_pool = ctx->pool;
   const hm::Dom dom = to_dom(dd);
   const bool has_mask = r.shape != ADF_SHAPE_NONE;
   const int ntx = 1 + (int)r.n_rec;
@@ -161,7 +162,7 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
       double* o = c.data() + (a == 0 ? 0 : a == 1 ? dd.nx : dd.nx + dd.ny);
       for (int64_t i = 1; i <= rr.len; ++i) o[i - 1] = rr.at(i);
     }
-    if (cudaMallocAsync((void**)&xyz, c.size() * 8, st) != cudaSuccess)
+    if (cudaMallocFromPoolAsync((void**)&xyz, c.size() * 8, ctx->pool, st) != cudaSuccess)
       return fail(ADF_E_NOMEM, "alloc");
     cudaMemcpyAsync(xyz, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st);
     s->h2d += (int64_t)(c.size() * 8);
