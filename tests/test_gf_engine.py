@@ -73,6 +73,21 @@ def test_gf_batched_matches_oracle_and_plain(adf, oracle, ctx):
         assert rel(r.vn, vo) < 1e-6
 
 
+def test_gf_batches_reuse_memory_without_carry_over(adf, ctx):
+    """Solve memory is recycled between batches by the context's pool: a
+    batch, a larger one (longer traces, bigger grid), then the first batch
+    again gives the first batch's results bit for bit."""
+    small = [(36, 40, "sphere", 0), (40, 30, "none", 1)]
+    first = [make_req(adf, *s) for s in small]
+    adf.gf_solve_batch(first, batched=True)
+    big = [make_req(adf, 48, 90, "cube", 2), make_req(adf, 44, 70, "ellipsoid", 3)]
+    adf.gf_solve_batch(big, batched=True)
+    again = [make_req(adf, *s) for s in small]
+    adf.gf_solve_batch(again, batched=True)
+    for a, b in zip(first, again):
+        assert np.array_equal(a.p, b.p) and np.array_equal(a.vn, b.vn)
+
+
 def test_gf_budget_admission(adf, ctx):
     """A budget that fits about two solves forces waves of admission; results
     equal the unconstrained batch."""
