@@ -30,9 +30,10 @@
 //           monopole and dipole channel in one instruction) from a window
 //           of T+LM-1 samples per channel.  Lanes start T samples apart, an
 //           odd stride, so the 32 lanes of a window load hit 32 banks.
-//   The per-pair partial sums are added to the output accumulators with a
-//   compensated (Kahan) FP32 sum, so the sum over thousands of surface
-//   points keeps FP32 round-off at the level of a single addition.
+//   The partial sums of KH_G consecutive surface points are added to the
+//   output accumulators with a compensated (Kahan) FP32 sum, so the sum over
+//   thousands of surface points keeps FP32 round-off at the level of a
+//   few additions.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -53,11 +54,15 @@ namespace {
 #ifndef KH_NRW
 #define KH_NRW 1
 #endif
+#ifndef KH_NG
+#define KH_NG 8
+#endif
 constexpr int KH_T = KH_NT;              // output samples per lane (odd)
 constexpr int KH_WARPS = KH_NWARPS;
 constexpr int KH_THREADS = 32 * KH_WARPS;
 constexpr int KH_TB = 32 * KH_T;         // output samples per CTA
 constexpr int KH_RW = KH_NRW;            // targets per warp
+constexpr int KH_G = KH_NG;              // surface points summed before each compensated add
 constexpr int KH_RT = KH_WARPS * KH_RW;  // targets per CTA
 constexpr int KH_SC_MAX = 32;            // surface points per staged chunk
 static_assert(KH_T % 2 == 1, "lanes must start an odd number of samples apart");
@@ -81,8 +86,8 @@ struct KhParams {
   const double* rp;  // (nr,3)
   const double* rn;  // (nr,3) target normals (velocity output)
   const int2* tile_lo;  // per target tile: {lo_min, lo_max}
-  const float* in_q;    // (pitch, ns): zero-padded columns, sample t at pad + t
-  const float* in_f;
+  const float* in_qf;   // (2 pitch, ns): zero-padded columns of {in_q, in_f} pairs,
+                        // the pair of sample t at 2 (pad + t)
   const float* cs_f;    // running sum of in_f, same layout (velocity output)
   float* out;           // (nt, nr)
   int* err;
@@ -109,14 +114,14 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
   const int g0 = tb - lo_max - (LM - 1);
   const int col0 = p.pad + g0;
   const int shift = col0 & 3;
-  const float* colq = p.in_q + (col0 - shift);
-  const float* colf = p.in_f + (col0 - shift);
+  const float* colqf = p.in_qf + 2 * (col0 - shift);
   const float* colc = KIND ? p.cs_f + (col0 - shift) : nullptr;
   const int npair = KH_RT * p.sc;
   constexpr int NROW = KIND ? 3 : 2;  // staged rows per surface point
   constexpr int NPAR = 8;             // lo, n, wb, 5 coefficients
 
-  // shared memory: 2 window buffers [sc][NROW][rowpad], 2 pair-parameter
+  // shared memory: 2 window buffers [sc][NROW][rowpad] (per surface point a
+  // row of rowpad {q, f} pairs, then for KIND 1 the running-sum row), 2 pair-parameter
   // buffers [NPAR][RT*sc], per-warp taps [warps][RW][LM][2]
   const int wbuf = p.sc * NROW * p.rowpad;
   float* const par0 = smem + 2 * wbuf;
@@ -143,8 +148,7 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     float* w = smem + (c & 1) * wbuf;
     for (int sl = 0; sl < nsc; ++sl) {
       const size_t off = (size_t)(s0 + sl) * p.pitch;
-      bulk_load(smem_u32(w + (size_t)(NROW * sl) * p.rowpad), colq + off, row_bytes, mb);
-      bulk_load(smem_u32(w + (size_t)(NROW * sl + 1) * p.rowpad), colf + off, row_bytes, mb);
+      bulk_load(smem_u32(w + (size_t)(NROW * sl) * p.rowpad), colqf + 2 * off, 2 * row_bytes, mb);
       if (KIND)
         bulk_load(smem_u32(w + (size_t)(NROW * sl + 2) * p.rowpad), colc + off, row_bytes, mb);
     }
@@ -238,15 +242,23 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
       ok = false;
     }
     const int nsc = min(p.sc, p.ns - c * p.sc);
-    const float* win = smem + (c & 1) * wbuf + shift;
+    const float* win = smem + (c & 1) * wbuf;
     const float* pb = par0 + (c & 1) * NPAR * npair;
     const int* pr_lo = reinterpret_cast<const int*>(pb);
     const int* pr_n = pr_lo + npair;
     const float* pr_wb = pb + 2 * npair;
     const float* pr_c = pb + 3 * npair;
+    // partial sums of up to KH_G surface points, then one compensated add
+    float2 c2[KH_RW][KH_T];
+#pragma unroll
+    for (int rho = 0; rho < KH_RW; ++rho)
+#pragma unroll
+      for (int j = 0; j < KH_T; ++j) c2[rho][j] = make_float2(0.f, 0.f);
     for (int sl = 0; ok && sl < nsc; ++sl) {
-      const float* wq = win + (size_t)(NROW * sl) * p.rowpad;
-      const float* wf = wq + p.rowpad;
+      // this point's {q, f} pairs from the first needed sample, and its
+      // running-sum row
+      const float2* wqf = reinterpret_cast<const float2*>(win + (size_t)(NROW * sl) * p.rowpad) + shift;
+      const float* wc = win + (size_t)(NROW * sl + 2) * p.rowpad + shift;
       // taps of this warp's targets: lane-parallel, one exp per tap
 #pragma unroll
       for (int rho = 0; rho < KH_RW; ++rho) {
@@ -279,36 +291,39 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
         // {monopole, dipole} input pairs: one paired FMA per tap and sample
         float2 x2[XN];
 #pragma unroll
-        for (int i = 0; i < XN; ++i) x2[i] = make_float2(wq[base + i], wf[base + i]);
-        float2 c2[KH_T];
-#pragma unroll
-        for (int j = 0; j < KH_T; ++j) c2[j] = make_float2(0.f, 0.f);
+        for (int i = 0; i < XN; ++i) x2[i] = wqf[base + i];
         const float4* t4p = reinterpret_cast<const float4*>(my_taps + rho * 2 * LM);
 #pragma unroll
         for (int k2 = 0; k2 < LM / 2; ++k2) {
           const float4 t4 = t4p[k2];
           const float2 ta = make_float2(t4.x, t4.y), tb2 = make_float2(t4.z, t4.w);
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(ta, x2[j + LM - 1 - 2 * k2], c2[j]);
+          for (int j = 0; j < KH_T; ++j)
+            c2[rho][j] = __ffma2_rn(ta, x2[j + LM - 1 - 2 * k2], c2[rho][j]);
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j) c2[j] = __ffma2_rn(tb2, x2[j + LM - 2 - 2 * k2], c2[j]);
+          for (int j = 0; j < KH_T; ++j)
+            c2[rho][j] = __ffma2_rn(tb2, x2[j + LM - 2 - 2 * k2], c2[rho][j]);
         }
         if (KIND == 1) {  // lags past the window: v_v's constant times the running sum
           const float ped = pr_c[4 * npair + pi];
-          const float* wc = wq + 2 * p.rowpad;
           const int cb = base + LM - 1 - pr_n[pi];
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j) c2[j].y = __fmaf_rn(ped, wc[cb + j], c2[j].y);
+          for (int j = 0; j < KH_T; ++j) c2[rho][j].y = __fmaf_rn(ped, wc[cb + j], c2[rho][j].y);
         }
-        // compensated accumulation over surface points
+      }
+      // compensated accumulation over groups of surface points
+      if (sl % KH_G == KH_G - 1 || sl == nsc - 1) {
 #pragma unroll
-        for (int j = 0; j < KH_T; ++j) {
-          const float cj = __fadd_rn(c2[j].x, c2[j].y);
-          const float y = __fsub_rn(cj, comp[rho][j]);
-          const float t = __fadd_rn(sum[rho][j], y);
-          comp[rho][j] = __fsub_rn(__fsub_rn(t, sum[rho][j]), y);
-          sum[rho][j] = t;
-        }
+        for (int rho = 0; rho < KH_RW; ++rho)
+#pragma unroll
+          for (int j = 0; j < KH_T; ++j) {
+            const float cj = __fadd_rn(c2[rho][j].x, c2[rho][j].y);
+            const float y = __fsub_rn(cj, comp[rho][j]);
+            const float t = __fadd_rn(sum[rho][j], y);
+            comp[rho][j] = __fsub_rn(__fsub_rn(t, sum[rho][j]), y);
+            sum[rho][j] = t;
+            c2[rho][j] = make_float2(0.f, 0.f);
+          }
       }
       __syncwarp();  // taps of the next surface point overwrite the buffer
     }
@@ -364,6 +379,14 @@ struct DevBuf {
 using namespace adf;
 
 // kind 0: pressure, kind 1: normal velocity (adf_kh_pressure / adf_kh_velocity)
+// {q, f} pairs of the padded input columns, so that a window's two channels
+// are read with one 64-bit load
+__global__ void adf_kh_interleave_kernel(const float* q, const float* f, float2* qf, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    qf[i] = make_float2(q[i], f[i]);
+}
+
 static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const float* in_f,
                   float* out, int kind) {
   if (!ctx || !d || !in_q || !in_f || !out || !d->s_pts || !d->s_nrm || !d->r_pts)
@@ -446,11 +469,12 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
                                std::to_string(wmax) + "-sample window, more than shared memory holds");
 
   DevBuf<double> dsp, dsn, drp, drn;
-  DevBuf<float> dq, df, dc, dout;
+  DevBuf<float> dq, df, dqf, dc, dout;
   DevBuf<int2> dtlo;
   DevBuf<int> derr;
   if (!dsp.alloc((size_t)3 * ns) || !dsn.alloc((size_t)3 * ns) || !drp.alloc((size_t)3 * nr) ||
       !dq.alloc((size_t)pitch * ns) || !df.alloc((size_t)pitch * ns) ||
+      !dqf.alloc((size_t)2 * pitch * ns) ||
       !dout.alloc((size_t)nt * nr) ||
       !dtlo.alloc((size_t)ntiles) || !derr.alloc(1) ||
       (kind && (!drn.alloc((size_t)3 * nr) || !dc.alloc((size_t)pitch * ns))))
@@ -476,6 +500,9 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
                     cudaMemcpyHostToDevice, st);
   cudaMemcpy2DAsync(df.p + pad, (size_t)4 * pitch, in_f, (size_t)4 * nt, (size_t)4 * nt, ns,
                     cudaMemcpyHostToDevice, st);
+  adf_kh_interleave_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dq.p, df.p,
+                                                         reinterpret_cast<float2*>(dqf.p),
+                                                         (long long)pitch * ns);
   if (kind) {
     cudaMemcpyAsync(drn.p, d->r_nrm, (size_t)24 * nr, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(dc.p, 0, (size_t)4 * pitch * ns, st);
@@ -503,7 +530,7 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   p.dt_sigma = (float)(d->dt / d->sigma);
   p.sp = dsp.p; p.sn = dsn.p; p.rp = drp.p; p.rn = drn.p;
   p.tile_lo = dtlo.p;
-  p.in_q = dq.p; p.in_f = df.p; p.cs_f = dc.p; p.out = dout.p;
+  p.in_qf = dqf.p; p.cs_f = dc.p; p.out = dout.p;
   p.err = derr.p;
 
   const void* fn = lm == 16 ? (kind ? (const void*)adf_kh_pressure_kernel<16, 1>
