@@ -694,7 +694,7 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 // range of each source is split over gf_ks blocks (blockIdx.x = o*ks + part)
 // whose partial sums the reduce kernel adds in a fixed order.  Rows before
 // `it` of pin come from gf_pin; row `it` is formed here and block 0 files it.
-__global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams p) {
+__global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it = S.it_base + p.step;
   if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
@@ -716,33 +716,74 @@ __global__ void __launch_bounds__(256) adf_gf_extrapolate_kernel(const EpiParams
   const int rb = (int)((long long)nin * part / ks), re = (int)((long long)nin * (part + 1) / ks);
   double a = 0.0, b = 0.0;
   // (r, tt) walk over this block's receivers, tt fastest: contiguous tensor
-  // and pin reads, the index stepped instead of divided
+  // and pin reads, the index stepped instead of divided.  GF_U elements per
+  // round: all their loads are issued before the first is accumulated, so
+  // each thread keeps GF_U loads in flight; the accumulation order of a
+  // thread is the walk order either way.
+  constexpr int GF_U = 4;
   int r = rb + (int)threadIdx.x / T, tt = (int)threadIdx.x - ((int)threadIdx.x / T) * T;
   const int step_r = (int)blockDim.x / T, step_t = (int)blockDim.x - step_r * T;
-  for (; r < re;) {
-    const int row = t0 + tt;
-    // tensor element [T-tt, ., .] (1-based lag) for this receiver and output
-    const long long g = (long long)(T - 1 - tt) +
-                        (long long)ngf * (kind == ADF_GF_PV_FROM_PIN_ ? o + (long long)n1 * r
-                                                                      : r + (long long)n1 * o);
-    if (kind == ADF_GF_PV_FROM_PV_) {
-      const int col = S.gf_irec[r];
-      const float pt = S.rec[0][(long long)row * ntx + col];
-      const float vt = S.vn_rec[(long long)row * ntx + col];
-      const float ps = __fadd_rn(__fmul_rn(S.gf_t[1][g], pt), __fmul_rn(S.gf_t[0][g], vt));
-      const float vs = __fadd_rn(__fmul_rn(S.gf_t[3][g], pt), __fmul_rn(S.gf_t[2][g], vt));
-      a = __dadd_rn(a, (double)ps);
-      b = __dadd_rn(b, (double)vs);
-    } else {
-      const double pin = row == it - 1 ? pin_now(r) : S.gf_pin[(long long)r * nt + row];
-      a = __dadd_rn(a, __dmul_rn((double)S.gf_t[0][g], pin));
-      b = __dadd_rn(b, __dmul_rn((double)S.gf_t[1][g], pin));
+  const long long so = kind == ADF_GF_PV_FROM_PIN_ ? (long long)ngf * o : (long long)ngf * n1 * o;
+  const long long sr = kind == ADF_GF_PV_FROM_PIN_ ? (long long)ngf * n1 : (long long)ngf;
+  while (r < re) {
+    int ru[GF_U], tu[GF_U];
+#pragma unroll
+    for (int u = 0; u < GF_U; ++u) {
+      ru[u] = r;
+      tu[u] = tt;
+      r += step_r;
+      tt += step_t;
+      if (tt >= T) {
+        tt -= T;
+        ++r;
+      }
     }
-    r += step_r;
-    tt += step_t;
-    if (tt >= T) {
-      tt -= T;
-      ++r;
+    if (kind == ADF_GF_PV_FROM_PV_) {
+      float g0[GF_U], g1[GF_U], g2[GF_U], g3[GF_U], pt[GF_U], vt[GF_U];
+#pragma unroll
+      for (int u = 0; u < GF_U; ++u) {
+        if (ru[u] < re) {
+          // tensor element [T-tt, ., .] (1-based lag) for this receiver and output
+          const long long g = (long long)(T - 1 - tu[u]) + so + sr * ru[u];
+          const int col = S.gf_irec[ru[u]];
+          const long long e = (long long)(t0 + tu[u]) * ntx + col;
+          g0[u] = S.gf_t[0][g];
+          g1[u] = S.gf_t[1][g];
+          g2[u] = S.gf_t[2][g];
+          g3[u] = S.gf_t[3][g];
+          pt[u] = S.rec[0][e];
+          vt[u] = S.vn_rec[e];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < GF_U; ++u) {
+        if (ru[u] < re) {
+          const float ps = __fadd_rn(__fmul_rn(g1[u], pt[u]), __fmul_rn(g0[u], vt[u]));
+          const float vs = __fadd_rn(__fmul_rn(g3[u], pt[u]), __fmul_rn(g2[u], vt[u]));
+          a = __dadd_rn(a, (double)ps);
+          b = __dadd_rn(b, (double)vs);
+        }
+      }
+    } else {
+      float g0[GF_U], g1[GF_U];
+      double pin[GF_U];
+#pragma unroll
+      for (int u = 0; u < GF_U; ++u) {
+        if (ru[u] < re) {
+          const long long g = (long long)(T - 1 - tu[u]) + so + sr * ru[u];
+          const int row = t0 + tu[u];
+          g0[u] = S.gf_t[0][g];
+          g1[u] = S.gf_t[1][g];
+          pin[u] = row == it - 1 ? pin_now(ru[u]) : S.gf_pin[(long long)ru[u] * nt + row];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < GF_U; ++u) {
+        if (ru[u] < re) {
+          a = __dadd_rn(a, __dmul_rn((double)g0[u], pin[u]));
+          b = __dadd_rn(b, __dmul_rn((double)g1[u], pin[u]));
+        }
+      }
     }
   }
   __shared__ double red[2][8];
