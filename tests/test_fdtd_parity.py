@@ -26,7 +26,7 @@ def rel_l2(a, b):
 
 
 def make_case(adf, oracle, nx, ny, nz, steps, npml=6, shape="sphere", seed=0, n_rec=40,
-              vn_inject=True, overlap=False, arith="promote"):
+              vn_inject=True, overlap=False, arith="promote", extra=None):
     kw = dict(tmax=(steps - 0.5) * DT, xmax=(nx - 1) * DX / 2, ymax=(ny - 1) * DX / 2,
               zmax=(nz - 1) * DX / 2, nx=nx, ny=ny, nz=nz, c0=C0, r0=RHO, cf=0.5)
     d = adf.Domain(**kw)
@@ -52,6 +52,11 @@ def make_case(adf, oracle, nx, ny, nz, steps, npml=6, shape="sphere", seed=0, n_
         pts.append([0.31 * d.xmax - 0.1 * DX, -0.2 * d.ymax, 0.11 * d.zmax + 0.3 * DX])
         dirs.append([0.0, 0.0, 0.0, 1.0])
         tfs.append(np.zeros(steps))
+    if extra is not None:  # caller-placed transceivers: extra(d, tq) -> [(point, dir, tf)]
+        for pt, dv, tf in extra(d, tq):
+            pts.append(pt)
+            dirs.append(dv)
+            tfs.append(tf)
     rp, rn = oracle.fibonacci_sphere(n_rec, R)
     for i in range(n_rec):
         pts.append(rp[i])
@@ -193,6 +198,31 @@ def test_overlapping_stencils_sequential_order(adf, oracle, ctx):
     """Overlapping source/receiver stencils: the reference's threaded loop is
     racy there; both implementations use ascending transceiver order."""
     case = make_case(adf, oracle, 40, 36, 32, steps=40, npml=4, shape="none", seed=3, overlap=True)
+    gpu, cpu = run_both(adf, oracle, case)
+    assert_parity(gpu, cpu, 1e-6)
+
+
+def test_entries_on_tile_edges(adf, oracle, ctx):
+    """Sources and receivers whose trilinear stencils straddle the step
+    kernel's tile edges: x = 63|64 and 127|128 (64-cell x tiles: the halo
+    column), y = 6|7 and 13|14 (7-row tiles: the halo row), z = 15|16 and
+    31|32 (16-plane chunks: the prologue plane).  Their injection must reach
+    the neighbouring tile's recomputed halo and every recording must be
+    written once; the result must match the oracle."""
+    def edges(d, tq):
+        def at(i, j, k):  # fractional P-grid cell coordinates (0-based) -> position
+            return [-d.xmax + i * DX, -d.ymax + j * DX, -d.zmax + k * DX]
+        n = len(tq)
+        return [
+            (at(63.5, 6.5, 15.5), [1.0, 0, 0, 0], tq * 700.0),            # q source on three edges
+            (at(127.6, 13.4, 31.5), [0.0, 0.6, -0.48, 0.64], tq * 1.5),   # f dipole on three edges
+            (at(64.2, 7.3, 16.1), [0.0, 0.0, 0.6, 0.8], np.zeros(n)),     # receivers just across
+            (at(63.0, 6.0, 15.0), [0.0, 1.0, 0.0, 0.0], np.zeros(n)),     # on a P node at the edges
+            (at(128.4, 20.5, 31.9), [0.0, 0.0, 0.0, 1.0], np.zeros(n)),
+            (at(0.6, 27.5, 47.5), [0.0, 1.0, 0.0, 0.0], np.zeros(n)),     # inside the x slab
+        ]
+    case = make_case(adf, oracle, 140, 30, 50, steps=40, npml=6, shape="sphere", seed=4,
+                     n_rec=24, extra=edges)
     gpu, cpu = run_both(adf, oracle, case)
     assert_parity(gpu, cpu, 1e-6)
 
