@@ -1,6 +1,5 @@
 // adf_internal.h -- structures shared by the host runtime and the kernels.
 #pragma once
-#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 

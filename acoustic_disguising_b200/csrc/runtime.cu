@@ -1,10 +1,9 @@
 // runtime.cu -- host runtime behind the C-ABI (include/adfdtd.h).
 //
-// Owns device memory, builds the per-solve descriptors, entry lists and TMA
-// tensor maps, and drives the fused step kernel.  Layout conversions between
+// Owns device memory, builds the per-solve descriptors, entry lists and work
+// items, and drives the fused step kernel.  Layout conversions between
 // the reference's Julia arrays and the HBM layout (see adf_internal.h) happen
 // here, once per call.
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <chrono>

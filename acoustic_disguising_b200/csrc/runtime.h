@@ -1,6 +1,5 @@
 // runtime.h -- host-side objects behind the C-ABI.
 #pragma once
-#include <cudaTypedefs.h>
 
 #include <string>
 #include <vector>

@@ -240,8 +240,8 @@ typedef struct {
 } adf_gf_request;
 
 /* Runs n requests.  batched=1: all requests that fit the HBM budget advance
- * together, one persistent launch per time step over a (solve, tile) work
- * list, the step loop captured in CUDA graphs.  batched=0: the plain path,
+ * together, one step-kernel launch per time step over all of their (solve,
+ * tile, z chunk) work items, the step loop captured in CUDA graphs.  batched=0: the plain path,
  * one solve at a time, one launch per step.                               */
 int adf_gf_solve_batch(adf_ctx* ctx, int64_t n, adf_gf_request* reqs, int batched);
 
