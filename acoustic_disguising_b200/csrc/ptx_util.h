@@ -40,7 +40,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
     if (mbar_try_wait(a, parity)) return true;
   return false;
 }
-// One-dimensional bulk copy global -> shared (no multicast), completing on
+// One-dimensional bulk copy global -> this CTA's shared memory, completing on
 // an mbarrier.  dst and src 16-B aligned, bytes a multiple of 16.
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
                                           uint32_t mbar) {
