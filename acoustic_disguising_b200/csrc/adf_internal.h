@@ -23,6 +23,10 @@ enum : int {
   SF_GF = 32,       // in-loop GF extrapolation between v2vn and vn2v
 };
 
+// Steps per block of the in-loop GF extrapolation: lags older than the block
+// are summed once per block, the rest step by step.
+constexpr int kGfBlock = 32;
+
 // GF map kinds, as ADF_GF_* in include/adfdtd.h
 enum : int { ADF_GF_PV_FROM_PIN_ = 0, ADF_GF_P_FROM_PIN_ = 1, ADF_GF_PV_FROM_PV_ = 2 };
 
@@ -69,10 +73,13 @@ struct SolveDev {
   const int* gf_irec;     // [n_in] 0-based transceiver columns read
   double* gf_pin;         // [n_in][nt] (p_rec - z0 vn_rec)/2 of recorded rows
   double* gf_part;        // [n_out][gf_ks][2] partial sums of the split reduction
+  double* gf_far;         // [n_out][gf_rs][kGfBlock][2] far-lag partials of the current
+                          // block of steps, or NULL (the map is summed step by step)
   double gf_z0;
   int gf_kind, gf_nt, gf_n1, gf_n2;
   int gf_nout, gf_nin;
-  int gf_ks, gf_pad_;     // receiver splits per driven source
+  int gf_ks;              // receiver splits per driven source (per-step kernel)
+  int gf_rs;              // receiver splits of the far-lag kernel, 0 = no blocking
 };
 
 // work item: {solve index, y tile | x tile << 16, z0, z1}
@@ -99,5 +106,8 @@ int step_x_tile();  // cells per x tile of a step work item
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
                                   cudaStream_t s);
+// far-lag part of the in-loop GF extrapolation for the block of kGfBlock steps
+// that starts at launch-step p.step
+cudaError_t launch_gf_far(const EpiParams& p, int max_blocks, int max_nsrc, cudaStream_t s);
 
 }  // namespace adf

@@ -703,7 +703,9 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
   if (o >= S.gf_nout) return;
   const int nt = S.nt, ntx = S.ntx, ngf = S.gf_nt, n1 = S.gf_n1, nin = S.gf_nin;
   const int kind = S.gf_kind;
-  const int T = min(it, ngf);
+  // lags 0..T-1 (T = min(it, ngf)); with blocking only 0..b, b = this step's
+  // place in its block, the older lags coming from adf_gf_far_kernel
+  const int T = S.gf_rs > 0 ? min(min(it, ngf), p.step % kGfBlock + 1) : min(it, ngf);
   const int t0 = it - T;  // 0-based row of tt = 1
   const long long cur = (long long)(it - 1) * ntx;
   auto pin_now = [&](int r) {
@@ -810,6 +812,117 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
   }
 }
 
+// Far-lag part of the in-loop GF extrapolation (extrapolation.jl:139-170),
+// block-causal form.  For the block of kGfBlock steps it0 .. it0+B-1 that
+// starts at this launch-step, step it0+b needs lags 0 .. T_b-1 of the map
+// (T_b = min(it0+b, ngf)).  Lags b+1 .. T_b-1 read input-history rows
+// it0-1+b-lag <= it0-2, all complete before the block starts, so they are
+// summed here once for the whole block: a contraction over (receiver, lag)
+// of the block's 32 steps x 32 sources, which reads each tensor slice once
+// per block instead of once per step.  Lags 0..b, whose rows appear during
+// the block, stay in adf_gf_extrapolate_kernel.  FP64 fused multiply-adds;
+// one partial per (source, receiver split, step), added in split order by
+// adf_gf_reduce_kernel.  Input-history kinds only.
+constexpr int kGfLC = 64;  // lags per staged chunk
+__global__ void __launch_bounds__(256) adf_gf_far_kernel(const EpiParams p) {
+  const SolveDev& S = p.solves[blockIdx.y];
+  const int it0 = S.it_base + p.step;
+  if (S.gf_rs <= 0 || it0 > S.it_stop || it0 >= S.nt || !(S.flags & SF_GF)) return;
+  const int rsn = S.gf_rs, nout = S.gf_nout;
+  const int ot = blockIdx.x / rsn, rsi = blockIdx.x - ot * rsn;
+  if (ot * 32 >= nout) return;
+  const int nt = S.nt, ngf = S.gf_nt, n1 = S.gf_n1, nin = S.gf_nin;
+  const bool pv = S.gf_kind == ADF_GF_PV_FROM_PIN_;
+  const int r0 = (int)((long long)nin * rsi / rsn), r1 = (int)((long long)nin * (rsi + 1) / rsn);
+  const int ol = (int)threadIdx.x & 31, bg = (int)threadIdx.x >> 5;  // steps b = bg + 8q
+  const int o = ot * 32 + ol;
+  __shared__ float sG[2][kGfLC][33];                 // lag-major, padded against conflicts
+  __shared__ double sH[kGfLC + kGfBlock - 1];        // history rows of the chunk
+  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  const int lag_hi = min(it0 + kGfBlock - 1, ngf) - 1;  // largest lag any step of the block uses
+  for (int r = r0; r < r1; ++r) {
+    const double* hist = S.gf_pin + (long long)r * nt;
+    for (int l0 = 1; l0 <= lag_hi; l0 += kGfLC) {
+      __syncthreads();  // the previous chunk has been used
+      for (int i = threadIdx.x; i < 32 * kGfLC; i += blockDim.x) {
+        const int oo = i / kGfLC, ll = i - oo * kGfLC;  // lag fastest: coalesced reads
+        const int lag = l0 + ll, og = ot * 32 + oo;
+        float v0 = 0.f, v1 = 0.f;
+        if (lag <= lag_hi && og < nout) {
+          const long long col = pv ? (long long)ngf * (og + (long long)n1 * r)
+                                   : (long long)ngf * (r + (long long)n1 * og);
+          v0 = S.gf_t[0][col + lag];
+          v1 = S.gf_t[1][col + lag];
+        }
+        sG[0][ll][oo] = v0;
+        sG[1][ll][oo] = v1;
+      }
+      // rows it0-1+b-lag of this chunk lie in [hlo, hlo + kGfLC + kGfBlock - 2]
+      const int hlo = it0 - l0 - kGfLC;
+      for (int i = threadIdx.x; i < kGfLC + kGfBlock - 1; i += blockDim.x) {
+        const int row = hlo + i;
+        sH[i] = (row >= 0 && row < nt) ? hist[row] : 0.0;
+      }
+      __syncthreads();
+      if (l0 >= kGfBlock && l0 + kGfLC <= min(it0, ngf)) {
+        // every lag of the chunk is past every step of the block and below
+        // every step's T: no per-step test
+        for (int ll = 0; ll < kGfLC; ++ll) {
+          const double g0 = (double)sG[0][ll][ol], g1 = (double)sG[1][ll][ol];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const double h = sH[bg + 8 * q + kGfLC - 1 - ll];
+            acc[0][q] = __fma_rn(g0, h, acc[0][q]);
+            acc[1][q] = __fma_rn(g1, h, acc[1][q]);
+          }
+        }
+      } else {
+        for (int ll = 0; ll < kGfLC; ++ll) {
+          const int lag = l0 + ll;
+          const double g0 = (double)sG[0][ll][ol], g1 = (double)sG[1][ll][ol];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int b = bg + 8 * q;
+            if (lag > b && lag < min(it0 + b, ngf)) {  // row it0-1+b-lag is complete and >= 0
+              const double h = sH[b + kGfLC - 1 - ll];
+              acc[0][q] = __fma_rn(g0, h, acc[0][q]);
+              acc[1][q] = __fma_rn(g1, h, acc[1][q]);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (o < nout) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double* pp = S.gf_far + (((long long)o * rsn + rsi) * kGfBlock + bg + 8 * q) * 2;
+      pp[0] = acc[0][q];
+      pp[1] = acc[1][q];
+    }
+  }
+}
+
+// Sums the far-lag partials of each (source, step of the block) over the
+// receiver splits, in split order, into split 0's slot.
+__global__ void adf_gf_far_combine_kernel(const EpiParams p) {
+  const SolveDev& S = p.solves[blockIdx.y];
+  const int it0 = S.it_base + p.step;
+  if (S.gf_rs <= 0 || it0 > S.it_stop || it0 >= S.nt || !(S.flags & SF_GF)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // (source, step of the block)
+  if (i >= S.gf_nout * kGfBlock) return;
+  const int o = i / kGfBlock, b = i - o * kGfBlock;
+  double sa = 0.0, sb = 0.0;
+  for (int k = 0; k < S.gf_rs; ++k) {
+    const double* pp = S.gf_far + (((long long)o * S.gf_rs + k) * kGfBlock + b) * 2;
+    sa = __dadd_rn(sa, pp[0]);
+    sb = __dadd_rn(sb, pp[1]);
+  }
+  double* out = S.gf_far + ((long long)o * S.gf_rs * kGfBlock + b) * 2;
+  out[0] = sa;
+  out[1] = sb;
+}
+
 // Adds each source's partial sums in split order and writes its p_src and
 // vn_src samples of row it+1.
 __global__ void adf_gf_reduce_kernel(const EpiParams p) {
@@ -821,6 +934,12 @@ __global__ void adf_gf_reduce_kernel(const EpiParams p) {
   double sa = 0.0, sb = 0.0;
   for (int k = 0; k < S.gf_ks; ++k) {
     const double* pp = S.gf_part + ((long long)o * S.gf_ks + k) * 2;
+    sa = __dadd_rn(sa, pp[0]);
+    sb = __dadd_rn(sb, pp[1]);
+  }
+  if (S.gf_rs > 0) {  // the far lags of this step, summed at its block's start
+    const double* pp =
+        S.gf_far + ((long long)o * S.gf_rs * kGfBlock + p.step % kGfBlock) * 2;
     sa = __dadd_rn(sa, pp[0]);
     sb = __dadd_rn(sb, pp[1]);
   }
@@ -865,6 +984,14 @@ cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_ns
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   adf_gf_reduce_kernel<<<dim3((max_nsrc + 127) / 128, p.n_solves), 128, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gf_far(const EpiParams& p, int max_blocks, int max_nsrc, cudaStream_t s) {
+  adf_gf_far_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), 256, 0, s>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  adf_gf_far_combine_kernel<<<dim3((max_nsrc * kGfBlock + 255) / 256, p.n_solves), 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 

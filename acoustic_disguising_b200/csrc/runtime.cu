@@ -365,11 +365,14 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   max_ntx = 0;
   max_gf_nsrc = 0;
   max_gf_blocks = 0;
+  max_gf_far_blocks = 0;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
     if (sd[i].flags & SF_GF) {
       max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
       max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
+      if (sd[i].gf_rs > 0)
+        max_gf_far_blocks = std::max(max_gf_far_blocks, (sd[i].gf_nout + 31) / 32 * sd[i].gf_rs);
     }
     const SolveDev& d = list[i]->dev;
     max_ty = std::max(max_ty, d.ty);
@@ -449,6 +452,10 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
   if (max_gf_nsrc > 0) {  // in-loop GF extrapolation, then vn2v! of those solves
+    // the far lags of a block of steps, at the block's first launch-step
+    if (max_gf_far_blocks > 0 && step % kGfBlock == 0 &&
+        (e2 = launch_gf_far(ep, max_gf_far_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
+      return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
     if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
     ep.phase = 2;
@@ -491,7 +498,7 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
   while (nsteps - done >= chunk) {
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += per_step * chunk + 1;
+    ctx->launches += per_step * chunk + 1 + (max_gf_far_blocks > 0 ? 2 * chunk / kGfBlock : 0);
     done += chunk;
   }
   for (int s = 0; s < nsteps - done; ++s) {
@@ -526,7 +533,7 @@ int Batch::run_chunk(adf_ctx* ctx, int n, int chunk) {
     }
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += per_step * chunk + 1;
+    ctx->launches += per_step * chunk + 1 + (max_gf_far_blocks > 0 ? 2 * chunk / kGfBlock : 0);
     return ADF_OK;
   }
   for (int s = 0; s < n; ++s) {
@@ -953,13 +960,29 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_src, rc);
     int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_rec, rc);
     double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_rec * d->nt, rc);
-    // receiver splits: about eight 256-thread blocks per SM in all
-    const int ks = (int)std::max<int64_t>(
-        1, std::min<int64_t>(gf->n_rec, (int64_t)8 * ctx->nsm / std::max<int64_t>(1, gf->n_src)));
+    // receiver splits of the per-step kernel: about eight 256-thread blocks
+    // per SM in all; one per source when the far lags are blocked (it then
+    // sums at most kGfBlock lags per receiver)
+    const int ks = gf->kind != ADF_GF_PV_FROM_PV
+                       ? 1
+                       : (int)std::max<int64_t>(
+                             1, std::min<int64_t>(gf->n_rec, (int64_t)8 * ctx->nsm /
+                                                                 std::max<int64_t>(1, gf->n_src)));
     double* part = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_src * ks * 2, rc);
+    // block-causal far lags for the input-history kinds: receiver splits for
+    // about two 256-thread blocks per SM over the 32-source tiles
+    int rs = 0;
+    double* far = nullptr;
+    if (gf->kind != ADF_GF_PV_FROM_PV && !rc) {
+      const int64_t otiles = (gf->n_src + 31) / 32;
+      rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (2 * ctx->nsm + otiles - 1) / otiles));
+      far = solve_dalloc<double>(*s, (size_t)gf->n_src * rs * kGfBlock * 2, rc);
+    }
     if (rc) return rc;
     sd.gf_part = part;
     sd.gf_ks = ks;
+    sd.gf_far = far;
+    sd.gf_rs = rs;
     std::vector<int> cs((size_t)gf->n_src), cr((size_t)gf->n_rec);
     for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
     for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);

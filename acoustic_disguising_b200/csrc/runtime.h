@@ -39,6 +39,7 @@ struct adf_ctx {
 namespace adf {
 
 constexpr int kGraphChunk = 32;  // steps per captured CUDA graph
+static_assert(kGraphChunk % kGfBlock == 0, "a graph chunk holds whole GF blocks");
 
 int fail(int code, const std::string& msg);
 
@@ -91,6 +92,7 @@ struct Batch {
   int max_ty = 1;            // tallest tile in the batch: the block is (32, max_ty + 1)
   int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
   int max_gf_blocks = 0;     // (source, receiver split) blocks of the GF kernel
+  int max_gf_far_blocks = 0; // (source tile, receiver split) blocks of the far-lag kernel
   int per_step = 2;          // kernel launches per launch-step
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;

@@ -69,16 +69,21 @@ def test_oracle_gf_discard_is_the_plain_run():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind,discard,tol", [
-    ("PVFromPin", False, 1e-6), ("PVFromPin", True, 1e-6), ("PFromPin", False, 1e-6),
+@pytest.mark.parametrize("kind,discard,tol,steps,nt_gf", [
+    ("PVFromPin", False, 1e-6, 60, 24), ("PVFromPin", True, 1e-6, 60, 24),
+    ("PFromPin", False, 1e-6, 60, 24),
     # PVFromPV: the reference sums Float32 terms sequentially in Float32, the
     # GPU in Float64, so the driven sources differ by Float32 round-off
-    ("PVFromPV", False, 1e-5),
+    ("PVFromPV", False, 1e-5, 60, 24),
+    # graph-replayed chunks, more lags than the 32 steps of a block: the far
+    # lags of each block come from the block-causal kernel
+    ("PVFromPin", False, 1e-6, 100, 40), ("PFromPin", False, 1e-6, 100, 40),
 ])
-def test_gf_map_matches_oracle(adf, oracle, ctx, kind, discard, tol):
-    case = make_case(adf, oracle, 40, 36, 32, steps=60, npml=5, shape="sphere", seed=8, n_rec=40)
+def test_gf_map_matches_oracle(adf, oracle, ctx, kind, discard, tol, steps, nt_gf):
+    case = make_case(adf, oracle, 40, 36, 32, steps=steps, npml=5, shape="sphere", seed=8,
+                     n_rec=40)
     d, o, g, cp, mask, field = case
-    ts, isr, irc = gf_inputs(g.dir.shape[1], kind)
+    ts, isr, irc = gf_inputs(g.dir.shape[1], kind, nt_gf=nt_gf)
     gg = to_adf_grid(adf, g)
     pc = _Cp(adf, cp)
     f_gpu = field.copy(order="F")
