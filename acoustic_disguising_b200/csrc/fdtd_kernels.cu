@@ -823,30 +823,37 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
 // the block, stay in adf_gf_extrapolate_kernel.  FP64 fused multiply-adds;
 // one partial per (source, receiver split, step), added in split order by
 // adf_gf_reduce_kernel.  Input-history kinds only.
-constexpr int kGfLC = 64;  // lags per staged chunk
+constexpr int kGfLC = 32;  // lags per staged chunk
+constexpr int kGfOT = 64;  // sources per tile (two per thread)
 __global__ void __launch_bounds__(256) adf_gf_far_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it0 = S.it_base + p.step;
   if (S.gf_rs <= 0 || it0 > S.it_stop || it0 >= S.nt || !(S.flags & SF_GF)) return;
   const int rsn = S.gf_rs, nout = S.gf_nout;
   const int ot = blockIdx.x / rsn, rsi = blockIdx.x - ot * rsn;
-  if (ot * 32 >= nout) return;
+  if (ot * kGfOT >= nout) return;
   const int nt = S.nt, ngf = S.gf_nt, n1 = S.gf_n1, nin = S.gf_nin;
   const bool pv = S.gf_kind == ADF_GF_PV_FROM_PIN_;
   const int r0 = (int)((long long)nin * rsi / rsn), r1 = (int)((long long)nin * (rsi + 1) / rsn);
-  const int ol = (int)threadIdx.x & 31, bg = (int)threadIdx.x >> 5;  // steps b = bg + 8q
-  const int o = ot * 32 + ol;
-  __shared__ float sG[2][kGfLC][33];                 // lag-major, padded against conflicts
-  __shared__ double sH[kGfLC + kGfBlock - 1];        // history rows of the chunk
-  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  // thread: sources ol and ol+32 of the tile, steps b = bg + 8q of the block
+  const int ol = (int)threadIdx.x & 31, bg = (int)threadIdx.x >> 5;
+  __shared__ double sG[2][kGfLC][kGfOT + 1];   // lag-major, Float64, padded against conflicts
+  __shared__ double sH[kGfLC + kGfBlock - 1];  // history rows of the chunk
+  double acc[2][2][4];
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[t][h][q] = 0.0;
   const int lag_hi = min(it0 + kGfBlock - 1, ngf) - 1;  // largest lag any step of the block uses
   for (int r = r0; r < r1; ++r) {
     const double* hist = S.gf_pin + (long long)r * nt;
     for (int l0 = 1; l0 <= lag_hi; l0 += kGfLC) {
       __syncthreads();  // the previous chunk has been used
-      for (int i = threadIdx.x; i < 32 * kGfLC; i += blockDim.x) {
+      for (int i = threadIdx.x; i < kGfOT * kGfLC; i += blockDim.x) {
         const int oo = i / kGfLC, ll = i - oo * kGfLC;  // lag fastest: coalesced reads
-        const int lag = l0 + ll, og = ot * 32 + oo;
+        const int lag = l0 + ll, og = ot * kGfOT + oo;
         float v0 = 0.f, v1 = 0.f;
         if (lag <= lag_hi && og < nout) {
           const long long col = pv ? (long long)ngf * (og + (long long)n1 * r)
@@ -854,8 +861,8 @@ __global__ void __launch_bounds__(256) adf_gf_far_kernel(const EpiParams p) {
           v0 = S.gf_t[0][col + lag];
           v1 = S.gf_t[1][col + lag];
         }
-        sG[0][ll][oo] = v0;
-        sG[1][ll][oo] = v1;
+        sG[0][ll][oo] = (double)v0;
+        sG[1][ll][oo] = (double)v1;
       }
       // rows it0-1+b-lag of this chunk lie in [hlo, hlo + kGfLC + kGfBlock - 2]
       const int hlo = it0 - l0 - kGfLC;
@@ -864,41 +871,35 @@ __global__ void __launch_bounds__(256) adf_gf_far_kernel(const EpiParams p) {
         sH[i] = (row >= 0 && row < nt) ? hist[row] : 0.0;
       }
       __syncthreads();
-      if (l0 >= kGfBlock && l0 + kGfLC <= min(it0, ngf)) {
-        // every lag of the chunk is past every step of the block and below
-        // every step's T: no per-step test
-        for (int ll = 0; ll < kGfLC; ++ll) {
-          const double g0 = (double)sG[0][ll][ol], g1 = (double)sG[1][ll][ol];
+      const bool full = l0 >= kGfBlock && l0 + kGfLC <= min(it0, ngf);
+      for (int ll = 0; ll < kGfLC; ++ll) {
+        const int lag = l0 + ll;
+        const double g00 = sG[0][ll][ol], g01 = sG[0][ll][ol + 32];
+        const double g10 = sG[1][ll][ol], g11 = sG[1][ll][ol + 32];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const double h = sH[bg + 8 * q + kGfLC - 1 - ll];
-            acc[0][q] = __fma_rn(g0, h, acc[0][q]);
-            acc[1][q] = __fma_rn(g1, h, acc[1][q]);
-          }
-        }
-      } else {
-        for (int ll = 0; ll < kGfLC; ++ll) {
-          const int lag = l0 + ll;
-          const double g0 = (double)sG[0][ll][ol], g1 = (double)sG[1][ll][ol];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int b = bg + 8 * q;
-            if (lag > b && lag < min(it0 + b, ngf)) {  // row it0-1+b-lag is complete and >= 0
-              const double h = sH[b + kGfLC - 1 - ll];
-              acc[0][q] = __fma_rn(g0, h, acc[0][q]);
-              acc[1][q] = __fma_rn(g1, h, acc[1][q]);
-            }
+        for (int q = 0; q < 4; ++q) {
+          const int b = bg + 8 * q;
+          // past every step of the block and below every step's T, or checked
+          if (full || (lag > b && lag < min(it0 + b, ngf))) {
+            const double h = sH[b + kGfLC - 1 - ll];
+            acc[0][0][q] = __fma_rn(g00, h, acc[0][0][q]);
+            acc[0][1][q] = __fma_rn(g01, h, acc[0][1][q]);
+            acc[1][0][q] = __fma_rn(g10, h, acc[1][0][q]);
+            acc[1][1][q] = __fma_rn(g11, h, acc[1][1][q]);
           }
         }
       }
     }
   }
-  if (o < nout) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int o = ot * kGfOT + ol + 32 * h;
+    if (o >= nout) continue;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       double* pp = S.gf_far + (((long long)o * rsn + rsi) * kGfBlock + bg + 8 * q) * 2;
-      pp[0] = acc[0][q];
-      pp[1] = acc[1][q];
+      pp[0] = acc[0][h][q];
+      pp[1] = acc[1][h][q];
     }
   }
 }

@@ -372,7 +372,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
       max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
       max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
       if (sd[i].gf_rs > 0)
-        max_gf_far_blocks = std::max(max_gf_far_blocks, (sd[i].gf_nout + 31) / 32 * sd[i].gf_rs);
+        max_gf_far_blocks = std::max(max_gf_far_blocks, (sd[i].gf_nout + 63) / 64 * sd[i].gf_rs);
     }
     const SolveDev& d = list[i]->dev;
     max_ty = std::max(max_ty, d.ty);
@@ -970,11 +970,11 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
                                                                  std::max<int64_t>(1, gf->n_src)));
     double* part = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_src * ks * 2, rc);
     // block-causal far lags for the input-history kinds: receiver splits for
-    // about two 256-thread blocks per SM over the 32-source tiles
+    // about two 256-thread blocks per SM over the 64-source tiles
     int rs = 0;
     double* far = nullptr;
     if (gf->kind != ADF_GF_PV_FROM_PV && !rc) {
-      const int64_t otiles = (gf->n_src + 31) / 32;
+      const int64_t otiles = (gf->n_src + 63) / 64;
       rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (2 * ctx->nsm + otiles - 1) / otiles));
       far = solve_dalloc<double>(*s, (size_t)gf->n_src * rs * kGfBlock * 2, rc);
     }
