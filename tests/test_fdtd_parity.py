@@ -173,7 +173,10 @@ def test_reciprocity_gpu(adf, oracle, ctx):
     (36, 33, 34, 1, "none"),       # npml=1: p-side CPML off without a mask
     (36, 33, 34, 1, "sphere"),     # npml=1 with a mask: p-side CPML on (no guard)
     (40, 40, 40, 0, "cube"),       # masked, no CPML
-    (300, 20, 18, 6, "sphere"),    # rows wider than 256 cells: two x boxes per row
+    (300, 20, 18, 6, "sphere"),    # five x tiles per row, the last one partial
+    (134, 24, 30, 6, "sphere"),    # x tile 1 meets only the v side of the x slab (x = 127)
+    (140, 22, 34, 15, "sphere"),   # npml = 15: the widest x slab staged with the field
+    (150, 24, 36, 18, "none"),     # npml = 18: x-slab memory read from global memory
 ])
 def test_run_fdtd_parity(adf, oracle, ctx, nx, ny, nz, npml, shape):
     case = make_case(adf, oracle, nx, ny, nz, steps=60, npml=npml, shape=shape, seed=nx + npml)
@@ -184,9 +187,9 @@ def test_run_fdtd_parity(adf, oracle, ctx, nx, ny, nz, npml, shape):
 
 @pytest.mark.parametrize("tile", ["8,16", "12,16", "2,8", "5,32"])
 def test_tile_shapes(adf, oracle, ctx, monkeypatch, tile):
-    """Every tile height / z-chunk depth gives the same result: 8-row tiles
-    (the large-grid default), 12-row tiles (y/z CPML memory read from global
-    memory instead of staged), 2-row tiles with short z chunks."""
+    """Every tile height / z-chunk depth gives the same result: heights above
+    the kernel's 7 rows (clamped to 7), 2-row tiles with short z chunks and
+    5-row tiles with 32-plane chunks."""
     monkeypatch.setenv("ADF_TILE", tile)
     case = make_case(adf, oracle, 48, 44, 40, steps=50, npml=6, shape="sphere", seed=17)
     gpu, cpu = run_both(adf, oracle, case)
