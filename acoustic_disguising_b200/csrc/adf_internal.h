@@ -104,7 +104,7 @@ cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t 
 int step_max_ty();
 int step_x_tile();  // cells per x tile of a step work item
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
-cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc, bool reduce,
                                   cudaStream_t s);
 // far-lag part of the in-loop GF extrapolation for the block of kGfBlock steps
 // that starts at launch-step p.step

@@ -680,6 +680,30 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 
 // Advances it_base of every solve by `by` steps: the last node of a captured
 // chunk of steps, so replaying the graph continues where it stopped.
+// Completes source o of step it from its summed lags: adds the far lags
+// summed at the block's start (block-causal kinds) and writes the p_src and
+// vn_src samples of row it+1 (extrapolation.jl:215-216, 228-229, 246-247).
+__device__ __forceinline__ void gf_finish(const SolveDev& S, int o, int it, int step, double sa,
+                                          double sb) {
+  if (S.gf_rs > 0) {
+    const double* pp = S.gf_far + ((long long)o * S.gf_rs * kGfBlock + step % kGfBlock) * 2;
+    sa = __dadd_rn(sa, pp[0]);
+    sb = __dadd_rn(sb, pp[1]);
+  }
+  const int col = S.gf_isrc[o];
+  float ps, vs;
+  if (S.gf_kind == ADF_GF_P_FROM_PIN_) {
+    const float pos = (float)sa, neg = (float)sb;
+    ps = (float)((double)__fadd_rn(pos, neg) / S.gf_z0);  // vn_src
+    vs = __fsub_rn(pos, neg);                              // p_src
+  } else {
+    ps = (float)sa;  // vn_src <- p_pin / (pv, pp)-derived
+    vs = (float)sb;  // p_src  <- v_pin / (vv, vp)-derived
+  }
+  S.src[0][(long long)it * S.src_ntx + col] = vs;
+  S.vn_src[(long long)it * S.ntx + col] = ps;
+}
+
 // In-loop GF extrapolation, extrapolate! (src/kernels/extrapolation.jl:204-249)
 // after v2vn! of step it < nt, for every driven source o:
 //   PVFromPin (:139-170): pin[t, r] = (p_rec - z0 vn_rec)/2 (Float64);
@@ -692,7 +716,8 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 // Sums are accumulated in Float64 (the Float32 zero of the reference is
 // promoted by the first Float64 add for the *FromPin kinds).  The receiver
 // range of each source is split over gf_ks blocks (blockIdx.x = o*ks + part)
-// whose partial sums the reduce kernel adds in a fixed order.  Rows before
+// whose partial sums the reduce kernel adds in a fixed order; with one block
+// per source (ks = 1) that block completes the source itself.  Rows before
 // `it` of pin come from gf_pin; row `it` is formed here and block 0 files it.
 __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
@@ -806,9 +831,13 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
       sa = __dadd_rn(sa, red[0][k]);
       sb = __dadd_rn(sb, red[1][k]);
     }
-    double* pp = S.gf_part + ((long long)o * ks + part) * 2;
-    pp[0] = sa;
-    pp[1] = sb;
+    if (ks == 1) {
+      gf_finish(S, o, it, p.step, sa, sb);
+    } else {
+      double* pp = S.gf_part + ((long long)o * ks + part) * 2;
+      pp[0] = sa;
+      pp[1] = sb;
+    }
   }
 }
 
@@ -925,11 +954,11 @@ __global__ void adf_gf_far_combine_kernel(const EpiParams p) {
 }
 
 // Adds each source's partial sums in split order and writes its p_src and
-// vn_src samples of row it+1.
+// vn_src samples of row it+1 (solves with more than one block per source).
 __global__ void adf_gf_reduce_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it = S.it_base + p.step;
-  if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF)) return;
+  if (it > S.it_stop || it >= S.nt || !(S.flags & SF_GF) || S.gf_ks == 1) return;
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= S.gf_nout) return;
   double sa = 0.0, sb = 0.0;
@@ -938,24 +967,7 @@ __global__ void adf_gf_reduce_kernel(const EpiParams p) {
     sa = __dadd_rn(sa, pp[0]);
     sb = __dadd_rn(sb, pp[1]);
   }
-  if (S.gf_rs > 0) {  // the far lags of this step, summed at its block's start
-    const double* pp =
-        S.gf_far + ((long long)o * S.gf_rs * kGfBlock + p.step % kGfBlock) * 2;
-    sa = __dadd_rn(sa, pp[0]);
-    sb = __dadd_rn(sb, pp[1]);
-  }
-  const int col = S.gf_isrc[o];
-  float ps, vs;
-  if (S.gf_kind == ADF_GF_P_FROM_PIN_) {
-    const float pos = (float)sa, neg = (float)sb;
-    ps = (float)((double)__fadd_rn(pos, neg) / S.gf_z0);  // vn_src
-    vs = __fsub_rn(pos, neg);                              // p_src
-  } else {
-    ps = (float)sa;  // vn_src <- p_pin / (pv, pp)-derived
-    vs = (float)sb;  // p_src  <- v_pin / (vv, vp)-derived
-  }
-  S.src[0][(long long)it * S.src_ntx + col] = vs;
-  S.vn_src[(long long)it * S.ntx + col] = ps;
+  gf_finish(S, o, it, p.step, sa, sb);
 }
 
 __global__ void adf_advance_kernel(SolveDev* solves, int n, int by) {
@@ -977,13 +989,13 @@ cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t 
 int step_max_ty() { return kMaxTy; }
 int step_x_tile() { return kXT; }
 
-cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc,
+cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc, bool reduce,
                                   cudaStream_t s) {
-  // (source, receiver split) blocks of the largest map in the batch, then
-  // the fixed-order reduction of the splits
+  // (source, receiver split) blocks of the largest map in the batch, then,
+  // when some solve splits its receivers, the fixed-order reduction
   adf_gf_extrapolate_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), 256, 0, s>>>(p);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if (e != cudaSuccess || !reduce) return e;
   adf_gf_reduce_kernel<<<dim3((max_nsrc + 127) / 128, p.n_solves), 128, 0, s>>>(p);
   return cudaGetLastError();
 }

@@ -366,11 +366,13 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   max_gf_nsrc = 0;
   max_gf_blocks = 0;
   max_gf_far_blocks = 0;
+  gf_reduce = false;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
     if (sd[i].flags & SF_GF) {
       max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
       max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
+      gf_reduce = gf_reduce || sd[i].gf_ks > 1;
       if (sd[i].gf_rs > 0)
         max_gf_far_blocks = std::max(max_gf_far_blocks, (sd[i].gf_nout + 63) / 64 * sd[i].gf_rs);
     }
@@ -411,7 +413,9 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
   cudaStreamSynchronize(st);
-  per_step = max_gf_nsrc > 0 ? 5 : 2;
+  // step + epilogue; GF solves add the extrapolation, its reduction when a
+  // source's receivers are split, and the vn2v! epilogue
+  per_step = max_gf_nsrc > 0 ? (gf_reduce ? 5 : 4) : 2;
   if (max_ty > step_max_ty()) return fail(ADF_E_ARG, "tile taller than the step kernel's rows");
   grid = n_items;
   if (graph_exec) {
@@ -456,7 +460,8 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
     if (max_gf_far_blocks > 0 && step % kGfBlock == 0 &&
         (e2 = launch_gf_far(ep, max_gf_far_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
-    if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
+    if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, gf_reduce, ctx->stream)) !=
+        cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
     ep.phase = 2;
     if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)

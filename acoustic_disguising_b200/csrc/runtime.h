@@ -93,6 +93,7 @@ struct Batch {
   int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
   int max_gf_blocks = 0;     // (source, receiver split) blocks of the GF kernel
   int max_gf_far_blocks = 0; // (source tile, receiver split) blocks of the far-lag kernel
+  bool gf_reduce = false;    // some GF solve splits a source's receivers over blocks
   int per_step = 2;          // kernel launches per launch-step
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;
