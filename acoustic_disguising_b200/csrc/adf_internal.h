@@ -26,6 +26,7 @@ enum : int {
 // Steps per block of the in-loop GF extrapolation: lags older than the block
 // are summed once per block, the rest step by step.
 constexpr int kGfBlock = 32;
+constexpr int kGfRing = 64;  // input-history rows kept receiver-major (>= kGfBlock + 1)
 
 // GF map kinds, as ADF_GF_* in include/adfdtd.h
 enum : int { ADF_GF_PV_FROM_PIN_ = 0, ADF_GF_P_FROM_PIN_ = 1, ADF_GF_PV_FROM_PV_ = 2 };
@@ -75,11 +76,16 @@ struct SolveDev {
   double* gf_part;        // [n_out][gf_ks][2] partial sums of the split reduction
   double* gf_far;         // [n_out][gf_rs][kGfBlock][2] far-lag partials of the current
                           // block of steps, or NULL (the map is summed step by step)
+  const float* gf_near;   // [2][n_out][gf_nl][n_in] lags 0..gf_nl-1 of the two tensors,
+                          // receiver fastest (blocked kinds), or NULL
+  double* gf_ring;        // [kGfRing][n_in] the last input-history rows, row mod kGfRing
   double gf_z0;
   int gf_kind, gf_nt, gf_n1, gf_n2;
   int gf_nout, gf_nin;
   int gf_ks;              // receiver splits per driven source (per-step kernel)
   int gf_rs;              // receiver splits of the far-lag kernel, 0 = no blocking
+  int gf_nl;              // lags held in gf_near: min(kGfBlock, nt_gf)
+  int gf_pad_;
 };
 
 // work item: {solve index, y tile | x tile << 16, z0, z1}
@@ -108,6 +114,7 @@ cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_ns
                                   cudaStream_t s);
 // far-lag part of the in-loop GF extrapolation for the block of kGfBlock steps
 // that starts at launch-step p.step
+cudaError_t launch_gf_near_pack(const SolveDev& d, float* near, cudaStream_t s);
 cudaError_t launch_gf_far(const EpiParams& p, int max_blocks, int max_nsrc, cudaStream_t s);
 
 }  // namespace adf

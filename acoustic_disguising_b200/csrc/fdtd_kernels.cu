@@ -737,11 +737,36 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
     const int col = S.gf_irec[r];
     return ((double)S.rec[0][cur + col] - (double)S.vn_rec[cur + col] * S.gf_z0) / 2.0;
   };
+  double a = 0.0, b = 0.0;
+  if (S.gf_near) {
+    // blocked kinds (one block per source): lags 0..T-1 <= b from the
+    // near-lag copy and the history ring, both receiver-major, so every lag
+    // is one coalesced row of each; thread t sums receivers t, t+256, ...
+    // Block 0 files row it-1 into the history and the ring; the other rows
+    // come from earlier launches.
+    const int nl = S.gf_nl;
+    const float* g0 = S.gf_near + (long long)o * nl * nin;
+    const float* g1 = g0 + (long long)S.gf_nout * nl * nin;
+    for (int r = threadIdx.x; r < nin; r += blockDim.x) {
+      const double h0 = pin_now(r);
+      if (blockIdx.x == 0) {
+        S.gf_pin[(long long)r * nt + (it - 1)] = h0;
+        S.gf_ring[(long long)((it - 1) % kGfRing) * nin + r] = h0;
+      }
+      a = __fma_rn((double)g0[r], h0, a);
+      b = __fma_rn((double)g1[r], h0, b);
+#pragma unroll 4
+      for (int lag = 1; lag < T; ++lag) {
+        const double h = S.gf_ring[(long long)((it - 1 - lag) % kGfRing) * nin + r];
+        a = __fma_rn((double)g0[(long long)lag * nin + r], h, a);
+        b = __fma_rn((double)g1[(long long)lag * nin + r], h, b);
+      }
+    }
+  } else {
   if (blockIdx.x == 0 && kind != ADF_GF_PV_FROM_PV_)
     for (int r = threadIdx.x; r < nin; r += blockDim.x)
       S.gf_pin[(long long)r * nt + (it - 1)] = pin_now(r);
   const int rb = (int)((long long)nin * part / ks), re = (int)((long long)nin * (part + 1) / ks);
-  double a = 0.0, b = 0.0;
   // (r, tt) walk over this block's receivers, tt fastest: contiguous tensor
   // and pin reads, the index stepped instead of divided.  GF_U elements per
   // round: all their loads are issued before the first is accumulated, so
@@ -812,6 +837,7 @@ __global__ void __launch_bounds__(256, 4) adf_gf_extrapolate_kernel(const EpiPar
         }
       }
     }
+  }
   }
   __shared__ double red[2][8];
 #pragma unroll
@@ -997,6 +1023,32 @@ cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_ns
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !reduce) return e;
   adf_gf_reduce_kernel<<<dim3((max_nsrc + 127) / 128, p.n_solves), 128, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+// Copies lags 0..nl-1 of the two tensors of an input-history map into the
+// receiver-major near-lag layout [2][n_out][nl][n_in] (set-up, once per map).
+__global__ void adf_gf_near_pack_kernel(const float* t0, const float* t1, float* near, int kind,
+                                        int ngf, int n1, int nout, int nin, int nl) {
+  const long long per = (long long)nout * nl * nin;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * per;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / per);
+    long long q = i - k * per;
+    const int r = (int)(q % nin);
+    q /= nin;
+    const int lag = (int)(q % nl);
+    const int o = (int)(q / nl);
+    const long long g = kind == ADF_GF_PV_FROM_PIN_
+                            ? lag + (long long)ngf * (o + (long long)n1 * r)
+                            : lag + (long long)ngf * (r + (long long)n1 * o);
+    near[i] = (k == 0 ? t0 : t1)[g];
+  }
+}
+
+cudaError_t launch_gf_near_pack(const SolveDev& d, float* near, cudaStream_t s) {
+  adf_gf_near_pack_kernel<<<4 * 148, 256, 0, s>>>(d.gf_t[0], d.gf_t[1], near, d.gf_kind, d.gf_nt,
+                                                  d.gf_n1, d.gf_nout, d.gf_nin, d.gf_nl);
   return cudaGetLastError();
 }
 

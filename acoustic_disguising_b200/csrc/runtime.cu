@@ -924,9 +924,13 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   if (stop_step < start_step) return ADF_OK;
   cudaSetDevice(ctx->device);
   size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
-  if (use_gf)
+  if (use_gf) {
     need += (size_t)4 * ntens * gf->nt_gf * gf->n1 * gf->n2 + (size_t)8 * gf->n_rec * d->nt +
             (size_t)4 * (gf->n_src + gf->n_rec);
+    if (gf->kind != ADF_GF_PV_FROM_PV)  // near-lag copy and history ring of the blocked kinds
+      need += (size_t)4 * 2 * std::min<int64_t>(kGfBlock, gf->nt_gf) * gf->n1 * gf->n2 +
+              (size_t)8 * kGfRing * gf->n_rec;
+  }
   if (need > ctx->budget) return fail(ADF_E_BUDGET, "solve exceeds the context's HBM budget");
   auto s = std::make_unique<Solve>();
   const hm::Dom dom = to_dom(*d);
@@ -983,11 +987,22 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
       rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (2 * ctx->nsm + otiles - 1) / otiles));
       far = solve_dalloc<double>(*s, (size_t)gf->n_src * rs * kGfBlock * 2, rc);
     }
+    // the blocked kinds' per-step sum reads lags 0..kGfBlock-1 from a
+    // receiver-major copy and the recent history from a receiver-major ring
+    float* near = nullptr;
+    double* ring = nullptr;
+    const int nl = (int)std::min<int64_t>(kGfBlock, gf->nt_gf);
+    if (rs > 0 && !rc) {
+      near = solve_dalloc<float>(*s, (size_t)2 * nl * gf->n1 * gf->n2, rc);
+      if (!rc) ring = solve_dalloc<double>(*s, (size_t)kGfRing * gf->n_rec, rc);
+    }
     if (rc) return rc;
     sd.gf_part = part;
     sd.gf_ks = ks;
     sd.gf_far = far;
     sd.gf_rs = rs;
+    sd.gf_ring = ring;
+    sd.gf_nl = nl;
     std::vector<int> cs((size_t)gf->n_src), cr((size_t)gf->n_rec);
     for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
     for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
@@ -1004,6 +1019,12 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     sd.gf_nout = (int)gf->n_src;
     sd.gf_nin = (int)gf->n_rec;
     sd.flags |= SF_GF;
+    if (near) {
+      cudaError_t e = launch_gf_near_pack(sd, near, ctx->stream);
+      if (e != cudaSuccess)
+        return fail(ADF_E_DEVICE, std::string("GF pack launch failed: ") + cudaGetErrorString(e));
+      sd.gf_near = near;
+    }
     // pin rows recorded before start_step (a resumed run) from the host traces
     if (start_step > 1 && gf->kind != ADF_GF_PV_FROM_PV) {
       std::vector<double> h((size_t)gf->n_rec * d->nt, 0.0);

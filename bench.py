@@ -90,6 +90,8 @@ def parse():
                     help="server slot limit (0: HBM budget only)")
     ap.add_argument("--kh-only", action="store_true",
                     help="run only the KH section and print it (profiling runs)")
+    ap.add_argument("--gf-only", action="store_true",
+                    help="run only the in-loop GF section and print it (profiling runs)")
     return ap.parse_args()
 
 
@@ -579,6 +581,7 @@ def b200_arm(args):
     if world == 1 and not args.no_kh:
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
     if world == 1 and not args.no_gf:
+        gf_section(A, ctx, nt=40)  # warm-up: graphs, pool blocks
         extra["gf_map"] = gf_section(A, ctx)
     if world == 1 and not args.no_step512:
         extra["step512"] = step512_section(A, ctx)
@@ -653,12 +656,26 @@ def kh_only(args):
     return 0
 
 
+def gf_only(args):
+    import acoustic_disguising_b200 as A
+
+    if not os.path.exists(A.LIB_PATH):
+        A.build()
+    ctx = A.Context(0)
+    gf_section(A, ctx, nt=40)
+    print(json.dumps({"gf_map": gf_section(A, ctx)}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     if args.kh_only:
         return kh_only(args)
+    if args.gf_only:
+        return gf_only(args)
     return b200_arm(args)
 
 

@@ -105,6 +105,34 @@ def test_gf_map_matches_oracle(adf, oracle, ctx, kind, discard, tol, steps, nt_g
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["PVFromPin", "PFromPin"])
+def test_gf_map_resumed_run(adf, oracle, ctx, kind):
+    """A run stopped after step 45 and resumed at step 46 matches one
+    uninterrupted oracle run: the resumed call starts its 32-step blocks at
+    step 46 and takes the input history before it from the host traces."""
+    case = make_case(adf, oracle, 40, 36, 32, steps=100, npml=5, shape="sphere", seed=8,
+                     n_rec=40)
+    d, o, g, cp, mask, field = case
+    ts, isr, irc = gf_inputs(g.dir.shape[1], kind, nt_gf=40)
+    gg = to_adf_grid(adf, g)
+    pc = _Cp(adf, cp)
+    gm = adf.GfMap(kind, tuple(ts), isr, irc, False)
+    f_gpu = field.copy(order="F")
+    adf.run_fdtd(d, f_gpu, gg, pc, mask, stop_step=45, gf_map=gm)
+    adf.run_fdtd(d, f_gpu, gg, pc, mask, start_step=46, gf_map=gm)
+    f_cpu = field.copy(order="F")
+    go, co = g.copy(), cp.copy()
+    oracle.run_fdtd_gf(o, f_cpu, go, co, mask, kind, ts, isr, irc, o.z0, discard=False)
+    errs = assert_parity((f_gpu, gg, pc), (f_cpu, go, co), 1e-6)
+    assert errs["rec0"] <= 1e-6
+    for k in isr - 1:
+        a = gg.src[0][:, k].astype(np.float64)
+        b = go.src[0][:, k].astype(np.float64)
+        assert np.abs(b).max() > 0
+        assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b)
+
+
+@pytest.mark.gpu
 def test_gf_map_rejects_bad_indices(adf, oracle, ctx):
     case = make_case(adf, oracle, 24, 22, 20, steps=10, npml=4, shape="none", seed=1)
     d, o, g, cp, mask, field = case
