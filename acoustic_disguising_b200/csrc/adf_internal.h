@@ -79,6 +79,7 @@ struct SolveDev {
   const float* gf_near;   // [2][n_out][gf_nl][n_in] lags 0..gf_nl-1 of the two tensors,
                           // receiver fastest (blocked kinds), or NULL
   double* gf_ring;        // [kGfRing][n_in] the last input-history rows, row mod kGfRing
+  const int* gf_col;      // [ntx] 1 + the last driven source writing the column, 0: none
   double gf_z0;
   int gf_kind, gf_nt, gf_n1, gf_n2;
   int gf_nout, gf_nin;
@@ -100,7 +101,6 @@ struct EpiParams {
   SolveDev* solves;
   int n_solves;
   int step;
-  int phase;  // 0: records, v2vn and vn2v; solves with SF_GF: 1 records + v2vn, 2 vn2v
 };
 
 

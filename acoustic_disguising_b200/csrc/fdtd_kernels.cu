@@ -640,17 +640,6 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
   if (it > S.it_stop) return;
   const int ntx = S.ntx;
   const bool gf = (S.flags & SF_GF) != 0;
-  if (p.phase == 2) {  // vn2v! of a GF solve, after the extrapolation wrote vn_src[it+1]
-    if (!gf || !S.vn_src || it >= S.nt) return;
-    for (int tx = blockIdx.x * blockDim.x + threadIdx.x; tx < ntx; tx += gridDim.x * blockDim.x) {
-      const long long nr = (long long)it * ntx + tx;
-      const float* d = S.dir + 4 * tx;
-      const float vs = S.vn_src[nr];
-#pragma unroll
-      for (int c = 1; c <= 3; ++c) S.src[c][nr] = __fadd_rn(S.src[c][nr], __fmul_rn(vs, d[c]));
-    }
-    return;
-  }
   for (int tx = blockIdx.x * blockDim.x + threadIdx.x; tx < ntx; tx += gridDim.x * blockDim.x) {
     const long long row = (long long)(it - 1) * ntx + tx;
     float r[4];
@@ -669,7 +658,9 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
     const float* d = S.dir + 4 * tx;
     S.vn_rec[row] =
         __fadd_rn(__fadd_rn(__fmul_rn(r[1], d[1]), __fmul_rn(r[2], d[2])), __fmul_rn(r[3], d[3]));
-    if (S.vn_src && it < S.nt && !gf) {
+    // vn2v! into row it+1; a GF solve's driven columns get it when the
+    // extrapolation has written their vn_src (gf_finish)
+    if (S.vn_src && it < S.nt && (!gf || S.gf_col[tx] == 0)) {
       const long long nr = row + ntx;
       const float vs = S.vn_src[nr];
 #pragma unroll
@@ -681,8 +672,9 @@ __global__ void adf_fdtd_epilogue_kernel(const EpiParams p) {
 // Advances it_base of every solve by `by` steps: the last node of a captured
 // chunk of steps, so replaying the graph continues where it stopped.
 // Completes source o of step it from its summed lags: adds the far lags
-// summed at the block's start (block-causal kinds) and writes the p_src and
-// vn_src samples of row it+1 (extrapolation.jl:215-216, 228-229, 246-247).
+// summed at the block's start (block-causal kinds), writes the p_src and
+// vn_src samples of row it+1 (extrapolation.jl:215-216, 228-229, 246-247)
+// and applies vn2v! to the column.
 __device__ __forceinline__ void gf_finish(const SolveDev& S, int o, int it, int step, double sa,
                                           double sb) {
   if (S.gf_rs > 0) {
@@ -702,6 +694,12 @@ __device__ __forceinline__ void gf_finish(const SolveDev& S, int o, int it, int 
   }
   S.src[0][(long long)it * S.src_ntx + col] = vs;
   S.vn_src[(long long)it * S.ntx + col] = ps;
+  if (S.gf_col[col] == o + 1) {  // vn2v! of the column (derivatives.jl:92-97), once
+    const long long nr = (long long)it * S.ntx + col;
+    const float* d = S.dir + 4 * col;
+#pragma unroll
+    for (int c = 1; c <= 3; ++c) S.src[c][nr] = __fadd_rn(S.src[c][nr], __fmul_rn(ps, d[c]));
+  }
 }
 
 // In-loop GF extrapolation, extrapolate! (src/kernels/extrapolation.jl:204-249)

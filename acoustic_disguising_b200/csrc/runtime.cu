@@ -413,9 +413,9 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
   cudaStreamSynchronize(st);
-  // step + epilogue; GF solves add the extrapolation, its reduction when a
-  // source's receivers are split, and the vn2v! epilogue
-  per_step = max_gf_nsrc > 0 ? (gf_reduce ? 5 : 4) : 2;
+  // step + epilogue; GF solves add the extrapolation and its reduction when
+  // a source's receivers are split
+  per_step = max_gf_nsrc > 0 ? (gf_reduce ? 4 : 3) : 2;
   if (max_ty > step_max_ty()) return fail(ADF_E_ARG, "tile taller than the step kernel's rows");
   grid = n_items;
   if (graph_exec) {
@@ -451,7 +451,6 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
   ep.solves = d_solves;
   ep.n_solves = (int)solves.size();
   ep.step = step;
-  ep.phase = 0;
   cudaError_t e2;
   if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
     return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
@@ -463,9 +462,6 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
     if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, gf_reduce, ctx->stream)) !=
         cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
-    ep.phase = 2;
-    if ((e2 = launch_epilogue(ep, max_ntx, ctx->stream)) != cudaSuccess)
-      return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
   }
   return ADF_OK;
 }
@@ -926,7 +922,7 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
   if (use_gf) {
     need += (size_t)4 * ntens * gf->nt_gf * gf->n1 * gf->n2 + (size_t)8 * gf->n_rec * d->nt +
-            (size_t)4 * (gf->n_src + gf->n_rec);
+            (size_t)4 * (gf->n_src + gf->n_rec + txs->ntx);
     if (gf->kind != ADF_GF_PV_FROM_PV)  // near-lag copy and history ring of the blocked kinds
       need += (size_t)4 * 2 * std::min<int64_t>(kGfBlock, gf->nt_gf) * gf->n1 * gf->n2 +
               (size_t)8 * kGfRing * gf->n_rec;
@@ -967,6 +963,7 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
       sd.gf_t[k] = t;
     }
     int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_src, rc);
+    int* gcol = rc ? nullptr : solve_dalloc<int>(*s, (size_t)txs->ntx, rc);
     int* irec = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_rec, rc);
     double* pin = rc ? nullptr : solve_dalloc<double>(*s, (size_t)gf->n_rec * d->nt, rc);
     // receiver splits of the per-step kernel: about eight 256-thread blocks
@@ -1007,6 +1004,12 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
     for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
     cudaMemcpy(isrc, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice);
+    {  // driven columns: the last source writing each one applies its vn2v!
+      std::vector<int> col((size_t)txs->ntx, 0);
+      for (int64_t k = 0; k < gf->n_src; ++k) col[(size_t)cs[(size_t)k]] = (int)k + 1;
+      cudaMemcpy(gcol, col.data(), col.size() * 4, cudaMemcpyHostToDevice);
+      sd.gf_col = gcol;
+    }
     cudaMemcpy(irec, cr.data(), cr.size() * 4, cudaMemcpyHostToDevice);
     sd.gf_isrc = isrc;
     sd.gf_irec = irec;
