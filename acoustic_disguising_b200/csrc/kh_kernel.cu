@@ -18,7 +18,7 @@
 // Work decomposition (CUDA cores, FP32 FMA bound):
 //   CTA   = 16 targets x one block of 32*T output samples, 16 warps
 //   warp  = KH_RW targets (default 1); lane = T consecutive output samples
-//           of each (T odd, default 13)
+//           of each (T odd, default 17: 128 registers, no spills)
 //   loop  = surface points in chunks of SC.  One thread stages chunk c+1's
 //           input windows into shared memory with bulk async copies while
 //           the CTA works on chunk c (double buffer, mbarrier completion);
@@ -46,7 +46,7 @@ namespace adf {
 namespace {
 
 #ifndef KH_NT
-#define KH_NT 13
+#define KH_NT 17
 #endif
 #ifndef KH_NWARPS
 #define KH_NWARPS 16
