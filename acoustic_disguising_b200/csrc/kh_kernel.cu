@@ -18,7 +18,7 @@
 // Work decomposition (CUDA cores, FP32 FMA bound):
 //   CTA   = 16 targets x one block of 32*T output samples, 16 warps
 //   warp  = KH_RW targets (default 1); lane = T consecutive output samples
-//           of each (T odd, default 17: 128 registers, no spills)
+//           of each (T odd, default 17: 128 registers)
 //   loop  = surface points in chunks of SC.  One thread stages chunk c+1's
 //           input windows into shared memory with bulk async copies while
 //           the CTA works on chunk c (double buffer, mbarrier completion);
