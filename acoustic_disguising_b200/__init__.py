@@ -10,7 +10,7 @@ from .api import (  # noqa: F401
     split_profiles, Cpml, shape_params,
     build_update_mask, Transceiver, TransceiverGrid, transceivers_to_grid, p_src, p_rec, vn_src,
     vn_rec, run_fdtd, GfMap, PVFromPin, PFromPin, PVFromPV, injection_coefficients, kh_pressure, kh_velocity, gf_postprocess, gf_unit_factors, fp32_fma_peak, GfRequest,
-    gf_solve_batch, impulsive_gfs, autotune, Server,
+    gf_solve_batch, impulsive_gfs, autotune, Server, pinned_zeros,
 )
 
 __all__ = [n for n in dir() if not n.startswith("_")]

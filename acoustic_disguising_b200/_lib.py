@@ -128,6 +128,8 @@ SIGNATURES = [
     ("adf_last_io_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("adf_kernel_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                     C.c_int]),
+    ("adf_host_pin", C.c_int, [C.c_void_p, C.c_size_t]),
+    ("adf_host_unpin", C.c_int, [C.c_void_p]),
     ("adf_gf_solve_batch", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(GfRequestC), C.c_int]),
     ("adf_autotune", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int,
                                C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import threading
+import weakref
 from dataclasses import dataclass, field as dc_field
 
 import numpy as np
@@ -583,6 +584,17 @@ class GfRequest:
         r.out_p = self.p.ctypes.data
         r.out_vn = self.vn.ctypes.data
         return r
+
+
+def pinned_zeros(shape, dtype=np.float32, order: str = "F") -> np.ndarray:
+    """A zero-filled host array page-locked for the library's copies
+    (adf_host_pin), e.g. GfRequest.p / .vn buffers reused across
+    gf_solve_batch calls; it is unpinned when the array is collected."""
+    a = np.zeros(shape, dtype, order=order)
+    if a.nbytes:
+        L.check(L.lib().adf_host_pin(a.ctypes.data, a.nbytes), "host_pin")
+        weakref.finalize(a, L.lib().adf_host_unpin, a.ctypes.data)
+    return a
 
 
 def gf_solve_batch(reqs, batched: bool = True, ctx: Context | None = None):

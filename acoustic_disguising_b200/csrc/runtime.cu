@@ -1148,6 +1148,26 @@ int adf_set_kernel_timing(adf_ctx* ctx, int on) {
   return ADF_OK;
 }
 
+int adf_host_pin(void* ptr, size_t bytes) {
+  if (!ptr || !bytes) return fail(ADF_E_ARG, "adf_host_pin: empty buffer");
+  const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("adf_host_pin: ") + cudaGetErrorString(e));
+  }
+  return ADF_OK;
+}
+
+int adf_host_unpin(void* ptr) {
+  if (!ptr) return fail(ADF_E_ARG, "adf_host_unpin: NULL pointer");
+  const cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("adf_host_unpin: ") + cudaGetErrorString(e));
+  }
+  return ADF_OK;
+}
+
 int adf_last_io_bytes(adf_ctx* ctx, int64_t* h2d, int64_t* d2h) {
   if (!ctx) return fail(ADF_E_ARG, "NULL ctx");
   if (h2d) *h2d = ctx->h2d_bytes;

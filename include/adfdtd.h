@@ -215,6 +215,13 @@ int adf_set_kernel_timing(adf_ctx* ctx, int on);
 int adf_last_io_bytes(adf_ctx* ctx, int64_t* h2d, int64_t* d2h);
 int adf_kernel_timing(adf_ctx* ctx, double* step_kernel_ms, int64_t* step_launches, int reset);
 
+/* Page-locks (pins) a caller's host buffer so that later calls copy to and
+ * from it by DMA, without staging; adf_host_unpin releases it before the
+ * caller frees the memory.  No reference counterpart: a host-memory helper
+ * for callers that reuse their trace buffers across calls.                 */
+int adf_host_pin(void* ptr, size_t bytes);
+int adf_host_unpin(void* ptr);
+
 /* ---- Impulsive Green's-function solves (impulsive_gfs, src/greens.jl:48-234) ----
  * One request = one FDTD solve: a point source at `src_point` with
  * direction {q,fx,fy,fz} driven by `src_tf` (nt Float64), recording p and
