@@ -629,7 +629,9 @@ def b200_arm(args):
         "config": workload_config(B, world),
         "e2e": {"value": e2e, "unit": "solves/s",
                 "h2d_bytes_per_step": int(statistics.mean(h2ds)),
-                "d2h_bytes_per_step": int(statistics.mean(d2hs))},
+                "d2h_bytes_per_step": int(statistics.mean(d2hs)),
+                "wall_ms_per_step": [round(w * 1e3, 1) for w in walls],
+                "device_ms_per_step": [round(d, 1) for d in devs]},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_note,

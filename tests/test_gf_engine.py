@@ -88,6 +88,24 @@ def test_gf_batches_reuse_memory_without_carry_over(adf, ctx):
         assert np.array_equal(a.p, b.p) and np.array_equal(a.vn, b.vn)
 
 
+def test_gf_pinned_result_buffers(adf, ctx):
+    """Result traces written into caller-owned page-locked buffers
+    (pinned_zeros, reused by a second batch) equal those of fresh arrays."""
+    specs = [(36, 40, "sphere", 0), (40, 30, "none", 1)]
+    fresh = [make_req(adf, *s) for s in specs]
+    adf.gf_solve_batch(fresh, batched=True)
+    bufs = [(adf.pinned_zeros((r.dom.nt, 64)), adf.pinned_zeros((r.dom.nt, 64))) for r in fresh]
+    for _ in range(2):
+        reqs = [make_req(adf, *s) for s in specs]
+        for r, (p, vn) in zip(reqs, bufs):
+            p.fill(np.nan)
+            vn.fill(np.nan)
+            r.p, r.vn = p, vn
+        adf.gf_solve_batch(reqs, batched=True)
+        for a, r in zip(fresh, reqs):
+            assert r.p is not None and np.array_equal(a.p, r.p) and np.array_equal(a.vn, r.vn)
+
+
 def test_gf_budget_admission(adf, ctx):
     """A budget that fits about two solves forces waves of admission; results
     equal the unconstrained batch."""
