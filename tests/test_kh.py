@@ -87,6 +87,27 @@ def test_kh_monopole_dipole_split(adf, oracle, ctx):
 
 
 @pytest.mark.gpu
+def test_kh_into_caller_buffers(adf, oracle, ctx):
+    """kh_pressure / kh_velocity write into a caller's page-locked output
+    (reused twice, from pinned inputs) exactly what they return otherwise."""
+    c = case(64, 40, 700, 5e-6, 0.25, 0.9)
+    q, f = adf.pinned_zeros(c["q"].shape), adf.pinned_zeros(c["f"].shape)
+    q[:], f[:] = c["q"], c["f"]
+    rn = c["rp"] / np.linalg.norm(c["rp"], axis=1, keepdims=True)
+    for fn, extra in ((adf.kh_pressure, ()), (adf.kh_velocity, (rn,))):
+        args = (c["sp"], c["sn"], c["rp"], *extra)
+        fresh = fn(*args, c["q"], c["f"], c["dt"], c["sigma"], C0, c["aq"], c["af"], rho=RHO)
+        out = adf.pinned_zeros(fresh.shape)
+        for _ in range(2):
+            out.fill(np.nan)
+            got = fn(*args, q, f, c["dt"], c["sigma"], C0, c["aq"], c["af"], rho=RHO, out=out)
+            assert got is out and np.array_equal(out, fresh)
+    with pytest.raises(ValueError, match="out must be"):
+        adf.kh_pressure(c["sp"], c["sn"], c["rp"], q, f, c["dt"], c["sigma"], C0, c["aq"],
+                        c["af"], out=np.zeros((3, 3), np.float32))
+
+
+@pytest.mark.gpu
 def test_kh_rejects_bad_arguments(adf, ctx):
     c = case(16, 8, 64, 5e-6, 0.25, 1.0)
     with pytest.raises(adf.AdfError, match="at most 32"):
