@@ -1,7 +1,7 @@
 """Golden fixtures (tests/golden/*.npz, written by tests/golden/make_golden.py).
 
 CPU: the oracle still reproduces every fixture bit for bit, so a change to
-the oracle cannot silently move the reference the GPU is judged against.
+the oracle cannot silently move the reference the GPU is compared against.
 GPU: the CUDA path, fed the fixtures' stored inputs, reproduces their
 outputs: CPML profiles and masks bit-exact, fields and traces within 1e-6
 (promote) / 1e-5 (fp32) relative L2, KH within 1e-5 relative L2.
