@@ -18,7 +18,7 @@
 // Work decomposition (CUDA cores, FP32 FMA bound):
 //   CTA   = 16 targets x one block of 32*T output samples, 16 warps
 //   warp  = KH_RW targets (default 1); lane = T consecutive output samples
-//           of each (T odd, default 17: 128 registers)
+//           of each (T odd: 13 or 17, chosen per call by the padded cost)
 //   loop  = surface points in chunks of SC.  One thread stages chunk c+1's
 //           input windows into shared memory with bulk async copies while
 //           the CTA works on chunk c (double buffer, mbarrier completion);
@@ -45,9 +45,6 @@ namespace adf {
 
 namespace {
 
-#ifndef KH_NT
-#define KH_NT 17
-#endif
 #ifndef KH_NWARPS
 #define KH_NWARPS 16
 #endif
@@ -57,15 +54,25 @@ namespace {
 #ifndef KH_NG
 #define KH_NG 8
 #endif
-constexpr int KH_T = KH_NT;              // output samples per lane (odd)
 constexpr int KH_WARPS = KH_NWARPS;
 constexpr int KH_THREADS = 32 * KH_WARPS;
-constexpr int KH_TB = 32 * KH_T;         // output samples per CTA
 constexpr int KH_RW = KH_NRW;            // targets per warp
 constexpr int KH_G = KH_NG;              // surface points summed before each compensated add
 constexpr int KH_RT = KH_WARPS * KH_RW;  // targets per CTA
 constexpr int KH_SC_MAX = 32;            // surface points per staged chunk
-static_assert(KH_T % 2 == 1, "lanes must start an odd number of samples apart");
+// Output samples per lane, T, is a template parameter: 17 (128 registers)
+// costs about 8 % less per sample than 13 (112 registers) on long traces, but
+// its CTAs cover 544 samples against 416, so short traces pad more.  The
+// launcher takes the one with the smaller padded cost.
+constexpr int KH_T_LONG = 17, KH_T_SHORT = 13;
+constexpr double KH_T_LONG_COST = 0.917;  // per-sample cost of 17 relative to 13
+
+int kh_samples_per_lane(int nt) {
+  const double c17 = KH_T_LONG_COST * (double)((nt + 32 * KH_T_LONG - 1) / (32 * KH_T_LONG)) *
+                     (32 * KH_T_LONG);
+  const double c13 = (double)((nt + 32 * KH_T_SHORT - 1) / (32 * KH_T_SHORT)) * (32 * KH_T_SHORT);
+  return c17 < c13 ? KH_T_LONG : KH_T_SHORT;
+}
 
 struct KhParams {
   int ns, nr, nt;
@@ -99,14 +106,15 @@ struct KhParams {
 // (v_p on in_q, v_v on in_f); v_v's Gaussian-CDF term tends to a constant,
 // so beyond each pair's window it is that constant times the running sum of
 // in_f (staged as a third row per surface point).
-template <int LM, int KIND>
+template <int LM, int KIND, int T>
 __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams p) {
-  constexpr int XN = KH_T + LM - 1;
+  static_assert(T % 2 == 1, "lanes must start an odd number of samples apart");
+  constexpr int XN = T + LM - 1;
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t full[2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x;
-  const int tb = blockIdx.y * KH_TB;
+  const int tb = blockIdx.y * (32 * T);
   const int r_base = tile * KH_RT;
   const int2 lob = p.tile_lo[tile];
   const int lo_min = lob.x, lo_max = lob.y;
@@ -220,11 +228,11 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     }
   };
 
-  float sum[KH_RW][KH_T], comp[KH_RW][KH_T];
+  float sum[KH_RW][T], comp[KH_RW][T];
 #pragma unroll
   for (int r = 0; r < KH_RW; ++r)
 #pragma unroll
-    for (int j = 0; j < KH_T; ++j) sum[r][j] = comp[r][j] = 0.f;
+    for (int j = 0; j < T; ++j) sum[r][j] = comp[r][j] = 0.f;
 
   if (threadIdx.x == 0) stage(0);
   params(0);
@@ -249,11 +257,11 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     const float* pr_wb = pb + 2 * npair;
     const float* pr_c = pb + 3 * npair;
     // partial sums of up to KH_G surface points, then one compensated add
-    float2 c2[KH_RW][KH_T];
+    float2 c2[KH_RW][T];
 #pragma unroll
     for (int rho = 0; rho < KH_RW; ++rho)
 #pragma unroll
-      for (int j = 0; j < KH_T; ++j) c2[rho][j] = make_float2(0.f, 0.f);
+      for (int j = 0; j < T; ++j) c2[rho][j] = make_float2(0.f, 0.f);
     for (int sl = 0; ok && sl < nsc; ++sl) {
       // this point's {q, f} pairs from the first needed sample, and its
       // running-sum row
@@ -287,7 +295,7 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
 #pragma unroll
       for (int rho = 0; rho < KH_RW; ++rho) {
         const int pi = sl * KH_RT + warp * KH_RW + rho;
-        const int base = KH_T * lane + (lo_max - pr_lo[pi]);
+        const int base = T * lane + (lo_max - pr_lo[pi]);
         // {monopole, dipole} input pairs: one paired FMA per tap and sample
         float2 x2[XN];
 #pragma unroll
@@ -298,17 +306,17 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
           const float4 t4 = t4p[k2];
           const float2 ta = make_float2(t4.x, t4.y), tb2 = make_float2(t4.z, t4.w);
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j)
+          for (int j = 0; j < T; ++j)
             c2[rho][j] = __ffma2_rn(ta, x2[j + LM - 1 - 2 * k2], c2[rho][j]);
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j)
+          for (int j = 0; j < T; ++j)
             c2[rho][j] = __ffma2_rn(tb2, x2[j + LM - 2 - 2 * k2], c2[rho][j]);
         }
         if (KIND == 1) {  // lags past the window: v_v's constant times the running sum
           const float ped = pr_c[4 * npair + pi];
           const int cb = base + LM - 1 - pr_n[pi];
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j) c2[rho][j].y = __fmaf_rn(ped, wc[cb + j], c2[rho][j].y);
+          for (int j = 0; j < T; ++j) c2[rho][j].y = __fmaf_rn(ped, wc[cb + j], c2[rho][j].y);
         }
       }
       // compensated accumulation over groups of surface points
@@ -316,7 +324,7 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
 #pragma unroll
         for (int rho = 0; rho < KH_RW; ++rho)
 #pragma unroll
-          for (int j = 0; j < KH_T; ++j) {
+          for (int j = 0; j < T; ++j) {
             const float cj = __fadd_rn(c2[rho][j].x, c2[rho][j].y);
             const float y = __fsub_rn(cj, comp[rho][j]);
             const float t = __fadd_rn(sum[rho][j], y);
@@ -335,10 +343,10 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
   for (int rho = 0; rho < KH_RW; ++rho) {
     const int r = r_base + warp * KH_RW + rho;
     if (r >= p.nr) continue;
-    const int t0 = tb + KH_T * lane;
+    const int t0 = tb + T * lane;
     float* o = p.out + (size_t)r * p.nt + t0;
 #pragma unroll
-    for (int j = 0; j < KH_T; ++j)
+    for (int j = 0; j < T; ++j)
       if (t0 + j < p.nt) o[j] = sum[rho][j];
   }
 }
@@ -426,6 +434,7 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   }
   rs = rs * (1 + 1e-12) + 1e-12;
   const double inv_c0dt = 1.0 / (d->c0 * d->dt);
+  const int T = kh_samples_per_lane(nt), TB = 32 * T;  // output samples per lane, per CTA
   const int ntiles = (nr + KH_RT - 1) / KH_RT;
   std::vector<int2> tlo((size_t)ntiles);
   int wmax = 0, lo_all = 0;
@@ -443,7 +452,7 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
     int lo_max = (int)std::max(0.0, std::min(lmax, (double)nt + 1));
     lo_min = std::min(lo_min, lo_max);
     tlo[(size_t)t] = make_int2(lo_min, lo_max);
-    wmax = std::max(wmax, KH_TB + (lo_max - lo_min) + lm - 1);
+    wmax = std::max(wmax, TB + (lo_max - lo_min) + lm - 1);
     lo_all = std::max(lo_all, lo_max);
   }
   // multiple of 4 floats so the tap buffer behind the rows stays 16-B aligned
@@ -461,9 +470,9 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   // Input columns are zero-padded so that every staged window lies inside
   // its column: pad zeros before sample 0 cover the earliest window start,
   // the tail covers the last time block's window end.
-  const int nblk = (nt + KH_TB - 1) / KH_TB;
+  const int nblk = (nt + TB - 1) / TB;
   const int pad = (lo_all + lm + 4 + 3) / 4 * 4;
-  const long long pitch = ((long long)pad + (long long)nblk * KH_TB + lo_all + 16 + 3) / 4 * 4;
+  const long long pitch = ((long long)pad + (long long)nblk * TB + lo_all + 16 + 3) / 4 * 4;
   if (smem > smem_cap)
     return fail(ADF_E_ARG, "adf_kh_pressure: the targets' delay spread needs a " +
                                std::to_string(wmax) + "-sample window, more than shared memory holds");
@@ -533,22 +542,19 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   p.in_qf = dqf.p; p.cs_f = dc.p; p.out = dout.p;
   p.err = derr.p;
 
-  const void* fn = lm == 16 ? (kind ? (const void*)adf_kh_pressure_kernel<16, 1>
-                                    : (const void*)adf_kh_pressure_kernel<16, 0>)
-                            : (kind ? (const void*)adf_kh_pressure_kernel<32, 1>
-                                    : (const void*)adf_kh_pressure_kernel<32, 0>);
-  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the instantiation for (taps, kind, samples per lane)
+  using KhFn = void (*)(KhParams);
+  static const KhFn kfn[2][2][2] = {
+      {{adf_kh_pressure_kernel<16, 0, KH_T_SHORT>, adf_kh_pressure_kernel<16, 0, KH_T_LONG>},
+       {adf_kh_pressure_kernel<16, 1, KH_T_SHORT>, adf_kh_pressure_kernel<16, 1, KH_T_LONG>}},
+      {{adf_kh_pressure_kernel<32, 0, KH_T_SHORT>, adf_kh_pressure_kernel<32, 0, KH_T_LONG>},
+       {adf_kh_pressure_kernel<32, 1, KH_T_SHORT>, adf_kh_pressure_kernel<32, 1, KH_T_LONG>}}};
+  const KhFn fn = kfn[lm == 16 ? 0 : 1][kind ? 1 : 0][T == KH_T_LONG ? 1 : 0];
+  e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("kh smem: ") + cudaGetErrorString(e));
-  const dim3 grid((unsigned)ntiles, (unsigned)((nt + KH_TB - 1) / KH_TB));
+  const dim3 grid((unsigned)ntiles, (unsigned)((nt + TB - 1) / TB));
   cudaEventRecord(ctx->ev0, st);
-  if (lm == 16 && !kind)
-    adf_kh_pressure_kernel<16, 0><<<grid, KH_THREADS, smem, st>>>(p);
-  else if (lm == 16)
-    adf_kh_pressure_kernel<16, 1><<<grid, KH_THREADS, smem, st>>>(p);
-  else if (!kind)
-    adf_kh_pressure_kernel<32, 0><<<grid, KH_THREADS, smem, st>>>(p);
-  else
-    adf_kh_pressure_kernel<32, 1><<<grid, KH_THREADS, smem, st>>>(p);
+  fn<<<grid, KH_THREADS, smem, st>>>(p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("kh launch: ") + cudaGetErrorString(e));
   cudaEventRecord(ctx->ev1, st);
