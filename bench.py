@@ -640,6 +640,7 @@ def b200_arm(args):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_note,
+                     "frac_of_nominal_8000": achieved / 8000.0,
                      "traffic": (tpc * cells * B) if tpc else None,
                      "kernel": "adf_fdtd_step_kernel", "bytes_per_launch": bytes_launch,
                      "mean_launch_ms": k_avg_ms, "launches_timed": k_n},
