@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import mmap
 import threading
 import weakref
 from dataclasses import dataclass, field as dc_field
@@ -599,11 +600,20 @@ class GfRequest:
 def pinned_zeros(shape, dtype=np.float32, order: str = "F") -> np.ndarray:
     """A zero-filled host array page-locked for the library's copies
     (adf_host_pin), e.g. GfRequest.p / .vn buffers reused across
-    gf_solve_batch calls; it is unpinned when the array is collected."""
-    a = np.zeros(shape, dtype, order=order)
-    if a.nbytes:
-        L.check(L.lib().adf_host_pin(a.ctypes.data, a.nbytes), "host_pin")
-        weakref.finalize(a, L.lib().adf_host_unpin, a.ctypes.data)
+    gf_solve_batch calls; it is unpinned when the array is collected.  The
+    array has pages of its own (page-aligned start, whole pages), since
+    page-locking works on pages and two buffers sharing one could not both
+    be registered."""
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape, dtype=np.int64)) * dt.itemsize
+    page = mmap.PAGESIZE
+    span = max(page, (n + page - 1) // page * page)
+    raw = np.zeros(span + page, np.uint8)
+    off = (-raw.ctypes.data) % page
+    buf = raw[off:off + span]
+    a = np.ndarray(shape, dt, buffer=buf, order=order)
+    L.check(L.lib().adf_host_pin(buf.ctypes.data, span), "host_pin")
+    weakref.finalize(a, L.lib().adf_host_unpin, buf.ctypes.data)
     return a
 
 
