@@ -372,12 +372,23 @@ __global__ void __launch_bounds__(256) adf_fma_peak_kernel(float* out, int iters
 namespace {
 
 template <typename T>
-struct DevBuf {
+struct DevBuf {  // device scratch from the context's pool, freed in stream order
   T* p = nullptr;
+  cudaStream_t s = nullptr;
+  explicit DevBuf(const adf_ctx* ctx) : s(ctx->stream), pool(ctx->pool) {}
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s);
   }
-  bool alloc(size_t n) { return cudaMalloc(&p, n * sizeof(T)) == cudaSuccess; }
+  bool alloc(size_t n) {
+    if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), n * sizeof(T), pool, s) == cudaSuccess)
+      return true;
+    cudaGetLastError();
+    p = nullptr;
+    return false;
+  }
+
+ private:
+  cudaMemPool_t pool;
 };
 
 }  // namespace
@@ -477,10 +488,12 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
     return fail(ADF_E_ARG, "adf_kh_pressure: the targets' delay spread needs a " +
                                std::to_string(wmax) + "-sample window, more than shared memory holds");
 
-  DevBuf<double> dsp, dsn, drp, drn;
-  DevBuf<float> dq, df, dqf, dc, dout;
-  DevBuf<int2> dtlo;
-  DevBuf<int> derr;
+  // scratch from the context's pool: after the first call of a size the
+  // memory stays mapped and later calls take it without driver allocations
+  DevBuf<double> dsp(ctx), dsn(ctx), drp(ctx), drn(ctx);
+  DevBuf<float> dq(ctx), df(ctx), dqf(ctx), dc(ctx), dout(ctx);
+  DevBuf<int2> dtlo(ctx);
+  DevBuf<int> derr(ctx);
   if (!dsp.alloc((size_t)3 * ns) || !dsn.alloc((size_t)3 * ns) || !drp.alloc((size_t)3 * nr) ||
       !dq.alloc((size_t)pitch * ns) || !df.alloc((size_t)pitch * ns) ||
       !dqf.alloc((size_t)2 * pitch * ns) ||
@@ -590,7 +603,7 @@ extern "C" int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms_out) {
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
   const int blocks = ctx->nsm * 8, iters = 4096;
-  DevBuf<float> o;
+  DevBuf<float> o(ctx);
   if (!o.alloc((size_t)blocks)) return fail(ADF_E_NOMEM, "adf_fp32_fma_peak: allocation failed");
   adf_fma_peak_kernel<<<blocks, 256, 0, ctx->stream>>>(o.p, 64, 0.999f, 1e-4f);  // warm-up
   cudaEventRecord(ctx->ev0, ctx->stream);
