@@ -933,6 +933,10 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   int rc = solve_alloc(ctx, *s, dom, (int)npml, mask != nullptr, flags, (int)txs->ntx);
   if (!rc) rc = solve_alloc_traces(*s, true);
   if (rc) return rc;
+  // the zeroing above runs on the context stream (non-blocking); the uploads
+  // below are synchronous copies on the legacy stream, which does not wait
+  // for it
+  cudaStreamSynchronize(ctx->stream);
   SolveDev& sd = s->dev;
   // field -> buffer 0 (input of step start_step)
   cudaMemcpy2D(sd.field, (size_t)sd.nxp * 4, field, (size_t)d->nx * 4, (size_t)d->nx * 4,
