@@ -21,6 +21,12 @@ time step over all of their tiles, graph-captured), and the p / v_n traces copie
           2 m sphere: TFLOP/s of the KH kernel against the FP32 FMA peak
           measured in the same run, the C-ABI call's wall time, and the
           relative L2 error of a sample of targets against the FP64 oracle
+  gf_map : in-loop GF extrapolation (run_fdtd! on 128^3 with a PVFromPin
+          map of 256 lags x 256 sources x 256 receivers): device time per
+          step of the map's work (the run minus the same run with the map
+          discarded)
+  step512 : one 512^3 solve (12-cell CPML, rigid ellipsoid): the step
+          kernel's roofline on the largest single-solve grid
   serving : a Poisson stream of GF solves of mixed grid sizes (96..256^3),
           step counts (500..3000) and scatterers, offered at 1.5x the plain
           path's capacity: p50/p99 latency and solves/s of the continuous-
