@@ -76,6 +76,10 @@ __device__ __forceinline__ void cpml_apply(R& dv, float& m, float a, float b) {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// field stores: evict-first (the next step reads them back from HBM, and the
+// halo rows that neighbouring tiles re-read are loads, which keep normal
+// priority)
+__device__ __forceinline__ void stcs4(float* p, float4 v) { __stcs(reinterpret_cast<float4*>(p), v); }
 __device__ __forceinline__ float4 neg4(float4 v) { return make_float4(-v.x, -v.y, -v.z, -v.w); }
 
 template <typename R>
@@ -594,12 +598,12 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
       }
       if (vrow) {
         float* o = fout + k * plane + rowoff;
-        st4(o, Pn);
-        st4(o + cs, vx);
+        stcs4(o, Pn);
+        stcs4(o + cs, vx);
         // rigid mirrors (forward.jl:134-137): Vy[:,1,:] = -Vy[:,2,:], Vz[:,:,1] = -Vz[:,:,2]
-        if (j != 0) st4(o + 2 * cs, vy);
+        if (j != 0) stcs4(o + 2 * cs, vy);
         if (j == 1) st4(o + 2 * cs - nxp, neg4(vy));
-        if (k != 0) st4(o + 3 * cs, vz);
+        if (k != 0) stcs4(o + 3 * cs, vz);
         if (k == 1) st4(o + 3 * cs - plane, neg4(vz));
       }
     }
