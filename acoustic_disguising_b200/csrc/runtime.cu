@@ -919,6 +919,7 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   if (npml > 63) return fail(ADF_E_ARG, "npml > 63 is not supported");
   if (stop_step < start_step) return ADF_OK;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // the checks below see only this call's errors
   size_t need = solve_bytes_estimate(d->nx, d->ny, d->nz, npml, txs->ntx, d->nt, mask);
   if (use_gf) {
     need += (size_t)4 * ntens * gf->nt_gf * gf->n1 * gf->n2 + (size_t)8 * gf->n_rec * d->nt +
@@ -1048,6 +1049,10 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   const float* w[4] = {txs->w[0], txs->w[1], txs->w[2], txs->w[3]};
   rc = solve_finalize(ctx, *s, idx, w, nullptr);
   if (rc) return rc;
+  {  // the uploads above are synchronous copies: a failure is the last error
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("upload: ") + cudaGetErrorString(e));
+  }
   sd.it_first = (int)start_step;
   sd.it_base = (int)start_step;
   sd.it_stop = (int)stop_step;
@@ -1103,6 +1108,7 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   download_traces(*s, txs);
   if (use_gf) download_gf_sources(*s, txs);
   cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();  // a failed download
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
   return ADF_OK;
 }
@@ -1127,10 +1133,10 @@ int adf_read_field(adf_ctx* ctx, int chan, float* out) {
   if (!ctx->cur) return fail(ADF_E_STATE, "adf_read_field is only valid inside a step callback");
   const SolveDev& sd = ctx->cur->dev;
   const int fb = (int)((ctx->cur_it - sd.it_first + 1) & 1);
-  cudaMemcpy2D(out, (size_t)sd.nx * 4,
-               sd.field + (size_t)fb * sd.buf_stride + (size_t)chan * sd.chan_stride,
-               (size_t)sd.nxp * 4, (size_t)sd.nx * 4, (size_t)sd.ny * sd.nz,
-               cudaMemcpyDeviceToHost);
+  const cudaError_t e = cudaMemcpy2D(
+      out, (size_t)sd.nx * 4, sd.field + (size_t)fb * sd.buf_stride + (size_t)chan * sd.chan_stride,
+      (size_t)sd.nxp * 4, (size_t)sd.nx * 4, (size_t)sd.ny * sd.nz, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("adf_read_field: ") + cudaGetErrorString(e));
   return ADF_OK;
 }
 
