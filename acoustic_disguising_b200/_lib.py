@@ -146,6 +146,8 @@ SIGNATURES = [
     ("adf_kh_velocity", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("adf_kh_test_fault", C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    ("adf_static_cpml_max_npml", C.c_int, []),
     ("adf_gf_postprocess", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                      C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                      C.c_double, C.c_int]),

@@ -166,13 +166,15 @@ def cpml_profiles(npml: int, vel_max: float, dt: float, rcoef: float, thickness:
     return o32, o64
 
 
-STATIC_CPML_MAX_NPML = 63
+def static_cpml_max_npml() -> int:
+    """The largest npml cpml_profiles_static accepts (read from the library)."""
+    return int(L.lib().adf_static_cpml_max_npml())
 
 
 def cpml_profiles_static(npml: int, vel_max: float, dt: float, rcoef: float, thickness: float,
                          fc: float, ctx: Context | None = None):
     """cpml_profiles through adf_cpml_profiles_static: the same values, computed
-    with fixed device scratch (npml <= STATIC_CPML_MAX_NPML) and no device
+    with fixed device scratch (npml <= static_cpml_max_npml()) and no device
     allocation.  The first call per device sets the scratch up, so make it
     before any stream capture; concurrent calls on one device race."""
     ctx = ctx or default_context()
@@ -482,6 +484,15 @@ def kh_pressure(s_pts, s_nrm, r_pts, in_q, in_f, dt: float, sigma: float, c0: fl
     out = _kh_out(out, nt, nr, "kh_pressure")
     L.check(L.lib().adf_kh_pressure(ctx.h, C.byref(desc), _p(q), _p(f), _p(out)), "kh_pressure")
     return out
+
+
+def kh_test_fault(skip_chunk: int, poll_limit: int, ctx: Context | None = None) -> None:
+    """Arms the next kh_pressure / kh_velocity call on ctx (one shot): its
+    device waits give up after `poll_limit` polls and the copies of staged
+    chunk `skip_chunk` are never issued, so that chunk's wait runs out with
+    nothing in flight and the call raises ADF_E_TIMEOUT (a test hook)."""
+    ctx = ctx or default_context()
+    L.check(L.lib().adf_kh_test_fault(ctx.h, int(skip_chunk), int(poll_limit)), "kh_test_fault")
 
 
 def kh_velocity(s_pts, s_nrm, r_pts, r_nrm, in_q, in_f, dt: float, sigma: float, c0: float,

@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/adfdtd.h"
+
 namespace adf {
 
 // One thread per profile entry.  t in [0, 2n) ongrd (left then right),
@@ -294,11 +296,12 @@ cudaError_t launch_gf_postprocess(int ncol, int n, int nt_out, double t_in0, dou
 // npml <= kStaticCpmlMaxNpml (8*npml+4 values) in Float64 followed by Float32.
 // Nothing in it has to start at zero: the profile kernel writes every value
 // that the copies back to the host read.
-constexpr int kStaticCpmlMaxNpml = 63;
+constexpr int kStaticCpmlMaxNpml = ADF_STATIC_CPML_MAX_NPML;
 constexpr int kStaticCpmlMaxVals = 8 * kStaticCpmlMaxNpml + 4;
 static __device__ __align__(256) double g_cpml_scratch[kStaticCpmlMaxVals + kStaticCpmlMaxVals / 2 + 1];
 
 int static_cpml_max_npml() { return kStaticCpmlMaxNpml; }
+extern "C" int adf_static_cpml_max_npml(void) { return kStaticCpmlMaxNpml; }
 
 // Device address of the scratch on the current device.  Taking it is the one
 // set-up step (it may load this module onto the device), so callers do it

@@ -98,6 +98,8 @@ struct KhParams {
   const float* cs_f;    // running sum of in_f, same layout (velocity output)
   float* out;           // (nt, nr)
   int* err;
+  unsigned wait_limit;  // polls of a chunk's bounded wait (kWaitLimit)
+  int skip_chunk;       // test hook: chunk whose copies are not issued (-1: none)
 };
 
 }  // namespace
@@ -112,6 +114,7 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
   constexpr int XN = T + LM - 1;
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t full[2];
+  __shared__ int s_abort;  // a chunk's bounded wait gave up
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x;
   const int tb = blockIdx.y * (32 * T);
@@ -141,6 +144,7 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     mbar_init(smem_u32(&full[0]), 1);
     mbar_init(smem_u32(&full[1]), 1);
     fence_mbar_init();
+    s_abort = 0;
   }
   __syncthreads();
 
@@ -153,6 +157,9 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
     // the buffer's previous contents were read through the generic proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(mb, row_bytes * (uint32_t)NROW * (uint32_t)nsc);
+    // test hook: the bytes are expected but never arrive, so this chunk's
+    // wait runs out with no copy in flight
+    if (c == p.skip_chunk) return;
     float* w = smem + (c & 1) * wbuf;
     for (int sl = 0; sl < nsc; ++sl) {
       const size_t off = (size_t)(s0 + sl) * p.pitch;
@@ -238,15 +245,22 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
   params(0);
   __syncthreads();
   bool ok = true;
+  int failed = -1;  // chunk whose wait gave up (the same in every thread after a barrier)
   for (int c = 0; c < nchunks; ++c) {
+    // a wait of the previous chunk gave up: stage nothing more
+    if (s_abort) {
+      failed = c - 1;
+      break;
+    }
     // chunk c+1's buffers were last read in chunk c-1, which every thread
     // has finished (barrier at the end of the previous iteration)
     if (c + 1 < nchunks) {
       if (threadIdx.x == 0) stage(c + 1);
       params(c + 1);
     }
-    if (!mbar_wait(smem_u32(&full[c & 1]), (uint32_t)(c >> 1) & 1u)) {
-      if (threadIdx.x == 0) atomicOr(p.err, 2);
+    if (!mbar_wait(smem_u32(&full[c & 1]), (uint32_t)(c >> 1) & 1u, p.wait_limit)) {
+      atomicOr(p.err, 2);
+      s_abort = 1;  // read by every thread after the barrier below
       ok = false;
     }
     const int nsc = min(p.sc, p.ns - c * p.sc);
@@ -336,6 +350,17 @@ __global__ void __launch_bounds__(KH_THREADS, 1) adf_kh_pressure_kernel(KhParams
       __syncwarp();  // taps of the next surface point overwrite the buffer
     }
     __syncthreads();
+  }
+  if (failed < 0 && s_abort) failed = nchunks - 1;
+  if (failed >= 0) {
+    // The chunk after the failed one was staged before the failure: its
+    // copies write into this CTA's shared memory, so let them land (again a
+    // bounded wait) before the CTA exits.  No output is written; the host
+    // reports ADF_E_TIMEOUT.
+    const int c = failed + 1;
+    if (threadIdx.x == 0 && c < nchunks && c != p.skip_chunk)
+      mbar_wait(smem_u32(&full[c & 1]), (uint32_t)(c >> 1) & 1u);
+    return;
   }
 
   // outputs: lane owns samples tb + T*lane .. +T-1 of each of its targets
@@ -554,6 +579,11 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   p.tile_lo = dtlo.p;
   p.in_qf = dqf.p; p.cs_f = dc.p; p.out = dout.p;
   p.err = derr.p;
+  // the one-shot test hook of adf_kh_test_fault
+  p.wait_limit = ctx->kh_wait_limit ? ctx->kh_wait_limit : kWaitLimit;
+  p.skip_chunk = ctx->kh_skip_chunk;
+  ctx->kh_wait_limit = 0;
+  ctx->kh_skip_chunk = -1;
 
   // the instantiation for (taps, kind, samples per lane)
   using KhFn = void (*)(KhParams);
@@ -596,6 +626,14 @@ extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* 
 extern "C" int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q,
                                const float* in_f, float* out) {
   return kh_run(ctx, d, in_q, in_f, out, 1);
+}
+
+extern "C" int adf_kh_test_fault(adf_ctx* ctx, int skip_chunk, uint32_t poll_limit) {
+  if (!ctx || skip_chunk < -1 || poll_limit == 0)
+    return fail(ADF_E_ARG, "adf_kh_test_fault: skip_chunk >= -1 and poll_limit > 0");
+  ctx->kh_skip_chunk = skip_chunk;
+  ctx->kh_wait_limit = poll_limit;
+  return ADF_OK;
 }
 
 extern "C" int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms_out) {

@@ -35,8 +35,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
 // surfaces as an error code instead of a hung GPU.  try_wait itself suspends
 // the thread for a bounded, hardware-chosen interval, so the loop does not
 // spin hot and wakes as soon as the phase completes.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity,
+                                          uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(a, parity)) return true;
   return false;
 }

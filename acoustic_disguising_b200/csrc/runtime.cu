@@ -210,8 +210,11 @@ static int build_entries(Solve& s, const float* const idx[4], const float* const
   cudaMemcpyAsync(d_inb, inb.data(), inb.size(), cudaMemcpyHostToDevice, st);
   s.h2d += (int64_t)(off.size() * 4 + seg.size() * sizeof(int4) + ew.size() * 12 + inb.size());
   cudaMemsetAsync(d_contrib, 0, (size_t)4 * ntx * 8 * 4, st);
-  // the vectors must outlive the async copies
-  cudaStreamSynchronize(st);
+  // the vectors must outlive the async copies; a failed copy is sticky in
+  // the stream or the thread's last error
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("entry upload: ") + cudaGetErrorString(e));
   d.tp_off = d_off;
   d.seg = d_seg;
   d.ent_w = d_w;
@@ -602,13 +605,18 @@ static void transpose_to_julia(const float* dv, float* jl, int64_t nt, int64_t n
         for (int64_t x = x0; x < std::min(ntx, x0 + B); ++x) jl[t + nt * x] = dv[t * ntx + x];
 }
 
-static int upload_traces(Solve& s, const adf_txgrid* txs, cudaStream_t st) {
+// Uploads on stream `st`, so the kernels that follow on it are ordered after
+// them; the staging vector is reused only once its copy has completed.
+static cudaError_t upload_traces(Solve& s, const adf_txgrid* txs, cudaStream_t st) {
   SolveDev& d = s.dev;
   const int64_t nt = d.nt, ntx = d.ntx;
   std::vector<float> tmp((size_t)(nt * ntx));
+  cudaError_t e = cudaSuccess;
   auto up = [&](const float* jl, float* dst) {
+    if (e != cudaSuccess) return;
     transpose_to_dev_layout(jl, tmp.data(), nt, ntx);
-    cudaMemcpy(dst, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(dst, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   };
   for (int c = 0; c < 4; ++c) {
     up(txs->src[c], d.src[c]);
@@ -616,9 +624,9 @@ static int upload_traces(Solve& s, const adf_txgrid* txs, cudaStream_t st) {
   }
   up(txs->vn_src, d.vn_src);
   up(txs->vn_rec, d.vn_rec);
-  cudaMemcpy(s.dir_dev, txs->dir, (size_t)4 * ntx * 4, cudaMemcpyHostToDevice);
-  (void)st;
-  return ADF_OK;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s.dir_dev, txs->dir, (size_t)4 * ntx * 4, cudaMemcpyHostToDevice, st);
+  return e;
 }
 
 static int download_traces(Solve& s, adf_txgrid* txs) {
@@ -649,8 +657,11 @@ static int download_gf_sources(Solve& s, adf_txgrid* txs) {
   return ADF_OK;
 }
 
-// psi: Julia (npml,ny,nz,2) / (nx,npml,nz,2) / (nx,ny,npml,2) <-> device
-static void psi_copy(Solve& s, int axis, bool vside, float* host, bool upload, int buffer) {
+// psi: Julia (npml,ny,nz,2) / (nx,npml,nz,2) / (nx,ny,npml,2) <-> device.
+// Uploads are stream-ordered on `st`; downloads are synchronous copies taken
+// after the caller has synchronised the stream that wrote the memory.
+static cudaError_t psi_copy(Solve& s, int axis, bool vside, float* host, bool upload, int buffer,
+                            cudaStream_t st) {
   SolveDev& d = s.dev;
   const long long n = vside ? d.npml + 1 : d.npml;
   float* base = vside ? d.psi_v[axis] : d.psi_p[axis];
@@ -660,18 +671,17 @@ static void psi_copy(Solve& s, int axis, bool vside, float* host, bool upload, i
     const size_t pitch = (size_t)(vside ? d.nvp : d.npp) * 4;
     const size_t rows = (size_t)d.ny * d.nz * 2;
     if (upload)
-      cudaMemcpy2D(dev, pitch, host, (size_t)n * 4, (size_t)n * 4, rows, cudaMemcpyHostToDevice);
-    else
-      cudaMemcpy2D(host, (size_t)n * 4, dev, pitch, (size_t)n * 4, rows, cudaMemcpyDeviceToHost);
-    return;
+      return cudaMemcpy2DAsync(dev, pitch, host, (size_t)n * 4, (size_t)n * 4, rows,
+                               cudaMemcpyHostToDevice, st);
+    return cudaMemcpy2D(host, (size_t)n * 4, dev, pitch, (size_t)n * 4, rows,
+                        cudaMemcpyDeviceToHost);
   }
   const size_t rows = axis == 1 ? (size_t)n * d.nz * 2 : (size_t)d.ny * n * 2;
   if (upload)
-    cudaMemcpy2D(dev, (size_t)d.nxp * 4, host, (size_t)d.nx * 4, (size_t)d.nx * 4, rows,
-                 cudaMemcpyHostToDevice);
-  else
-    cudaMemcpy2D(host, (size_t)d.nx * 4, dev, (size_t)d.nxp * 4, (size_t)d.nx * 4, rows,
-                 cudaMemcpyDeviceToHost);
+    return cudaMemcpy2DAsync(dev, (size_t)d.nxp * 4, host, (size_t)d.nx * 4, (size_t)d.nx * 4,
+                             rows, cudaMemcpyHostToDevice, st);
+  return cudaMemcpy2D(host, (size_t)d.nx * 4, dev, (size_t)d.nxp * 4, (size_t)d.nx * 4, rows,
+                      cudaMemcpyDeviceToHost);
 }
 
 // ---------------------------------------------------------------------------
@@ -785,16 +795,24 @@ int adf_time_axis(const adf_domain* d, double* out) {
 int adf_cpml_profiles(adf_ctx* ctx, int64_t npml, double vel_max, double dt, double rcoef,
                       double thickness, double fc, float* out32, double* out64) {
   if (!ctx || npml < 0 || !out32) return fail(ADF_E_ARG, "bad cpml arguments");
-  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  cudaGetLastError();  // the checks below see only this call's errors
   const size_t n = (size_t)(8 * npml + 4);
   float* d32 = nullptr;
   double* d64 = nullptr;
-  if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&d64, n * 8) != cudaSuccess)
+  if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&d64, n * 8) != cudaSuccess) {
+    cudaFree(d32);  // whichever was allocated (cudaFree(nullptr) is a no-op)
+    cudaGetLastError();
     return fail(ADF_E_NOMEM, "cudaMalloc failed");
-  launch_cpml_profiles((int)npml, vel_max, dt, rcoef, thickness, fc, d32, d64, ctx->stream);
-  cudaMemcpyAsync(out32, d32, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
-  if (out64) cudaMemcpyAsync(out64, d64, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  }
+  e = launch_cpml_profiles((int)npml, vel_max, dt, rcoef, thickness, fc, d32, d64, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out32, d32, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && out64)
+    e = cudaMemcpyAsync(out64, d64, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  const cudaError_t es = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = es;
   cudaFree(d32);
   cudaFree(d64);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
@@ -819,6 +837,7 @@ int adf_cpml_profiles_static(adf_ctx* ctx, int64_t npml, double vel_max, double 
                                std::to_string(max_npml) + "); use adf_cpml_profiles");
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  cudaGetLastError();  // a leftover error of an earlier call is not this call's
   double* d64 = nullptr;
   float* d32 = nullptr;
   {
@@ -859,16 +878,19 @@ int adf_build_mask(adf_ctx* ctx, const adf_domain* d, int shape, const double* p
   if (!ctx || !d) return fail(ADF_E_ARG, "bad mask arguments");
   if (shape == ADF_SHAPE_NONE) return 1;
   if (shape < 0 || shape > 4) return fail(ADF_E_ARG, "unknown shape");
-  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  cudaGetLastError();
   uint32_t* bits = nullptr;
   uint8_t* jl = nullptr;
   const int mw = (int)(((d->nx + 7) / 8 + 3) / 4 * 4);
   int rc = build_mask_device(ctx, *d, shape, params, mw, &bits, out_bool ? &jl : nullptr);
   if (rc) return rc;
   if (out_bool)
-    cudaMemcpyAsync(out_bool, jl, (size_t)4 * d->nx * d->ny * d->nz, cudaMemcpyDeviceToHost,
-                    ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    e = cudaMemcpyAsync(out_bool, jl, (size_t)4 * d->nx * d->ny * d->nz, cudaMemcpyDeviceToHost,
+                        ctx->stream);
+  const cudaError_t es = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = es;
   cudaFree(bits);
   if (jl) cudaFree(jl);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
@@ -934,37 +956,45 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   int rc = solve_alloc(ctx, *s, dom, (int)npml, mask != nullptr, flags, (int)txs->ntx);
   if (!rc) rc = solve_alloc_traces(*s, true);
   if (rc) return rc;
-  // the zeroing above runs on the context stream (non-blocking); the uploads
-  // below are synchronous copies on the legacy stream, which does not wait
-  // for it
-  cudaStreamSynchronize(ctx->stream);
+  // Every upload below is a stream-ordered copy on the context stream: the
+  // zeroing above, the copies, the set-up kernels and the steps run in that
+  // order.  A pageable source is staged before cudaMemcpyAsync returns.
+  cudaStream_t st = ctx->stream;
   SolveDev& sd = s->dev;
+  cudaError_t ue = cudaSuccess;  // the first failed upload
+  auto up = [&](cudaError_t e) {
+    if (ue == cudaSuccess && e != cudaSuccess) ue = e;
+  };
   // field -> buffer 0 (input of step start_step)
-  cudaMemcpy2D(sd.field, (size_t)sd.nxp * 4, field, (size_t)d->nx * 4, (size_t)d->nx * 4,
-               (size_t)d->ny * d->nz * 4, cudaMemcpyHostToDevice);
+  up(cudaMemcpy2DAsync(sd.field, (size_t)sd.nxp * 4, field, (size_t)d->nx * 4, (size_t)d->nx * 4,
+                       (size_t)d->ny * d->nz * 4, cudaMemcpyHostToDevice, st));
   if (mask) {
     uint8_t* jl = nullptr;
     const size_t mb = (size_t)4 * d->nx * d->ny * d->nz;
-    if (cudaMalloc(&jl, mb) != cudaSuccess) return fail(ADF_E_NOMEM, "mask staging alloc failed");
-    cudaMemcpy(jl, mask, mb, cudaMemcpyHostToDevice);
-    launch_pack_mask(jl, sd.nx, sd.ny, sd.nz, sd.mw, s->mask_bits, ctx->stream);
-    cudaStreamSynchronize(ctx->stream);
+    if (cudaMalloc(&jl, mb) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADF_E_NOMEM, "mask staging alloc failed");
+    }
+    up(cudaMemcpyAsync(jl, mask, mb, cudaMemcpyHostToDevice, st));
+    up(launch_pack_mask(jl, sd.nx, sd.ny, sd.nz, sd.mw, s->mask_bits, st));
+    up(cudaStreamSynchronize(st));
     cudaFree(jl);
   }
   if (npml > 0) {
-    cudaMemcpy(s->coef_dev, cpml->coef, (size_t)(8 * npml + 4) * 4, cudaMemcpyHostToDevice);
+    up(cudaMemcpyAsync(s->coef_dev, cpml->coef, (size_t)(8 * npml + 4) * 4,
+                       cudaMemcpyHostToDevice, st));
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 2; ++b) {
-        if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], true, b);
-        if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], true, b);
+        if (cpml->mv[a]) up(psi_copy(*s, a, false, cpml->mv[a], true, b, st));
+        if (cpml->mp[a]) up(psi_copy(*s, a, true, cpml->mp[a], true, b, st));
       }
   }
-  upload_traces(*s, txs, ctx->stream);
+  up(upload_traces(*s, txs, st));
   if (use_gf) {  // GF tensors, 0-based columns, Float64 pin history
     const size_t ng = (size_t)gf->nt_gf * gf->n1 * gf->n2;
     for (int k = 0; k < ntens && !rc; ++k) {
       float* t = solve_dalloc<float>(*s, ng, rc);
-      if (!rc) cudaMemcpy(t, gf->t[k], ng * 4, cudaMemcpyHostToDevice);
+      if (!rc) up(cudaMemcpyAsync(t, gf->t[k], ng * 4, cudaMemcpyHostToDevice, st));
       sd.gf_t[k] = t;
     }
     int* isrc = rc ? nullptr : solve_dalloc<int>(*s, (size_t)gf->n_src, rc);
@@ -1008,14 +1038,15 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     std::vector<int> cs((size_t)gf->n_src), cr((size_t)gf->n_rec);
     for (int64_t k = 0; k < gf->n_src; ++k) cs[(size_t)k] = (int)(gf->i_src[k] - 1);
     for (int64_t k = 0; k < gf->n_rec; ++k) cr[(size_t)k] = (int)(gf->i_rec[k] - 1);
-    cudaMemcpy(isrc, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice);
+    up(cudaMemcpyAsync(isrc, cs.data(), cs.size() * 4, cudaMemcpyHostToDevice, st));
     {  // driven columns: the last source writing each one applies its vn2v!
       std::vector<int> col((size_t)txs->ntx, 0);
       for (int64_t k = 0; k < gf->n_src; ++k) col[(size_t)cs[(size_t)k]] = (int)k + 1;
-      cudaMemcpy(gcol, col.data(), col.size() * 4, cudaMemcpyHostToDevice);
+      up(cudaMemcpyAsync(gcol, col.data(), col.size() * 4, cudaMemcpyHostToDevice, st));
+      up(cudaStreamSynchronize(st));  // before `col` goes out of scope
       sd.gf_col = gcol;
     }
-    cudaMemcpy(irec, cr.data(), cr.size() * 4, cudaMemcpyHostToDevice);
+    up(cudaMemcpyAsync(irec, cr.data(), cr.size() * 4, cudaMemcpyHostToDevice, st));
     sd.gf_isrc = isrc;
     sd.gf_irec = irec;
     sd.gf_pin = pin;
@@ -1042,17 +1073,20 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
           h[(size_t)(r * d->nt + t)] =
               ((double)txs->rec[0][o] - (double)txs->vn_rec[o] * gf->z0) / 2.0;
         }
-      cudaMemcpy(pin, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+      up(cudaMemcpyAsync(pin, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
+      up(cudaStreamSynchronize(st));  // before `h` goes out of scope
     }
+    up(cudaStreamSynchronize(st));  // before `cs` and `cr` go out of scope
   }
   const float* idx[4] = {txs->idx[0], txs->idx[1], txs->idx[2], txs->idx[3]};
   const float* w[4] = {txs->w[0], txs->w[1], txs->w[2], txs->w[3]};
+  up(cudaStreamSynchronize(st));
+  if (ue != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("upload: ") + cudaGetErrorString(ue));
+  }
   rc = solve_finalize(ctx, *s, idx, w, nullptr);
   if (rc) return rc;
-  {  // the uploads above are synchronous copies: a failure is the last error
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("upload: ") + cudaGetErrorString(e));
-  }
   sd.it_first = (int)start_step;
   sd.it_base = (int)start_step;
   sd.it_stop = (int)stop_step;
@@ -1102,8 +1136,8 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
                cudaMemcpyDeviceToHost);
   if (npml > 0)
     for (int a = 0; a < 3; ++a) {
-      if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], false, fb);
-      if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], false, fb);
+      if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], false, fb, st);
+      if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], false, fb, st);
     }
   download_traces(*s, txs);
   if (use_gf) download_gf_sources(*s, txs);

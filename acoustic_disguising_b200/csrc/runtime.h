@@ -31,6 +31,9 @@ struct adf_ctx {
   // per-launch timing of the step kernel
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // traffic of the last call
   bool kernel_timing = false;
+  // one-shot test hook of the next KH call (adf_kh_test_fault)
+  int kh_skip_chunk = -1;
+  uint32_t kh_wait_limit = 0;
   std::vector<cudaEvent_t> kev;  // 2 per launch-step of a chunk
   double kernel_ms = 0.0;
   int64_t kernel_launches = 0;

@@ -146,13 +146,17 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
   std::vector<float> sv(4 * nt);
   for (int c = 0; c < 4; ++c)
     for (size_t t = 0; t < nt; ++t) sv[c * nt + t] = (float)(r.src_tf[t] * r.src_dir[c]);
-  cudaMemcpyAsync(srcs, sv.data(), sv.size() * 4, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(dir, dirs.data(), dirs.size() * 4, cudaMemcpyHostToDevice, st);
+  cudaError_t ue = cudaSuccess;  // the first failed set-up copy or launch
+  auto up = [&](cudaError_t e) {
+    if (ue == cudaSuccess && e != cudaSuccess) ue = e;
+  };
+  up(cudaMemcpyAsync(srcs, sv.data(), sv.size() * 4, cudaMemcpyHostToDevice, st));
+  up(cudaMemcpyAsync(dir, dirs.data(), dirs.size() * 4, cudaMemcpyHostToDevice, st));
   s->h2d += (int64_t)(sv.size() * 4 + dirs.size() * 4);
   // CPML profiles in FP64 on the device: Cpml(dom; npml, rcoef, fc)
   if (r.npml > 0)
-    launch_cpml_profiles((int)r.npml, dd.c0, dd.dt, r.pml_rcoef, dd.dx * (double)r.npml,
-                         r.pml_fc, s->coef_dev, nullptr, st);
+    up(launch_cpml_profiles((int)r.npml, dd.c0, dd.dt, r.pml_rcoef, dd.dx * (double)r.npml,
+                            r.pml_fc, s->coef_dev, nullptr, st));
   // scatterer mask straight into the bitmask
   double* xyz = nullptr;
   if (has_mask) {
@@ -164,10 +168,11 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
     }
     if (cudaMallocFromPoolAsync((void**)&xyz, c.size() * 8, ctx->pool, st) != cudaSuccess)
       return fail(ADF_E_NOMEM, "alloc");
-    cudaMemcpyAsync(xyz, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st);
+    up(cudaMemcpyAsync(xyz, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st));
     s->h2d += (int64_t)(c.size() * 8);
-    launch_mask(r.shape, r.shape_params, xyz, xyz + dd.nx, xyz + dd.nx + dd.ny, (int)dd.nx,
-                (int)dd.ny, (int)dd.nz, d.mw, s->mask_bits, nullptr, st);
+    up(launch_mask(r.shape, r.shape_params, xyz, xyz + dd.nx, xyz + dd.nx + dd.ny, (int)dd.nx,
+                   (int)dd.ny, (int)dd.nz, d.mw, s->mask_bits, nullptr, st));
+    up(cudaStreamSynchronize(st));  // before `c` goes out of scope
     cudaFreeAsync(xyz, st);
   }
   std::vector<int> col(ntx, -1);
@@ -176,6 +181,11 @@ static int gf_setup(adf_ctx* ctx, GfJob& j) {
   const float* wp[4] = {w[0].data(), w[1].data(), w[2].data(), w[3].data()};
   rc = solve_finalize(ctx, *s, ip, wp, col.data());
   if (rc) return rc;
+  up(cudaStreamSynchronize(st));  // sv and dirs outlive their copies
+  if (ue != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("GF set-up: ") + cudaGetErrorString(ue));
+  }
   ctx->h2d_bytes += s->h2d;
   d.it_first = 1;
   d.it_base = 1;

@@ -36,12 +36,24 @@ int build_mask_device(adf_ctx* ctx, const adf_domain& d, int shape, const double
     cudaFree(*bits);
     return fail(ADF_E_NOMEM, "alloc");
   }
-  cudaMemcpyAsync(dxyz, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-  launch_mask(shape, params, dxyz, dxyz + d.nx, dxyz + d.nx + d.ny, (int)d.nx, (int)d.ny,
-              (int)d.nz, mw, *bits, jl ? *jl : nullptr, ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e =
+      cudaMemcpyAsync(dxyz, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = launch_mask(shape, params, dxyz, dxyz + d.nx, dxyz + d.nx + d.ny, (int)d.nx, (int)d.ny,
+                    (int)d.nz, mw, *bits, jl ? *jl : nullptr, ctx->stream);
+  const cudaError_t es = cudaStreamSynchronize(ctx->stream);  // xyz outlives its copy
+  if (e == cudaSuccess) e = es;
   cudaFree(dxyz);
-  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaFree(*bits);
+    *bits = nullptr;
+    if (jl) {
+      cudaFree(*jl);
+      *jl = nullptr;
+    }
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  }
   return ADF_OK;
 }
 

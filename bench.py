@@ -31,6 +31,9 @@ time step over all of their tiles, graph-captured), and the p / v_n traces copie
           step counts (500..3000) and scatterers, offered at 1.5x the plain
           path's capacity: p50/p99 latency and solves/s of the continuous-
           batching server against the plain one-solve-at-a-time path
+  parity : the first solve of the workload over its first 200 steps against
+          the oracle in the same arithmetic and against the oracle's FP64 run
+          (relative L2 of the p and v_n traces), outside the timed region
 
 `--impl reference` times the CPU restatement of the reference's Threads
 path (oracle/) on this host's cores on a bounded sample of the same solve.
@@ -92,6 +95,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-step512", action="store_true", help="skip the 512^3 step section")
     ap.add_argument("--no-gf", action="store_true", help="skip the in-loop GF section")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity section")
     ap.add_argument("--serving-requests", type=int, default=20)
     ap.add_argument("--serving-resident", type=int, default=2,
                     help="server slot limit (0: HBM budget only)")
@@ -232,6 +236,40 @@ def cpu_sample(steps, threads):
     O.run_fdtd(d, f, g, cp, m, start_step=2, stop_step=1 + steps, nthreads=threads)
     sec = time.perf_counter() - t0
     return sec / steps
+
+
+def parity_section(A, ctx, steps=200, arith="promote"):
+    """The headline workload's first solve (256^3, sphere, 2048-point shell)
+    over its first `steps` steps through the C-ABI, against the oracle in the
+    same arithmetic (the 1e-5 bar) and against the oracle's FP64 run (the
+    stated error).  Runs outside the timed region."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+
+    O.build()
+    _, reqs = make_requests(A, 0, 1, arith, steps)
+    req = reqs[0]
+    A.gf_solve_batch([req], batched=True, ctx=ctx)
+    d = O.domain(tmax=tmax_of(steps), xmax=(N - 1) * DX / 2, nx=N, c0=C0, r0=RHO, cf=0.5)
+    pts = np.vstack([req.src_point, req.rec_points])
+    dirs = np.vstack([[1.0, 0, 0, 0], np.hstack([np.zeros((N_REC, 1)), req.rec_normals])])
+    tfs = np.vstack([req.src_tf, np.zeros((N_REC, steps))])
+    m = O.build_update_mask(d, "sphere", radius=R_SPHERE)
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+    g = O.transceivers_to_grid(d, pts, dirs, tfs)
+    f = np.zeros((N, N, N, 4), np.float32, order="F")
+    O.run_fdtd(d, f, g, O.CpmlState(d, NPML, 1e-4, PML_FC), m, mode=arith)
+    del f
+    same = {"p": rel(req.p, g.rec[0][:, 1:]), "vn": rel(req.vn, g.vn_rec[:, 1:])}
+    g64 = O.transceivers_to_grid64(d, pts, dirs, tfs)
+    f64 = np.zeros((N, N, N, 4), np.float64, order="F")
+    O.run_fdtd64(d, f64, g64, O.CpmlState64(d, NPML, 1e-4, PML_FC), m)
+    del f64
+    fp64 = {"p": rel(req.p, g64.rec[0][:, 1:]), "vn": rel(req.vn, g64.vn_rec[:, 1:])}
+    return {"workload": f"source 0 of the headline workload, first {steps} of its {NT} steps, "
+                        "p and v_n traces of the 2048-point shell",
+            f"rel_l2_vs_{arith}_oracle": same, "rel_l2_vs_fp64_oracle": fp64,
+            "tolerance": 1e-5, "pass": max(same.values()) <= 1e-5}
 
 
 def reference_arm(args):
@@ -606,6 +644,8 @@ def b200_arm(args):
     if world == 1 and not args.no_serving:
         extra["serving"] = serving_section(A, ctx, args.serving_requests,
                                            args.serving_resident)
+    if world == 1 and not args.no_parity:
+        extra["parity"] = parity_section(A, ctx, arith=args.arith)
     dev_total = reduce_max(sum(devs), dist, f"cuda:{local}")
     wall_total = reduce_max(sum(walls), dist, f"cuda:{local}")
     k_avg_ms = reduce_max(k_ms / max(k_n, 1), dist, f"cuda:{local}")
@@ -648,6 +688,10 @@ def b200_arm(args):
                      "frac": achieved / peak, "peak_source": peak_note,
                      "frac_of_nominal_8000": achieved / 8000.0,
                      "traffic": (tpc * cells * B) if tpc else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                       "cell-step of a one-launch capture of this kernel "
+                                       "(profiles/fdtd_step_256cube.md), scaled to this "
+                                       "launch's cells" if tpc else None,
                      "kernel": "adf_fdtd_step_kernel", "bytes_per_launch": bytes_launch,
                      "mean_launch_ms": k_avg_ms, "launches_timed": k_n},
         "gcell_upd_per_s": cells * NT * solves / (dev_total / 1e3) / 1e9,

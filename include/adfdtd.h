@@ -136,6 +136,10 @@ int adf_cpml_profiles(adf_ctx* ctx, int64_t npml, double vel_max, double dt, dou
 int adf_cpml_profiles_static(adf_ctx* ctx, int64_t npml, double vel_max, double dt,
                              double rcoef, double thickness, double fc, float* out32,
                              double* out64);
+/* The largest npml adf_cpml_profiles_static accepts, for callers that
+ * cannot read the macro (ccall, ctypes).  Always ADF_STATIC_CPML_MAX_NPML. */
+#define ADF_STATIC_CPML_MAX_NPML 63
+int adf_static_cpml_max_npml(void);
 
 /* build_update_mask (src/geometry.jl:250-280), evaluated on the GPU.
  * out_bool: (nx,ny,nz,4) uint8 Julia layout, or NULL.  Returns 1 (writing
@@ -314,6 +318,15 @@ int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
  * roofline denominator of adf_kh_pressure.  Measurement helper with no
  * reference counterpart; ms (optional) receives the probe's duration.      */
 int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms);
+
+/* Test hook with no reference counterpart: arms the next adf_kh_pressure /
+ * adf_kh_velocity call on ctx (one shot) so that its bounded waits give up
+ * after poll_limit polls and the bulk copies of staged chunk skip_chunk
+ * (0-based; -1 none) are never issued.  Nothing is then in flight when that
+ * chunk's wait runs out: the call returns ADF_E_TIMEOUT with the context
+ * still usable, which is how a test shows that a device wait ends in an
+ * error code instead of a hang.                                           */
+int adf_kh_test_fault(adf_ctx* ctx, int skip_chunk, uint32_t poll_limit);
 
 /* impulsive_gfs post-processing of recorded GF traces (src/greens.jl:174-190,
  * src/resample.jl:32-76, src/greens_io.jl:195-205), on the GPU, per column

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -359,10 +360,13 @@ struct Scal {
   R fq, fv, dx, dy, dz;
 };
 
-struct View {
+// Field view over storage S: float (the reference's Float32 arrays) or
+// double (the FP64 error-statement run, every array in Float64).
+template <typename S>
+struct ViewT {
   int64_t nx, ny, nz;
-  float* f;
-  inline float& P(int64_t i, int64_t j, int64_t k) { return f[idx(i, j, k, 0)]; }
+  S* f;
+  inline S& P(int64_t i, int64_t j, int64_t k) { return f[idx(i, j, k, 0)]; }
   inline int64_t idx(int64_t i, int64_t j, int64_t k, int c) const {
     return (i - 1) + nx * ((j - 1) + ny * ((k - 1) + nz * (int64_t)c));
   }
@@ -370,83 +374,84 @@ struct View {
 
 // update_p! (updates.jl:105-142) for one cell, used on the rigid planes and
 // on the npml==0 unmasked interior
-template <typename R>
-inline void update_p_plain(View& v, const Scal<R>& s, int64_t i, int64_t j, int64_t k) {
-  float* f = v.f;
+template <typename R, typename S>
+inline void update_p_plain(ViewT<S>& v, const Scal<R>& s, int64_t i, int64_t j, int64_t k) {
+  S* f = v.f;
+  const S m2 = -2;
   R dvx, dvy, dvz;
   if (i == v.nx)
-    dvx = (R)(-2.0f * f[v.idx(i, j, k, 1)]) / s.dx;
+    dvx = (R)(m2 * f[v.idx(i, j, k, 1)]) / s.dx;
   else
     dvx = (R)(f[v.idx(i + 1, j, k, 1)] - f[v.idx(i, j, k, 1)]) / s.dx;
   if (j == v.ny)
-    dvy = (R)(-2.0f * f[v.idx(i, j, k, 2)]) / s.dy;
+    dvy = (R)(m2 * f[v.idx(i, j, k, 2)]) / s.dy;
   else
     dvy = (R)(f[v.idx(i, j + 1, k, 2)] - f[v.idx(i, j, k, 2)]) / s.dy;
   if (k == v.nz)
-    dvz = (R)(-2.0f * f[v.idx(i, j, k, 3)]) / s.dz;
+    dvz = (R)(m2 * f[v.idx(i, j, k, 3)]) / s.dz;
   else
     dvz = (R)(f[v.idx(i, j, k + 1, 3)] - f[v.idx(i, j, k, 3)]) / s.dz;
-  float& P = f[v.idx(i, j, k, 0)];
-  P = (float)((R)P - s.fq * (dvx + dvy + dvz));
+  S& P = f[v.idx(i, j, k, 0)];
+  P = (S)((R)P - s.fq * (dvx + dvy + dvz));
 }
 
 // CPML memory update `m = b*m + a*d; d += m` (updates.jl:46-61).  b*m is a
 // Float32 product; a*d promotes to R.
-template <typename R>
-inline void cpml_apply(R& dv, float* m, float a, float b) {
-  float bm = b * (*m);
+template <typename R, typename S>
+inline void cpml_apply(R& dv, S* m, S a, S b) {
+  S bm = b * (*m);
   R nm = (R)bm + (R)a * dv;
-  *m = (float)nm;
+  *m = (S)nm;
   dv = dv + (R)(*m);
 }
 
 // update_p_cpml! (updates.jl:21-103) / update_p_cpml_mask! (:320-378) /
 // update_p_mask! (:288-318) for one interior cell
-template <typename R>
-inline void update_p_interior(View& v, const Scal<R>& s, or_cpml* cp, const uint8_t* mask,
+template <typename R, typename S, typename CP>
+inline void update_p_interior(ViewT<S>& v, const Scal<R>& s, CP* cp, const uint8_t* mask,
                               bool guard, int64_t i, int64_t j, int64_t k) {
-  float* f = v.f;
+  S* f = v.f;
   const int64_t nx = v.nx, ny = v.ny, nz = v.nz;
   R dvx = (R)(f[v.idx(i + 1, j, k, 1)] - f[v.idx(i, j, k, 1)]) / s.dx;
   R dvy = (R)(f[v.idx(i, j + 1, k, 2)] - f[v.idx(i, j, k, 2)]) / s.dy;
   R dvz = (R)(f[v.idx(i, j, k + 1, 3)] - f[v.idx(i, j, k, 3)]) / s.dz;
   const int64_t npml = cp ? cp->npml : 0;
   if (cp && npml > 0 && (!guard || npml > 1)) {
-    const float* co = cp->coef;
-    const float* A[2] = {co, co + npml};
-    const float* B[2] = {co + 4 * npml + 2, co + 5 * npml + 2};
+    const S* co = cp->coef;
+    const S* A[2] = {co, co + npml};
+    const S* B[2] = {co + 4 * npml + 2, co + 5 * npml + 2};
     int64_t l;
     int side;
     boundary_index(i, nx, npml, l, side);
     if (side > 0) {
-      float* m = cp->mv[0] + (l - 1) + npml * ((j - 1) + ny * ((k - 1) + nz * (side - 1)));
+      S* m = cp->mv[0] + (l - 1) + npml * ((j - 1) + ny * ((k - 1) + nz * (side - 1)));
       cpml_apply(dvx, m, A[side - 1][l - 1], B[side - 1][l - 1]);
     }
     boundary_index(j, ny, npml, l, side);
     if (side > 0) {
-      float* m = cp->mv[1] + (i - 1) + nx * ((l - 1) + npml * ((k - 1) + nz * (side - 1)));
+      S* m = cp->mv[1] + (i - 1) + nx * ((l - 1) + npml * ((k - 1) + nz * (side - 1)));
       cpml_apply(dvy, m, A[side - 1][l - 1], B[side - 1][l - 1]);
     }
     boundary_index(k, nz, npml, l, side);
     if (side > 0) {
-      float* m = cp->mv[2] + (i - 1) + nx * ((j - 1) + ny * ((l - 1) + npml * (side - 1)));
+      S* m = cp->mv[2] + (i - 1) + nx * ((j - 1) + ny * ((l - 1) + npml * (side - 1)));
       cpml_apply(dvz, m, A[side - 1][l - 1], B[side - 1][l - 1]);
     }
   }
-  float& P = f[v.idx(i, j, k, 0)];
+  S& P = f[v.idx(i, j, k, 0)];
   if (mask) {
     R coeff = s.fq * (R)(mask[v.idx(i, j, k, 0)] ? 1 : 0);
-    P = (float)((R)P - coeff * (dvx + dvy + dvz));
+    P = (S)((R)P - coeff * (dvx + dvy + dvz));
   } else {
-    P = (float)((R)P - s.fq * (dvx + dvy + dvz));
+    P = (S)((R)P - s.fq * (dvx + dvy + dvz));
   }
 }
 
 // update_vx!/vy!/vz! (updates.jl:192-274) and the _mask variants (:380-501)
-template <typename R>
-inline void update_v(View& v, const Scal<R>& s, or_cpml* cp, const uint8_t* mask, int axis,
+template <typename R, typename S, typename CP>
+inline void update_v(ViewT<S>& v, const Scal<R>& s, CP* cp, const uint8_t* mask, int axis,
                      int64_t i, int64_t j, int64_t k) {
-  float* f = v.f;
+  S* f = v.f;
   const int64_t nx = v.nx, ny = v.ny, nz = v.nz;
   const int c = axis + 1;
   R h = axis == 0 ? s.dx : axis == 1 ? s.dy : s.dz;
@@ -455,16 +460,16 @@ inline void update_v(View& v, const Scal<R>& s, or_cpml* cp, const uint8_t* mask
   const int64_t npml = cp ? cp->npml : 0;
   const int64_t nm = npml + 1;  // size(mp_*, axis)
   if (cp && nm > 1) {
-    const float* co = cp->coef;
-    const float* A[2] = {co + 2 * npml, co + 3 * npml + 1};
-    const float* B[2] = {co + 6 * npml + 2, co + 7 * npml + 3};
+    const S* co = cp->coef;
+    const S* A[2] = {co + 2 * npml, co + 3 * npml + 1};
+    const S* B[2] = {co + 6 * npml + 2, co + 7 * npml + 3};
     int64_t ii = axis == 0 ? i : axis == 1 ? j : k;
     int64_t nd = axis == 0 ? nx : axis == 1 ? ny : nz;
     int64_t l;
     int side;
     boundary_index(ii, nd, nm, l, side);
     if (side > 0) {
-      float* m;
+      S* m;
       if (axis == 0)
         m = cp->mp[0] + (l - 1) + nm * ((j - 1) + ny * ((k - 1) + nz * (side - 1)));
       else if (axis == 1)
@@ -474,32 +479,33 @@ inline void update_v(View& v, const Scal<R>& s, or_cpml* cp, const uint8_t* mask
       cpml_apply(dp, m, A[side - 1][l - 1], B[side - 1][l - 1]);
     }
   }
-  float& V = f[v.idx(i, j, k, c)];
+  S& V = f[v.idx(i, j, k, c)];
   if (mask) {
     R coeff = s.fv * (R)(mask[v.idx(i, j, k, c)] ? 1 : 0);
-    V = (float)((R)V - coeff * dp);
+    V = (S)((R)V - coeff * dp);
   } else {
-    V = (float)((R)V - s.fv * dp);
+    V = (S)((R)V - s.fv * dp);
   }
 }
 
 // interp_trilinear! (derivatives.jl:30-60) with transceivers in ascending
 // order (the reference's parallel order is undefined where stencils overlap)
-inline void interp_trilinear(View& v, int c, int64_t it, const float* idx, const float* w,
-                             const float* src, float* rec, int64_t ntx, int64_t nt) {
+template <typename S>
+inline void interp_trilinear(ViewT<S>& v, int c, int64_t it, const float* idx, const S* w,
+                             const S* src, S* rec, int64_t ntx, int64_t nt) {
   for (int64_t is = 0; is < ntx; ++is) {
     int64_t I = (int64_t)idx[3 * is + 0];
     int64_t J = (int64_t)idx[3 * is + 1];
     int64_t K = (int64_t)idx[3 * is + 2];
     bool inb = I >= 1 && I < v.nx && J >= 1 && J < v.ny && K >= 1 && K < v.nz;
     if (!inb) continue;
-    float s = src[(it - 1) + nt * is];
-    float& r = rec[(it - 1) + nt * is];
+    S s = src[(it - 1) + nt * is];
+    S& r = rec[(it - 1) + nt * is];
     for (int kk = 0; kk < 2; ++kk)
       for (int jj = 0; jj < 2; ++jj)
         for (int ii = 0; ii < 2; ++ii) {
-          float wv = w[ii + 2 * jj + 4 * kk + 8 * is];
-          float& fv = v.f[v.idx(I + ii, J + jj, K + kk, c)];
+          S wv = w[ii + 2 * jj + 4 * kk + 8 * is];
+          S& fv = v.f[v.idx(I + ii, J + jj, K + kk, c)];
           r += wv * fv;
           fv += wv * s;
         }
@@ -575,10 +581,13 @@ void gf_extrapolate(const or_gfmap* g, or_txgrid* txs, int64_t nt, int64_t it) {
   }
 }
 
-template <typename R>
-int run_fdtd_t(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp,
-               const uint8_t* mask, int64_t start, int64_t stop, const or_gfmap* gf = nullptr) {
-  View v{d->nx, d->ny, d->nz, field};
+// R: arithmetic of the updates; S, TX, CP: storage of the field, the
+// transceiver buffers and the CPML memory (Float32, or Float64 throughout
+// for the FP64 run, which has no GF map).
+template <typename R, typename S, typename TX, typename CP>
+int run_fdtd_t(const or_domain* d, S* field, TX* txs, CP* cp, const uint8_t* mask, int64_t start,
+               int64_t stop, const or_gfmap* gf = nullptr) {
+  ViewT<S> v{d->nx, d->ny, d->nz, field};
   Scal<R> s{(R)d->fact_m0, (R)d->fact_m1, (R)d->dx, (R)d->dy, (R)d->dz};
   const int64_t nx = d->nx, ny = d->ny, nz = d->nz, nt = d->nt;
   const int64_t npml = cp ? cp->npml : 0;
@@ -597,7 +606,7 @@ int run_fdtd_t(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp,
           for (int64_t i = 1; i <= nx - 1; ++i) update_p_plain<R>(v, s, i, j, k);
       });
     } else {
-      or_cpml* cpu = npml == 0 ? nullptr : cp;
+      CP* cpu = npml == 0 ? nullptr : cp;
       bool guard = (mask == nullptr);  // update_p_cpml! guards npml>1, the mask variant does not
       pfor(1, (nz - 1) + 1, [&](int64_t k) {
         for (int64_t j = 1; j <= ny - 1; ++j)
@@ -622,18 +631,20 @@ int run_fdtd_t(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cp,
                        nt);
     // forward.jl:120 v2vn!
     for (int64_t is = 0; is < txs->ntx; ++is) {
-      const float* n = txs->dir + 4 * is;
+      const S* n = txs->dir + 4 * is;
       int64_t o = (it - 1) + nt * is;
       txs->vn_rec[o] = txs->rec[1][o] * n[1] + txs->rec[2][o] * n[2] + txs->rec[3][o] * n[3];
     }
     // forward.jl:123-128 in-loop GF extrapolation
-    if (gf && it < nt) gf_extrapolate(gf, txs, nt, it);
+    if constexpr (std::is_same<TX, or_txgrid>::value) {
+      if (gf && it < nt) gf_extrapolate(gf, txs, nt, it);
+    }
     // forward.jl:130-132 vn2v! into row it+1
     if (it < nt) {
       for (int64_t is = 0; is < txs->ntx; ++is) {
-        const float* n = txs->dir + 4 * is;
+        const S* n = txs->dir + 4 * is;
         int64_t o = it + nt * is;
-        float vn = txs->vn_src[o];
+        S vn = txs->vn_src[o];
         txs->src[1][o] += vn * n[1];
         txs->src[2][o] += vn * n[2];
         txs->src[3][o] += vn * n[3];
@@ -998,6 +1009,18 @@ int or_run_fdtd(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
   set_threads(nthreads);
   if (mode == OR_MODE_FP32)
     return run_fdtd_t<float>(d, field, txs, cpml, mask, start_step, stop_step);
+  return run_fdtd_t<double>(d, field, txs, cpml, mask, start_step, stop_step);
+}
+
+// run_fdtd! with every array in Float64: the FP64 run the error statements
+// of the Float32 paths are measured against.  Same operation order as the
+// Float32 restatement; coefficients, weights and sources unrounded.
+int or_run_fdtd64(const or_domain* d, double* field, or_txgrid64* txs, or_cpml64* cpml,
+                  const uint8_t* mask, int64_t start_step, int64_t stop_step, int nthreads) {
+  if (!d || !field || !txs) return -1;
+  if (start_step < 1) return -1;
+  if (stop_step > d->nt) return -1;
+  set_threads(nthreads);
   return run_fdtd_t<double>(d, field, txs, cpml, mask, start_step, stop_step);
 }
 

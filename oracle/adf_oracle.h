@@ -69,6 +69,25 @@ typedef struct {
   const float* coef;
 } or_cpml;
 
+/* The same buffers in Float64, for the FP64 run (or_run_fdtd64).  idx stays
+ * Float32: its values are small integers, exact in either type.          */
+typedef struct {
+  int64_t ntx, nt;
+  float* idx[4];
+  double* w[4];
+  double* src[4];
+  double* rec[4];
+  double* dir;
+  double* vn_src;
+  double* vn_rec;
+} or_txgrid64;
+typedef struct {
+  int64_t npml;
+  double* mv[3];
+  double* mp[3];
+  const double* coef;
+} or_cpml64;
+
 enum { OR_MODE_PROMOTE = 0, OR_MODE_FP32 = 1 };
 enum { OR_SHAPE_NONE = 0, OR_SHAPE_SPHERE = 1, OR_SHAPE_CUBE = 2, OR_SHAPE_CROSS = 3,
        OR_SHAPE_ELLIPSOID = 4 };
@@ -107,6 +126,11 @@ int or_pack_transceivers(const or_domain* d, const double* points, const double*
 int or_run_fdtd(const or_domain* d, float* field, or_txgrid* txs, or_cpml* cpml,
                 const uint8_t* mask, int64_t start_step, int64_t stop_step, int mode,
                 int nthreads);
+/* run_fdtd! in Float64 throughout (field, memory, coefficients, weights,
+ * traces): the reference's algorithm without any Float32 rounding, which
+ * the error statements of the Float32 paths are measured against.        */
+int or_run_fdtd64(const or_domain* d, double* field, or_txgrid64* txs, or_cpml64* cpml,
+                  const uint8_t* mask, int64_t start_step, int64_t stop_step, int nthreads);
 
 /* In-loop GF extrapolation of run_fdtd!(...; gf_map) (src/kernels/
  * extrapolation.jl:36-87, 91-249; forward.jl:123-128), after v2vn! of each

@@ -58,6 +58,11 @@ class _Cpml(C.Structure):
                 ("coef", C.c_void_p)]
 
 
+# the Float64 run's buffers have the same fields (pointer types differ only)
+_TxGrid64 = _TxGrid
+_Cpml64 = _Cpml
+
+
 class _GfMap(C.Structure):
     _fields_ = [("kind", C.c_int), ("nt_gf", C.c_int64), ("n1", C.c_int64), ("n2", C.c_int64),
                 ("t", C.c_void_p * 4), ("i_src", C.c_void_p), ("n_src", C.c_int64),
@@ -91,6 +96,8 @@ def lib():
                                            C.POINTER(_TxGrid)]
         L.or_run_fdtd.argtypes = [dp, C.c_void_p, C.POINTER(_TxGrid), C.POINTER(_Cpml),
                                   C.c_void_p, C.c_int64, C.c_int64, C.c_int, C.c_int]
+        L.or_run_fdtd64.argtypes = [dp, C.c_void_p, C.POINTER(_TxGrid64), C.POINTER(_Cpml64),
+                                    C.c_void_p, C.c_int64, C.c_int64, C.c_int]
         L.or_run_fdtd_gf.argtypes = [dp, C.c_void_p, C.POINTER(_TxGrid), C.POINTER(_Cpml),
                                      C.c_void_p, C.c_int64, C.c_int64, C.c_int,
                                      C.POINTER(_GfMap), C.c_int]
@@ -332,6 +339,56 @@ def run_fdtd(d: Domain, field, txs: TxGrid, cpml: CpmlState, mask=None, start_st
     _chk(lib().or_run_fdtd(C.byref(d), _p(field), C.byref(cg), C.byref(cc) if cc else None,
                            _p(mask) if mask is not None else None, start_step, stop_step,
                            MODES[mode], nthreads), "run_fdtd")
+    return field
+
+
+def transceivers_to_grid64(d: Domain, points, directions, tfs) -> TxGrid:
+    """transceiversToGrid with Float64 weights and sources (the FP64 run's
+    inputs): the weights of trilinearInterpolation and tf * direction
+    unrounded; indices as in the Float32 grid."""
+    points = np.asarray(points, np.float64).reshape(-1, 3)
+    directions = np.asarray(directions, np.float64).reshape(-1, 4)
+    ntx, nt = points.shape[0], d.nt
+    tfs = np.asarray(tfs, np.float64).reshape(ntx, nt)
+    idx = [np.zeros((3, ntx), np.float32, order="F") for _ in range(4)]
+    w = [np.zeros((2, 2, 2, ntx), np.float64, order="F") for _ in range(4)]
+    for i in range(ntx):
+        ii, ww = trilinear(d, points[i])
+        for c in range(4):
+            idx[c][:, i] = ii[:, c]
+            w[c][..., i] = ww[..., c]
+    src = [np.asfortranarray((tfs * directions[:, c:c + 1]).T) for c in range(4)]
+    rec = [np.zeros((nt, ntx), np.float64, order="F") for _ in range(4)]
+    return TxGrid(idx, w, src, rec, np.asfortranarray(directions.T),
+                  np.zeros((nt, ntx), np.float64, order="F"),
+                  np.zeros((nt, ntx), np.float64, order="F"))
+
+
+class CpmlState64(CpmlState):
+    """Cpml memory and coefficients in Float64 (the FP64 run)."""
+
+    def __init__(self, d: Domain, npml: int, rcoef=1e-4, fc=3e3):
+        super().__init__(d, npml, rcoef, fc)
+        self.mv = [a.astype(np.float64, order="F") for a in self.mv]
+        self.mp = [a.astype(np.float64, order="F") for a in self.mp]
+        self.coef = np.concatenate([np.asarray(p, np.float64) for p in self.profiles64])
+
+
+def run_fdtd64(d: Domain, field, txs: TxGrid, cpml: CpmlState64, mask=None, start_step=1,
+               stop_step=None, nthreads=0):
+    """run_fdtd! with every array in Float64 (or_run_fdtd64): the reference
+    algorithm without Float32 rounding, for error statements."""
+    stop_step = d.nt if stop_step is None else stop_step
+    assert field.flags.f_contiguous and field.dtype == np.float64
+    assert field.shape == (d.nx, d.ny, d.nz, 4)
+    assert txs.w[0].dtype == np.float64 and txs.src[0].dtype == np.float64
+    cg = txs._c()
+    cc = cpml._c() if cpml is not None else None
+    if cc is not None:
+        assert cpml.coef.dtype == np.float64 and cpml.mv[0].dtype == np.float64
+    _chk(lib().or_run_fdtd64(C.byref(d), _p(field), C.byref(cg), C.byref(cc) if cc else None,
+                             _p(mask) if mask is not None else None, start_step, stop_step,
+                             nthreads), "run_fdtd64")
     return field
 
 

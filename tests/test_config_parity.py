@@ -1,0 +1,203 @@
+"""GPU parity at the benchmark workloads' full grid sizes, against the oracle
+in promote mode (the bar: 1e-5 relative L2) and against the oracle's FP64
+run (the error statement: every trace and field of the Float32 path against
+the reference algorithm without Float32 rounding).
+
+Cases:
+* the plain single solve, in full: 96^3, 10-cell CPML (fc 2 kHz), a q point
+  source at the centre driven by a 2 kHz Ricker wavelet, 64 Fibonacci
+  receivers at 30 cells, 800 steps (run_fdtd!, src/simulation.jl:542-557);
+* one impulsive GF solve of the 256^3 retrieval workload through the GF
+  engine, batched and plain: rigid sphere of 24 cells, source on the
+  60-cell Fibonacci sphere, 2048-point shell at 45 cells, 400 of its 2000
+  steps (impulsive_gfs' solve loop, src/greens.jl:143-199);
+* the 512^3 hologram grid: 12-cell CPML, rigid ellipsoid 80/60/40 cells,
+  a random initial pressure field so that every CPML slab and the mask are
+  active from step 1, a point source and a 256-point shell, 20 steps.
+
+Set-up values are checked first: CPML profiles (after Float32 rounding),
+masks, transceiver indices, weights and sources bit-exact; the host-side
+wavelets and Fibonacci points (numpy against the oracle's libm) to the last
+unit in the last place.
+When $ADF_PARITY_LOG names a file, each case appends its measured errors
+to it as one JSON line.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DX = 0.005
+C0, RHO = 343.0, 1.2
+DT = 0.5 * DX / C0 / np.sqrt(3.0)
+TOL = 1e-5        # trace / field bar against the oracle in the same arithmetic
+FP64_BOUND = 1e-3  # sanity bound of the stated FP64 errors (Float32 storage)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a))
+
+
+def record(case, **errs):
+    path = os.environ.get("ADF_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"case": case, **errs}) + "\n")
+
+
+def domains(adf, oracle, n, steps):
+    kw = dict(tmax=(steps - 0.5) * DT, xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
+    d, o = adf.Domain(**kw), oracle.domain(**kw)
+    assert d.nt == steps == o.nt and d.dt == o.dt and d.dx == o.dx
+    return d, o
+
+
+def packed_pair(adf, oracle, d, o, pts, dirs, tfs):
+    """transceiversToGrid on both sides; indices, weights and sources bit-exact."""
+    g = adf.transceivers_to_grid(d, [adf.Transceiver(p, q, t) for p, q, t in zip(pts, dirs, tfs)])
+    go = oracle.transceivers_to_grid(o, pts, dirs, tfs)
+    for c in range(4):
+        assert np.array_equal(g.idx[c], go.idx[c]), f"indices of channel {c}"
+        assert np.array_equal(g.w[c], go.w[c]), f"weights of channel {c}"
+        assert np.array_equal(g.src[c], go.src[c]), f"sources of channel {c}"
+    assert np.array_equal(g.direction, go.dir)
+    return g, go
+
+
+def cpml_pair(adf, oracle, d, o, npml, fc):
+    cp = adf.Cpml(d, npml, 1e-4, fc)
+    co = oracle.CpmlState(o, npml, 1e-4, fc)
+    assert np.array_equal(cp.coef, co.coef), "CPML profiles after Float32 rounding"
+    return cp, co
+
+
+def trace_errors(g, go, prefix=""):
+    return {prefix + "p_rec": rel_l2(g.rec[0], go.rec[0]),
+            prefix + "vn_rec": rel_l2(g.vn_rec, go.vn_rec)}
+
+
+def field_errors(f, fo, prefix=""):
+    return {f"{prefix}field{c}": rel_l2(f[..., c], fo[..., c]) for c in range(4)}
+
+
+def test_plain_solve_96cube_800_steps(adf, oracle, ctx):
+    n, steps, npml = 96, 800, 10
+    d, o = domains(adf, oracle, n, steps)
+    # host-side set-up values (numpy against the oracle's libm: last-ulp level);
+    # both sides are then packed from the same Float64 inputs
+    tf = adf.ricker_wavelet(d, 2000.0, injection=False)
+    assert np.allclose(tf, oracle.ricker_wavelet(o, 2000.0, injection=False), rtol=0, atol=1e-15)
+    rp, rn = adf.fibonacci_sphere(64, 30 * DX)
+    rpo, rno = oracle.fibonacci_sphere(64, 30 * DX)
+    assert np.allclose(rp, rpo, rtol=0, atol=1e-15) and np.allclose(rn, rno, rtol=0, atol=1e-15)
+    pts = np.vstack([[0.0, 0.0, 0.0], rp])
+    dirs = np.vstack([[1.0, 0, 0, 0], np.hstack([np.zeros((64, 1)), rn])])
+    tfs = np.vstack([tf, np.zeros((64, steps))])
+    g, go = packed_pair(adf, oracle, d, o, pts, dirs, tfs)
+    cp, co = cpml_pair(adf, oracle, d, o, npml, 2000.0)
+    f = np.zeros((n, n, n, 4), np.float32, order="F")
+    fo = f.copy(order="F")
+    adf.run_fdtd(d, f, g, cp, None)
+    oracle.run_fdtd(o, fo, go, co, None)
+    errs = {**trace_errors(g, go), **field_errors(f, fo)}
+    for a in range(3):
+        errs[f"mv{a}"] = rel_l2(cp.mv[a], co.mv[a])
+        errs[f"mp{a}"] = rel_l2(cp.mp[a], co.mp[a])
+    g64 = oracle.transceivers_to_grid64(o, pts, dirs, tfs)
+    f64 = np.zeros((n, n, n, 4), np.float64, order="F")
+    oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, npml, 1e-4, 2000.0), None)
+    e64 = {**trace_errors(g, g64), **field_errors(f, f64)}
+    e64_oracle = trace_errors(go, g64)  # the promote oracle itself against FP64
+    record("96^3 plain solve, 800 steps", vs_promote=errs, vs_fp64=e64,
+           promote_oracle_vs_fp64=e64_oracle)
+    assert np.abs(go.rec[0][:, 1:]).max() > 0 and np.abs(co.mv[0]).max() > 0
+    bad = {k: v for k, v in errs.items() if not v <= TOL}
+    assert not bad, f"against the promote oracle: {bad}; all {errs}"
+    assert max(e64.values()) < FP64_BOUND, e64
+
+
+def gf_request(adf, d, n_rec=2048):
+    src, _ = adf.fibonacci_sphere(512, 60 * DX)
+    rp, rn = adf.fibonacci_sphere(n_rec, 45 * DX)
+    tf, _ = adf.impulsive_wavelet(d, 2000.0)
+    return adf.GfRequest(d, src[0], [1.0, 0, 0, 0], tf, rp, rn, npml=10, pml_fc=2000.0,
+                         scatterer="sphere", scatterer_kw=dict(radius=24 * DX))
+
+
+def test_gf_solve_256cube_shell_2048(adf, oracle, ctx):
+    n, steps = 256, 400
+    d, o = domains(adf, oracle, n, steps)
+    req = gf_request(adf, d)
+    # the mask the engine builds on the device, against the oracle's
+    m = adf.build_update_mask(d, "sphere", radius=24 * DX)
+    mo = oracle.build_update_mask(o, "sphere", radius=24 * DX)
+    assert np.array_equal(m, mo.astype(bool)), "mask"
+    tfo, _ = oracle.impulsive_wavelet(o, 2000.0)
+    assert np.allclose(req.src_tf, tfo, rtol=1e-14, atol=0)
+    adf.gf_solve_batch([req], batched=True)
+    plain = gf_request(adf, d)
+    adf.gf_solve_batch([plain], batched=False)
+    assert np.array_equal(req.p, plain.p) and np.array_equal(req.vn, plain.vn)
+    nr = req.rec_points.shape[0]
+    pts = np.vstack([req.src_point, req.rec_points])
+    dirs = np.vstack([[1.0, 0, 0, 0], np.hstack([np.zeros((nr, 1)), req.rec_normals])])
+    tfs = np.vstack([req.src_tf, np.zeros((nr, steps))])
+    go = oracle.transceivers_to_grid(o, pts, dirs, tfs)
+    co = oracle.CpmlState(o, 10, 1e-4, 2000.0)
+    assert np.array_equal(adf.Cpml(d, 10, 1e-4, 2000.0).coef, co.coef)
+    fo = np.zeros((n, n, n, 4), np.float32, order="F")
+    oracle.run_fdtd(o, fo, go, co, mo)
+    errs = {"p": rel_l2(req.p, go.rec[0][:, 1:]), "vn": rel_l2(req.vn, go.vn_rec[:, 1:])}
+    del fo
+    g64 = oracle.transceivers_to_grid64(o, pts, dirs, tfs)
+    f64 = np.zeros((n, n, n, 4), np.float64, order="F")
+    oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, 10, 1e-4, 2000.0), mo)
+    del f64
+    e64 = {"p": rel_l2(req.p, g64.rec[0][:, 1:]), "vn": rel_l2(req.vn, g64.vn_rec[:, 1:])}
+    record("256^3 GF solve, 2048-point shell, 400 steps", vs_promote=errs, vs_fp64=e64,
+           promote_oracle_vs_fp64={"p": rel_l2(go.rec[0][:, 1:], g64.rec[0][:, 1:]),
+                                   "vn": rel_l2(go.vn_rec[:, 1:], g64.vn_rec[:, 1:])})
+    assert np.abs(go.rec[0][:, 1:]).max() > 0
+    assert max(errs.values()) <= TOL, errs
+    assert max(e64.values()) < FP64_BOUND, e64
+
+
+def test_hologram_grid_512cube_ellipsoid(adf, oracle, ctx):
+    n, steps, npml = 512, 20, 12
+    d, o = domains(adf, oracle, n, steps)
+    kw = dict(semi_axes=(80 * DX, 60 * DX, 40 * DX))
+    m = adf.build_update_mask(d, "ellipsoid", **kw)
+    mo = oracle.build_update_mask(o, "ellipsoid", **kw)
+    assert np.array_equal(m, mo.astype(bool)), "mask"
+    tf = adf.ricker_wavelet(d, 8000.0, injection=False) * 1e3
+    rp, rn = adf.fibonacci_sphere(256, 130 * DX)
+    pts = np.vstack([[0.0, 0.0, 100 * DX], rp])
+    dirs = np.vstack([[1.0, 0, 0, 0], np.hstack([np.zeros((256, 1)), rn])])
+    tfs = np.vstack([tf, np.zeros((256, steps))])
+    g, go = packed_pair(adf, oracle, d, o, pts, dirs, tfs)
+    cp, co = cpml_pair(adf, oracle, d, o, npml, 2000.0)
+    rng = np.random.default_rng(512)
+    f = np.zeros((n, n, n, 4), np.float32, order="F")
+    f[..., 0] = rng.standard_normal((n, n, n), dtype=np.float32) * 1e-3
+    fo = f.copy(order="F")
+    f64 = f.astype(np.float64, order="F")
+    adf.run_fdtd(d, f, g, cp, m)
+    oracle.run_fdtd(o, fo, go, co, mo)
+    errs = {**trace_errors(g, go), **field_errors(f, fo)}
+    for a in range(3):
+        errs[f"mv{a}"] = rel_l2(cp.mv[a], co.mv[a])
+        errs[f"mp{a}"] = rel_l2(cp.mp[a], co.mp[a])
+    del fo
+    g64 = oracle.transceivers_to_grid64(o, pts, dirs, tfs)
+    oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, npml, 1e-4, 2000.0), mo)
+    e64 = {**trace_errors(g, g64), **field_errors(f, f64)}
+    record("512^3 ellipsoid, random initial field, 20 steps", vs_promote=errs, vs_fp64=e64)
+    bad = {k: v for k, v in errs.items() if not v <= TOL}
+    assert not bad, f"against the promote oracle: {bad}; all {errs}"
+    assert max(e64.values()) < FP64_BOUND, e64

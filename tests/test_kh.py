@@ -151,3 +151,21 @@ def test_kh_velocity_matches_fp64_oracle(adf, oracle, ctx, ns, nr, nt, dt, r_sur
     assert np.isfinite(out).all()
     assert np.abs(ref).max() > 0
     assert rel_l2(out, ref) <= RTOL_L2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("skip", [0, 1])
+def test_kh_bounded_wait_ends_in_an_error_code(adf, oracle, ctx, skip):
+    """A staged chunk whose bytes never arrive (its copies are not issued, so
+    nothing is in flight) makes every CTA's bounded wait give up: the call
+    returns ADF_E_TIMEOUT instead of hanging, and the context then runs a
+    normal call correctly.  skip 0 also drains the next chunk's copies, which
+    were issued before the wait gave up."""
+    c = case(96, 40, 700, 5e-6, 0.25, 0.9)
+    adf.kh_test_fault(skip, 64, ctx=ctx)
+    with pytest.raises(adf.AdfError) as ei:
+        adf.kh_pressure(c["sp"], c["sn"], c["rp"], c["q"], c["f"], c["dt"], c["sigma"], C0,
+                        c["aq"], c["af"], rho=RHO, ctx=ctx)
+    assert ei.value.code == -6, ei.value
+    out, ref = run_pair(adf, oracle, c)  # the hook is one-shot
+    assert rel_l2(out, ref) <= RTOL_L2

@@ -36,6 +36,34 @@ def test_reciprocity_reference_setup(oracle):
     assert rms / peak < 0.01
 
 
+def test_fp64_run_reciprocity_and_float32_gap(oracle):
+    """The oracle's FP64 run (every array in Float64) on test_reciprocity.jl's
+    set-up: reciprocity holds in FP64 too, and the Float32-storage run in
+    promote mode stays within Float32 rounding of it (the error the GPU
+    parity tests state against this run)."""
+    d = oracle.domain(tmax=4.0e-4, xmax=0.3, nx=51, cf=0.5)
+    src, _ = oracle.impulsive_wavelet(d, 7000.0)
+    zero = np.zeros(d.nt)
+    A = [0.10, -0.05, 0.02]
+    B = [-0.04, 0.07, 0.06]
+
+    def record_at(a, b):
+        args = ([a, b], [[1, 0, 0, 0], [1, 0, 0, 0]], [src, zero])
+        g64 = oracle.transceivers_to_grid64(d, *args)
+        f64 = np.zeros((51, 51, 51, 4), np.float64, order="F")
+        oracle.run_fdtd64(d, f64, g64, oracle.CpmlState64(d, 6, 1e-4, 3e3), None)
+        g = oracle.transceivers_to_grid(d, *args)
+        f = np.zeros((51, 51, 51, 4), np.float32, order="F")
+        oracle.run_fdtd(d, f, g, oracle.CpmlState(d, 6, 1e-4, 3e3), None)
+        r64, r32 = g64.rec[0][:, 1], g.rec[0][:, 1].astype(np.float64)
+        assert np.linalg.norm(r32 - r64) / np.linalg.norm(r64) < 1e-5
+        assert np.abs(f - f64).max() > 0  # the runs really differ in precision
+        return r64
+
+    ab, ba = record_at(A, B), record_at(B, A)
+    assert np.sqrt(np.mean((ab - ba) ** 2)) / np.abs(ab).max() < 0.01
+
+
 def _random_problem(rng, n_in, n_out, k, nt):
     pin = rng.standard_normal((nt, n_in)).astype(np.float32)
     pp = rng.standard_normal((k, n_out, n_in)).astype(np.float32)
