@@ -15,6 +15,11 @@ namespace adf {
 //         a=0: [nz][ny][npml]   a=1: [nz][npml][nxp]   a=2: [npml][ny][nxp]
 // psi_v[a]: v-side, the same with npml+1.
 // traces: src/rec/vn_src/vn_rec [nt][ntx] (transceiver fastest).
+// Staged planes of the step kernel: x range xb-4 .. xb+kXT+3 of a 64-cell
+// tile (the halo column xb-1 and Vx at xb+64 included), rows j0-1 .. j0+ty.
+constexpr int kStageW = 72;
+constexpr int kStepRing = 3;  // planes k, k+1 resident while k+2 lands
+
 enum : int {
   SF_MASK = 1,      // solve has a scatterer mask
   SF_PCPML = 2,     // p-side CPML active (npml>1, or npml>=1 with a mask)
@@ -45,6 +50,9 @@ struct SolveDev {
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;
+  // two CUtensorMaps (128 B each) over field buffers 0 and 1: 4D (x: nxp,
+  // y: ny, z: nz, channel: 4), box (kStageW, ty + 2, 1, 4), zero fill
+  const void* fmap;
   long long buf_stride;   // floats per field buffer (4*nz*ny*nxp)
   long long chan_stride;  // floats per channel (nz*ny*nxp)
   float* psi_p[3];

@@ -24,6 +24,7 @@
 // variant.  Injection/recording (derivatives.jl:30-60) is pure Float32 with
 // separate multiply and add, as the reference computes it.
 #include "adf_internal.h"
+#include "ptx_util.h"
 
 namespace adf {
 
@@ -185,23 +186,24 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
   return make_float4(o[0], o[1], o[2], o[3]);
 }
 
-// The same update for one cell (the halo column x = xb-1 of an x tile).
+// The same update for one cell (the halo column x = xb-1 of an x tile), from
+// the staged planes: `st` is plane k, `stn` plane k+1, `c` the cell's offset
+// in a channel of a stage and `cst` the channel stride.
 template <typename R>
 __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
-                                               const float* co, const float* fld, int x) {
+                                               const float* co, const float* st, const float* stn,
+                                               int c, int cst, int x) {
   using A = Arith<R>;
   const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, j = rc.j, k = rc.k, nxp = rc.nxp;
-  const long long cs = S.chan_stride, plane = (long long)ny * nxp;
-  const float* b = fld + ((long long)k * ny + j) * nxp + x;
   const bool rigid_y = j == ny - 1, rigid_z = k == nz - 1;
   const bool plain_rigid = rigid_y || rigid_z;
   const bool upd = x <= nx - 2 && !(rigid_y && rigid_z);
-  const float P = __ldg(b);
+  const float P = st[c];
   if (!upd) return P;
-  const float X0 = __ldg(b + cs), X1 = __ldg(b + cs + 1);
-  const float Y0 = __ldg(b + 2 * cs), Z0 = __ldg(b + 3 * cs);
-  const float dy = rigid_y ? __fmul_rn(-2.0f, Y0) : __fsub_rn(__ldg(b + 2 * cs + nxp), Y0);
-  const float dz = rigid_z ? __fmul_rn(-2.0f, Z0) : __fsub_rn(__ldg(b + 3 * cs + plane), Z0);
+  const float X0 = st[cst + c], X1 = st[cst + c + 1];
+  const float Y0 = st[2 * cst + c], Z0 = st[3 * cst + c];
+  const float dy = rigid_y ? __fmul_rn(-2.0f, Y0) : __fsub_rn(st[2 * cst + c + kStageW], Y0);
+  const float dz = rigid_z ? __fmul_rn(-2.0f, Z0) : __fsub_rn(stn[3 * cst + c], Z0);
   R dvx = A::mul(A::cv(__fsub_rn(X1, X0)), g.rdx);
   R dvy = A::mul(A::cv(dy), g.rdy);
   R dvz = A::mul(A::cv(dz), g.rdz);
@@ -458,9 +460,16 @@ constexpr int kXT = 64;             // cells per x tile (4 warps)
 constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..] = cells
 constexpr int kStepThreads = 32 * kXT / 16;  // warps of 4 quads x 8 rows
 
+constexpr int kStageFloats = 4 * (kMaxTy + 2) * kStageW;  // one staged plane, 4 channels
+// Polls of a staged plane's bounded wait: a plane lands within microseconds,
+// so a limit far below kWaitLimit keeps a lost copy from stalling the GPU
+constexpr uint32_t kStepWaitLimit = 1u << 20;
+static_assert((kStageFloats * 4) % 128 == 0, "stages stay 128-B aligned");
+
 template <typename R>
 __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
-                                          float* sPn, float* sV, const float* co) {
+                                          float* sPn, float* sV, const float* co, float* ring,
+                                          uint64_t* rbar) {
   const int lane = threadIdx.x, wid = threadIdx.y;
   const int tid = wid * 32 + lane, nthr = blockDim.x * blockDim.y;
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxp = S.nxp, ty = S.ty, npml = S.npml;
@@ -475,7 +484,6 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   const bool vrow = act && r >= 1;      // ... and owns it (velocity update, stores)
   const int rb = (it - S.it_first) & 1, wb = rb ^ 1;
   const long long cs = S.chan_stride, plane = (long long)ny * nxp;
-  const float* fin = S.field + rb * S.buf_stride;
   float* fout = S.field + wb * S.buf_stride;
   const bool has_mask = (S.flags & SF_MASK) != 0;
   const bool pcp = (S.flags & SF_PCPML) != 0, vcp = (S.flags & SF_VCPML) != 0;
@@ -515,13 +523,40 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   const int pq = r * kPnPitch + 4 + 4 * qx;  // this quad in a shared new-P plane
   const int z0 = item.z, z1 = item.w;
   const int kfirst = z0 > 0 ? z0 - 1 : z0;
+  // Planes kfirst .. klast are staged by TMA into a ring of kStepRing slots
+  // (the last one only for Vz of plane z1-1; plane nz would be all zeros,
+  // which the loop supplies itself).  A stage holds channels P, Vx, Vy, Vz of
+  // rows j0-1 .. j0+ty and x = xb-4 .. xb+67 (zero outside the grid).
+  const int klast = min(z1, nz - 1);
+  const int cst = (ty + 2) * kStageW;         // channel stride in a stage
+  const int so = r * kStageW + 4 + 4 * qx;    // this quad in a stage channel
+  const void* fmap = static_cast<const char*>(S.fmap) + rb * 128;
+  auto slot_of = [&](int k) { return (k - kfirst) % kStepRing; };
+  auto issue = [&](int k) {  // one thread
+    const int sl = slot_of(k);
+    fence_proxy_async_smem();  // the slot was last read through the generic proxy
+    const uint32_t bar = smem_u32(rbar + sl);
+    mbar_expect_tx(bar, (uint32_t)(16 * cst));
+    tma_load_4d(smem_u32(ring + sl * kStageFloats), fmap, xb - 4, j0 - 1, k, 0, bar);
+  };
+  auto wait = [&](int k) {
+    const int u = k - kfirst;
+    if (!mbar_wait(smem_u32(rbar + u % kStepRing), (uint32_t)(u / kStepRing) & 1u, kStepWaitLimit))
+      atomicOr(S.err, 4);  // reported as ADF_E_TIMEOUT; the values read are wrong
+  };
+  if (tid == 0)
+    for (int k = kfirst; k <= min(klast, kfirst + kStepRing - 1); ++k) issue(k);
+  wait(kfirst);
   float4 Z0 = make_float4(0.f, 0.f, 0.f, 0.f), Pzm = Z0;
-  if (act) Z0 = ldg4(fin + 3 * cs + kfirst * plane + rowoff);
+  if (act) Z0 = ld4(ring + slot_of(kfirst) * kStageFloats + 3 * cst + so);
   const int* tp = S.tp_off + (long long)T * nz * 4;
   for (int k = kfirst; k < z1; ++k) {
     const bool prologue = k < z0;
     rc.k = k;
     float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
+    const float* st = ring + slot_of(k) * kStageFloats;
+    const float* stn = ring + slot_of(k + 1) * kStageFloats;
+    if (k + 1 <= klast) wait(k + 1);
     const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
     const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
     const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
@@ -529,13 +564,12 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     float4 Pn = make_float4(0.f, 0.f, 0.f, 0.f), X4 = Pn, Y0 = Pn, Z1 = Pn;
     uint32_t nib = 0xFFFFu;
     if (act) {
-      const float* b = fin + k * plane + rowoff;
-      const float4 P4 = ldg4(b);
-      X4 = ldg4(b + cs);
-      Y0 = ldg4(b + 2 * cs);
-      const float X5 = x0 + 4 < nxp ? __ldg(b + cs + 4) : 0.f;
-      const float4 Y1 = j + 1 < ny ? ldg4(b + 2 * cs + nxp) : Pn;
-      Z1 = k + 1 < nz ? ldg4(b + 3 * cs + plane) : Pn;
+      const float4 P4 = ld4(st + so);
+      X4 = ld4(st + cst + so);
+      Y0 = ld4(st + 2 * cst + so);
+      const float X5 = st[cst + so + 4];
+      const float4 Y1 = ld4(st + 2 * cst + so + kStageW);
+      Z1 = k + 1 < nz ? ld4(stn + 3 * cst + so) : Pn;
       if (has_mask)
         nib = (__ldg(S.mask_bits + ((long long)k * ny + j) * S.mw + (x0 >> 3)) >> ((x0 & 4) * 4)) &
               0xFFFFu;
@@ -546,8 +580,11 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
         Pn = p_update_quad<R>(S, rc, g, co, x0, vrow && !prologue, P4, X4, X5, Y0, Y1, Z0, Z1, nib);
       st4(pn + pq, Pn);
     }
-    if (qx == 0 && r >= 1 && row_ok && xb > 0) pn[pq - 1] = p_update_cell<R>(S, rc, g, co, fin, xb - 1);
+    if (qx == 0 && r >= 1 && row_ok && xb > 0)
+      pn[pq - 1] = p_update_cell<R>(S, rc, g, co, st, stn, so - 1, cst, xb - 1);
     __syncthreads();
+    // every read of plane k's stage is done: refill its slot
+    if (tid == 0 && k + kStepRing <= klast) issue(k + kStepRing);
     // ---- q channel: inject/record on the new P (forward.jl:92) ----
     if (off0 < off1) {
       apply_entries(S, off0, off1, 0, nxp, xb - 1, xb + kXT, xb, !prologue, it, tid, nthr,
@@ -612,7 +649,18 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   }
 }
 
-__global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) adf_fdtd_step_kernel(const StepParams p) {
+// Shared memory: the staged-plane ring (dynamic, kStepRing * kStageFloats
+// floats) plus the new-P planes, the f-channel staging and the descriptor:
+// 43.4 KB per CTA, five CTAs per SM.
+constexpr int kStepCtasPerSm = 5;
+// (+128 B so that the ring can start on a 128-B boundary, as TMA destinations must)
+constexpr size_t kStepDynSmem = sizeof(float) * kStepRing * kStageFloats + 128;
+
+__global__ void __launch_bounds__(kStepThreads, kStepCtasPerSm) adf_fdtd_step_kernel(const StepParams p) {
+  extern __shared__ __align__(128) float dyn_smem[];
+  float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dyn_smem) + 127) &
+                                         ~static_cast<uintptr_t>(127));
+  __shared__ __align__(8) uint64_t rbar[kStepRing];
   __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
   __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
   __shared__ float s_co[kMaxCoef];
@@ -628,12 +676,16 @@ __global__ void __launch_bounds__(kStepThreads, 1024 / kStepThreads) adf_fdtd_st
     for (int w = tid; w < (int)(sizeof(SolveDev) / 4); w += nthr) dst[w] = src[w];
     const int ncoef = 8 * G.npml + 4;
     for (int w = tid; w < ncoef; w += nthr) s_co[w] = G.coef[w];
+    if (tid == 0) {
+      for (int q = 0; q < kStepRing; ++q) mbar_init(smem_u32(rbar + q), 1);
+      fence_mbar_init();
+    }
   }
   __syncthreads();
   if (S.flags & SF_FP32)
-    step_item<float>(p, S, item, it, sPn, sV, s_co);
+    step_item<float>(p, S, item, it, sPn, sV, s_co, ring, rbar);
   else
-    step_item<double>(p, S, item, it, sPn, sV, s_co);
+    step_item<double>(p, S, item, it, sPn, sV, s_co, ring, rbar);
 }
 
 // Per-step trace assembly (derivatives.jl:51-56 record sums in corner order,
@@ -1010,7 +1062,7 @@ cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s) {
 
 cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s) {
   (void)max_ty;  // the block always holds kMaxTy rows; shorter tiles idle the rest
-  adf_fdtd_step_kernel<<<grid, dim3(32, kXT / 16), 0, s>>>(p);
+  adf_fdtd_step_kernel<<<grid, dim3(32, kXT / 16), kStepDynSmem, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -50,6 +50,21 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
       ::"r"(dst), "l"((uint64_t)src), "r"(bytes), "r"(mbar)
       : "memory");
 }
+// Four-dimensional tiled TMA load of one box global -> this CTA's shared
+// memory, completing on an mbarrier.  `map` is a CUtensorMap in global
+// memory (64-B aligned); the innermost coordinate x times the element size
+// must be a multiple of 16 bytes.  No multicast.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int x, int y, int z,
+                                            int c, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(mbar)
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }

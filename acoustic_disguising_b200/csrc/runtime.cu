@@ -19,6 +19,9 @@
 #include "../../include/adfdtd.h"
 #include "adf_internal.h"
 #include "host_math.h"
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "runtime.h"
 
 namespace adf {
@@ -234,6 +237,50 @@ template float* solve_dalloc<float>(Solve&, size_t, int&);
 template int* solve_dalloc<int>(Solve&, size_t, int&);
 template double* solve_dalloc<double>(Solve&, size_t, int&);
 
+// The step kernel's TMA descriptors of the two field buffers: a 4D tiled map
+// (x: nxp, y: ny, z: nz, channel: 4) with the staged box (kStageW, ty+2, 1, 4)
+// and zero fill outside the grid.  cuTensorMapEncodeTiled comes from the
+// driver through the runtime's entry-point query (no link against libcuda).
+static int make_field_maps(Solve& s) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    cudaGetLastError();
+  });
+  if (!encode) return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled is not available");
+  SolveDev& d = s.dev;
+  const cuuint64_t dims[4] = {(cuuint64_t)d.nxp, (cuuint64_t)d.ny, (cuuint64_t)d.nz, 4};
+  const cuuint64_t strides[3] = {(cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * d.ny * 4,
+                                 (cuuint64_t)d.chan_stride * 4};
+  const cuuint32_t box[4] = {(cuuint32_t)kStageW, (cuuint32_t)(d.ty + 2), 1, 4};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  for (int b = 0; b < 2; ++b) {
+    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(s.fmap_host + 128 * b);
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d.field + b * d.buf_stride,
+                              dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  }
+  int rc = ADF_OK;
+  void* dm = dalloc<unsigned char>(s, sizeof(s.fmap_host), rc);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(dm, s.fmap_host, sizeof(s.fmap_host), cudaMemcpyHostToDevice, s.stream) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, "tensor map upload failed");
+  }
+  d.fmap = dm;
+  return ADF_OK;
+}
+
 // Allocates everything except traces; field/psi zeroed.
 int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_mask, int arith,
                 int ntx) {
@@ -266,6 +313,8 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   d.field = dalloc<float>(s, (size_t)2 * d.buf_stride, rc);
   if (rc) return rc;
   cudaMemsetAsync(d.field, 0, (size_t)2 * d.buf_stride * 4, s.stream);
+  rc = make_field_maps(s);
+  if (rc) return rc;
   if (has_mask) {
     s.mask_bits = dalloc<uint32_t>(s, (size_t)d.mw * d.ny * d.nz, rc);
     if (rc) return rc;
@@ -572,6 +621,15 @@ int Batch::check_error(adf_ctx* ctx) {
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("device error: ") + cudaGetErrorString(e));
+  // per-solve error words written by the kernels (bit 2: a bounded wait for
+  // a staged plane gave up)
+  for (Solve* s : solves) {
+    int w = 0;
+    if (s->dev.err && cudaMemcpy(&w, s->dev.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(ADF_E_DEVICE, "error word read failed");
+    if (w & 4) return fail(ADF_E_TIMEOUT, "step kernel: a bounded wait for a staged plane gave up");
+    if (w) return fail(ADF_E_STATE, "step kernel error word " + std::to_string(w));
+  }
   return ADF_OK;
 }
 
