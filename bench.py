@@ -381,6 +381,45 @@ def kh_section(A, ctx, steps, warmup):
     }
 
 
+def kh_sharded_section(A, ctx, dist, device):
+    """The KH workload with its targets split across the ranks: rank 0 holds
+    the surface traces and broadcasts them once; each rank sums its block of
+    targets on its GPU; the blocks are all-gathered.  TFLOP/s from the
+    slowest rank's kernel time (max over ranks)."""
+    from acoustic_disguising_b200.shard import kh_sharded, target_block
+
+    rank, world = dist.get_rank(), dist.get_world_size()
+    sp, sn = A.fibonacci_sphere(KH_NS, KH_R_SURF)
+    rp, _ = A.fibonacci_sphere(KH_NR, KH_R_TGT)
+    q_in = f_in = None
+    if rank == 0:
+        rng = np.random.default_rng(KH_SEED)
+        f_in = ricker_noise(rng, KH_NT, KH_NS, KH_DT, 8e3)  # p traces
+        q_in = ricker_noise(rng, KH_NT, KH_NS, KH_DT, 8e3)  # v_n traces
+    sigma = math.sqrt(math.log(2.0)) / (2 * math.pi * KH_F3DB)
+    dS = 4 * math.pi * KH_R_SURF ** 2 / KH_NS
+    aq, af = -RHO * dS * KH_DT, -dS * KH_DT
+    kms = []
+
+    def compute(sp_, sn_, q, f, rp_, _rn):
+        out = A.kh_pressure(sp_, sn_, rp_, q, f, KH_DT, sigma, C0, aq, af, rho=RHO, ctx=ctx)
+        kms.append(ctx.last_timing()[0])
+        return out
+
+    full = None
+    for _ in range(2):  # warm-up, then the timed call
+        kms.clear()
+        full = kh_sharded(compute, sp if rank == 0 else None, sn if rank == 0 else None,
+                          q_in, f_in, rp, dist=dist, device=device)
+    k_ms = reduce_max(kms[-1], dist, device)
+    flop = 64.0 * KH_NS * KH_NR * KH_NT
+    b, e = target_block(KH_NR, rank, world)
+    return {"workload": "the KH section's workload, targets split across ranks (rank 0 "
+                        "broadcasts the surface traces once, blocks all-gathered)",
+            "value": flop / (k_ms / 1e3) / 1e12, "unit": "TFLOP/s", "kernel_ms_max": k_ms,
+            "targets_per_rank": e - b, "result_shape": list(full.shape)}
+
+
 # ---------------------------------------------------------------------------
 # Serving: Poisson stream of mixed GF solves, batched server vs plain path
 # ---------------------------------------------------------------------------
@@ -636,6 +675,8 @@ def b200_arm(args):
     extra = {}
     if world == 1 and not args.no_kh:
         extra["kh"] = kh_section(A, ctx, steps=3, warmup=1)
+    if world > 1 and not args.no_kh:  # every rank takes part in the collectives
+        extra["kh_sharded"] = kh_sharded_section(A, ctx, dist, f"cuda:{local}")
     if world == 1 and not args.no_gf:
         gf_section(A, ctx, nt=40)  # warm-up: graphs, pool blocks
         extra["gf_map"] = gf_section(A, ctx)
