@@ -147,6 +147,11 @@ SIGNATURES = [
                                   C.c_void_p]),
     ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("adf_kh_test_fault", C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    ("adf_run_fdtd_kh", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_void_p,
+                                  C.POINTER(TxGridC), C.POINTER(CpmlC), C.c_void_p, C.c_int64,
+                                  C.c_int64, C.c_int, C.POINTER(KhDescC), C.c_void_p,
+                                  C.c_void_p]),
+    ("adf_last_kh_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("adf_static_cpml_max_npml", C.c_int, []),
     ("adf_gf_postprocess", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                      C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p,

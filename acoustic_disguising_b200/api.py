@@ -60,6 +60,12 @@ class Context:
         L.check(L.lib().adf_last_timing(self.h, C.byref(ms), C.byref(n)), "adf_last_timing")
         return ms.value, n.value
 
+    def last_kh_ms(self) -> float:
+        """Kernel time of the last KH extrapolation on this context."""
+        ms = C.c_double()
+        L.check(L.lib().adf_last_kh_ms(self.h, C.byref(ms)), "adf_last_kh_ms")
+        return ms.value
+
 
 def default_context() -> Context:
     global _ctx
@@ -437,6 +443,44 @@ def run_fdtd(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | 
                                  int(start_step), stop_step, L.ARITH[arith], cb, None),
             "run_fdtd")
     return field
+
+
+def run_fdtd_kh(d: L.Domain, field: np.ndarray, txs: TransceiverGrid, cpml: Cpml | None,
+                va, surface_cols, s_pts, s_nrm, r_pts, sigma: float, aq: float, af: float,
+                nt: int | None = None, window_sigmas: float = 6.0, arith: str = "promote",
+                ctx: Context | None = None, out: np.ndarray | None = None) -> np.ndarray:
+    """build_hologram's run_fdtd! followed by the two-way KH pressure of its
+    recorded shell (part3_kh_extrapolation.jl:168-185) in one call:
+    out[t, r] = aq sum_s p_p(s,r) (*) vn[:, s] + af sum_s p_v(s,r) (*) p[:, s]
+    over the transceivers `surface_cols` (1-based; s_pts, s_nrm their points
+    and outward normals), targets r_pts, rows 1..nt (default dom.nt).  The
+    traces stay in HBM between the two.  `field`, `txs` and `cpml` are
+    advanced in place as by run_fdtd.  Returns out (nt, nr) Float32."""
+    ctx = ctx or default_context()
+    if field.dtype != np.float32 or not field.flags.f_contiguous:
+        raise ValueError("field must be a Fortran-ordered float32 array")
+    if field.shape != (d.nx, d.ny, d.nz, 4):
+        raise ValueError("field shape must be (nx, ny, nz, 4)")
+    nt = int(d.nt) if nt is None else int(nt)
+    cols = np.ascontiguousarray(surface_cols, np.int64)
+    sp = np.asfortranarray(s_pts, np.float64)
+    sn = np.asfortranarray(s_nrm, np.float64)
+    rp = np.asfortranarray(r_pts, np.float64)
+    ns, nr = sp.shape[0], rp.shape[0]
+    if cols.shape != (ns,) or sn.shape != (ns, 3) or rp.shape[1] != 3:
+        raise ValueError("run_fdtd_kh: shape mismatch")
+    desc = L.KhDescC(ns=ns, nr=nr, nt=nt, dt=d.dt, sigma=sigma, c0=d.c0, rho=d.r0, aq=aq, af=af,
+                     window_sigmas=window_sigmas, s_pts=sp.ctypes.data, s_nrm=sn.ctypes.data,
+                     r_pts=rp.ctypes.data)
+    out = _kh_out(out, nt, nr, "run_fdtd_kh")
+    mask = None if va is None else np.asfortranarray(va, dtype=np.uint8)
+    cg = txs._c()
+    cc = cpml._c() if cpml is not None else None
+    L.check(L.lib().adf_run_fdtd_kh(ctx.h, C.byref(d), _p(field), C.byref(cg),
+                                    C.byref(cc) if cc is not None else None, _p(mask), 1,
+                                    int(d.nt), L.ARITH[arith], C.byref(desc), _p(cols), _p(out)),
+            "run_fdtd_kh")
+    return out
 
 
 def injection_coefficients(d: L.Domain, radius: float, n_points: int,

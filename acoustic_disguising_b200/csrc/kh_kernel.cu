@@ -431,10 +431,43 @@ __global__ void adf_kh_interleave_kernel(const float* q, const float* f, float2*
     qf[i] = make_float2(q[i], f[i]);
 }
 
+// Columns cols[s] of two [nt][ntx] trace arrays in HBM (a solve's recorded
+// v_n and p, transceiver fastest) into the zero-padded KH input columns
+// dq[s][pad + t], df[s][pad + t]: a 32 x 32 tiled transpose per array.
+__global__ void adf_kh_gather_kernel(const float* q, const float* f, int ntx, int nt,
+                                     const int* cols, int ns, float* dq, float* df,
+                                     long long pitch, int pad) {
+  __shared__ float tq[32][33], tf[32][33];
+  const int s0 = blockIdx.x * 32, t0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {  // rows t, columns s: coalesced reads
+    const int t = t0 + i, sl = s0 + threadIdx.x;
+    float a = 0.f, b = 0.f;
+    if (t < nt && sl < ns) {
+      const long long o = (long long)t * ntx + cols[sl];
+      a = q[o];
+      b = f[o];
+    }
+    tq[i][threadIdx.x] = a;
+    tf[i][threadIdx.x] = b;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {  // rows s, samples t: coalesced writes
+    const int sl = s0 + i, t = t0 + threadIdx.x;
+    if (sl < ns && t < nt) {
+      dq[(long long)sl * pitch + pad + t] = tq[threadIdx.x][i];
+      df[(long long)sl * pitch + pad + t] = tf[threadIdx.x][i];
+    }
+  }
+}
+
+// in_q / in_f either host arrays (nt, ns) or, with `dev`, columns of
+// device-resident traces (pressure only).
 static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const float* in_f,
-                  float* out, int kind) {
-  if (!ctx || !d || !in_q || !in_f || !out || !d->s_pts || !d->s_nrm || !d->r_pts)
+                  float* out, int kind, const KhDevSrc* dev = nullptr) {
+  if (!ctx || !d || (!dev && (!in_q || !in_f)) || !out || !d->s_pts || !d->s_nrm || !d->r_pts)
     return fail(ADF_E_ARG, "adf_kh_pressure: null argument");
+  if (dev && (kind != 0 || !dev->q || !dev->f || !dev->cols || dev->ntx < 1))
+    return fail(ADF_E_ARG, "KH from device traces: pressure only, traces and columns required");
   if (kind == 1 && (!d->r_nrm || !(d->rho > 0)))
     return fail(ADF_E_ARG, "adf_kh_velocity: target normals and a positive rho are required");
   if (d->ns < 1 || d->nr < 1 || d->nt < 1 || !(d->dt > 0) || !(d->sigma > 0) || !(d->c0 > 0))
@@ -543,10 +576,16 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   cudaMemcpyAsync(drp.p, d->r_pts, (size_t)24 * nr, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(dq.p, 0, (size_t)4 * pitch * ns, st);
   cudaMemsetAsync(df.p, 0, (size_t)4 * pitch * ns, st);
-  cudaMemcpy2DAsync(dq.p + pad, (size_t)4 * pitch, in_q, (size_t)4 * nt, (size_t)4 * nt, ns,
-                    cudaMemcpyHostToDevice, st);
-  cudaMemcpy2DAsync(df.p + pad, (size_t)4 * pitch, in_f, (size_t)4 * nt, (size_t)4 * nt, ns,
-                    cudaMemcpyHostToDevice, st);
+  if (dev) {
+    const dim3 gg((unsigned)((ns + 31) / 32), (unsigned)((nt + 31) / 32));
+    adf_kh_gather_kernel<<<gg, dim3(32, 8), 0, st>>>(dev->q, dev->f, dev->ntx, nt, dev->cols, ns,
+                                                      dq.p, df.p, pitch, pad);
+  } else {
+    cudaMemcpy2DAsync(dq.p + pad, (size_t)4 * pitch, in_q, (size_t)4 * nt, (size_t)4 * nt, ns,
+                      cudaMemcpyHostToDevice, st);
+    cudaMemcpy2DAsync(df.p + pad, (size_t)4 * pitch, in_f, (size_t)4 * nt, (size_t)4 * nt, ns,
+                      cudaMemcpyHostToDevice, st);
+  }
   adf_kh_interleave_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dq.p, df.p,
                                                          reinterpret_cast<float2*>(dqf.p),
                                                          (long long)pitch * ns);
@@ -609,14 +648,21 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   ctx->last_ms = ms;
+  ctx->kh_ms = ms;
   ctx->launches = 1;
   ctx->h2d_bytes = (int64_t)48 * ns + (kind ? 48 : 24) * (int64_t)nr +
-                   (int64_t)(kind ? 12 : 8) * nt * ns;
+                   (dev ? 0 : (int64_t)(kind ? 12 : 8) * nt * ns);
   ctx->d2h_bytes = (int64_t)4 * nt * nr;
   if (herr & 2) return fail(ADF_E_TIMEOUT, "KH: a bounded wait for a staged chunk gave up");
   if (herr) return fail(ADF_E_STATE, "KH: a pair's delay fell outside its tile bound");
   return ADF_OK;
 }
+
+namespace adf {
+int kh_pressure_dev(adf_ctx* ctx, const adf_kh_desc* d, const KhDevSrc& src, float* out) {
+  return kh_run(ctx, d, nullptr, nullptr, out, 0, &src);
+}
+}  // namespace adf
 
 extern "C" int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q,
                                const float* in_f, float* out) {

@@ -962,11 +962,29 @@ int adf_pack_transceivers(const adf_domain* d, const double* points, const doubl
   return pack_transceivers_host(to_dom(*d), points, dirs, tf, o);
 }
 
+// The KH extrapolation that follows a run on the recorded traces of some of
+// its transceivers (adf_run_fdtd_kh), or none.
+struct KhAfter {
+  const adf_kh_desc* desc = nullptr;
+  const int64_t* cols = nullptr;  // 1-based transceiver indices, desc->ns of them
+  float* out = nullptr;
+};
+
 static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
                          adf_cpml* cpml, const uint8_t* mask, int64_t start_step,
                          int64_t stop_step, int flags, const adf_gfmap* gf, adf_step_cb cb,
-                         void* user) {
+                         void* user, const KhAfter& kh = KhAfter()) {
   if (!ctx || !d || !field || !txs) return fail(ADF_E_ARG, "NULL argument");
+  if (kh.desc) {
+    if (!kh.cols || !kh.out) return fail(ADF_E_ARG, "KH: surface columns and output required");
+    if (kh.desc->nt < 1 || kh.desc->nt > stop_step)
+      return fail(ADF_E_ARG, "KH: nt must lie in 1..stop_step (recorded rows)");
+    if (!(std::fabs(kh.desc->dt - d->dt) <= 1e-12 * d->dt))
+      return fail(ADF_E_ARG, "KH: dt must equal the domain's time step");
+    for (int64_t k = 0; k < kh.desc->ns; ++k)
+      if (kh.cols[k] < 1 || kh.cols[k] > txs->ntx)
+        return fail(ADF_E_ARG, "KH: surface column outside 1..ntx");
+  }
   const bool use_gf = gf && !gf->discard;
   int ntens = 0;
   if (gf) {
@@ -1187,6 +1205,21 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   ctx->last_ms = ms;
   ctx->cur = nullptr;
   if (rc) return rc;
+  if (kh.desc) {  // KH on the recorded v_n (monopole) and p (dipole) columns, in HBM
+    std::vector<int> c0((size_t)kh.desc->ns);
+    for (int64_t k = 0; k < kh.desc->ns; ++k) c0[(size_t)k] = (int)(kh.cols[k] - 1);
+    int* dcols = solve_dalloc<int>(*s, c0.size(), rc);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(dcols, c0.data(), c0.size() * 4, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADF_E_DEVICE, "KH column upload failed");
+    }
+    KhDevSrc src{sd.vn_rec, sd.rec[0], sd.ntx, dcols};
+    rc = kh_pressure_dev(ctx, kh.desc, src, kh.out);
+    ctx->last_ms = ms;  // the run's own time; KH's is ctx->kh_ms
+    if (rc) return rc;
+  }
   // output buffer of the last executed step
   const int fb = (int)((stop_step - start_step + 1) & 1);
   cudaMemcpy2D(field, (size_t)d->nx * 4, sd.field + (size_t)fb * sd.buf_stride,
@@ -1210,6 +1243,24 @@ int adf_run_fdtd(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* tx
                  int flags, adf_step_cb cb, void* user) {
   return run_fdtd_impl(ctx, d, field, txs, cpml, mask, start_step, stop_step, flags, nullptr,
                        cb, user);
+}
+
+int adf_run_fdtd_kh(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                    adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                    int flags, const adf_kh_desc* kh, const int64_t* kh_cols, float* kh_out) {
+  if (!kh) return fail(ADF_E_ARG, "NULL KH descriptor");
+  KhAfter a;
+  a.desc = kh;
+  a.cols = kh_cols;
+  a.out = kh_out;
+  return run_fdtd_impl(ctx, d, field, txs, cpml, mask, start_step, stop_step, flags, nullptr,
+                       nullptr, nullptr, a);
+}
+
+int adf_last_kh_ms(adf_ctx* ctx, double* ms) {
+  if (!ctx || !ms) return fail(ADF_E_ARG, "bad arguments");
+  *ms = ctx->kh_ms;
+  return ADF_OK;
 }
 
 int adf_run_fdtd_gf(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,

@@ -27,6 +27,7 @@ struct adf_ctx {
   struct adf::Solve* cur = nullptr;  // solve whose field adf_read_field reads
   int64_t cur_it = 0;
   double last_ms = 0.0;
+  double kh_ms = 0.0;  // kernel time of the last KH extrapolation
   int64_t launches = 0;
   // per-launch timing of the step kernel
   int64_t h2d_bytes = 0, d2h_bytes = 0;  // traffic of the last call
@@ -129,6 +130,17 @@ int build_mask_device(adf_ctx* ctx, const adf_domain& d, int shape, const double
                       uint32_t** bits, uint8_t** jl);
 int pack_transceivers_host(const hm::Dom& d, const double* points, const double* dirs,
                            const double* tf, adf_txgrid* o);
+
+// KH pressure on columns of device-resident traces (kh_kernel.cu): q and f
+// are [nt][ntx] arrays in HBM (a solve's vn_rec and p_rec), cols the ns
+// 0-based columns in device memory; out (nt, nr) on the host.
+struct KhDevSrc {
+  const float* q;
+  const float* f;
+  int ntx;
+  const int* cols;
+};
+int kh_pressure_dev(adf_ctx* ctx, const adf_kh_desc* d, const KhDevSrc& src, float* out);
 
 // kernels (fdtd_kernels.cu)
 cudaError_t launch_advance(SolveDev* solves, int n, int by, cudaStream_t s);

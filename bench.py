@@ -31,6 +31,9 @@ time step over all of their tiles, graph-captured), and the p / v_n traces copie
           step counts (500..3000) and scatterers, offered at 1.5x the plain
           path's capacity: p50/p99 latency and solves/s of the continuous-
           batching server against the plain one-solve-at-a-time path
+  hologram512 : the 512^3 hologram run (12-cell CPML, ellipsoid, C_f/C_q
+          injection at 8192 points, 8192-point shell, 4000 steps) and the KH
+          pressure of its shell to 16384 targets, through adf_run_fdtd_kh
   parity : the first solve of the workload over its first 200 steps against
           the oracle in the same arithmetic and against the oracle's FP64 run
           (relative L2 of the p and v_n traces), outside the timed region
@@ -96,6 +99,10 @@ def parse():
     ap.add_argument("--no-step512", action="store_true", help="skip the 512^3 step section")
     ap.add_argument("--no-gf", action="store_true", help="skip the in-loop GF section")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity section")
+    ap.add_argument("--no-hologram", action="store_true", help="skip the 512^3 hologram section")
+    ap.add_argument("--hologram-only", action="store_true",
+                    help="run only the 512^3 hologram section and print it (profiling runs)")
+    ap.add_argument("--hologram-nt", type=int, default=H_NT)
     ap.add_argument("--serving-requests", type=int, default=20)
     ap.add_argument("--serving-resident", type=int, default=2,
                     help="server slot limit (0: HBM budget only)")
@@ -551,6 +558,82 @@ def step512_section(A, ctx, nt=48, tune=True):
 
 
 # ---------------------------------------------------------------------------
+# Hologram synthesis at 512^3: distributed C_f/C_q injection at 8192 points,
+# an 8192-point recording shell, 4000 steps, then KH to 16384 targets
+# ---------------------------------------------------------------------------
+H_N, H_NPML, H_NT = 512, 12, 4000
+H_NIN, H_RIN, H_NOUT, H_ROUT = 8192, 100 * DX, 8192, 130 * DX
+H_SEMI = (80 * DX, 60 * DX, 40 * DX)
+H_NR, H_RT, H_F3DB, H_SEED = 16384, 2.0, 20e3, 20261204
+
+
+def hologram_section(A, ctx, nt=H_NT):
+    """build_hologram's run at the large size, end to end through the C-ABI:
+    transceivers packed as build_txs does (shell first, then the injection
+    surface, directions [0, n]), inner sources p_src = C_q vn and vn_src =
+    C_f p (inject_inner_sources!) from seeded band-limited noise traces,
+    run_fdtd! over `nt` steps, then the two-way KH pressure of the recorded
+    shell to 16384 targets on a 2 m sphere, the traces handed over in HBM."""
+    d = A.Domain(tmax=tmax_of(nt), xmax=(H_N - 1) * DX / 2, nx=H_N, c0=C0, r0=RHO, cf=0.5)
+    op, on = A.fibonacci_sphere(H_NOUT, H_ROUT)
+    ip, inn = A.fibonacci_sphere(H_NIN, H_RIN)
+    zero = np.zeros(d.nt)
+    txs = [A.Transceiver(op[k], np.r_[0.0, on[k]], zero) for k in range(H_NOUT)]
+    txs += [A.Transceiver(ip[k], np.r_[0.0, inn[k]], zero) for k in range(H_NIN)]
+    g = A.transceivers_to_grid(d, txs)
+    cf_, cq_, _ = A.injection_coefficients(d, H_RIN, H_NIN, ctx=ctx)
+    rng = np.random.default_rng(H_SEED)
+    p_tr = ricker_noise(rng, nt, H_NIN, d.dt, 2000.0)   # stand-ins for GF-convolved signals
+    vn_tr = ricker_noise(rng, nt, H_NIN, d.dt, 2000.0) / (RHO * C0)
+    inner = slice(H_NOUT, H_NOUT + H_NIN)
+    g.vn_src[:, inner] = cf_ * p_tr
+    g.src[0][:, inner] = cq_ * vn_tr
+    cp = A.Cpml(d, H_NPML, 1e-4, PML_FC, ctx=ctx)
+    m = A.build_update_mask(d, "ellipsoid", ctx=ctx, semi_axes=H_SEMI)
+    f = np.zeros((H_N, H_N, H_N, 4), np.float32, order="F")
+    rp, _ = A.fibonacci_sphere(H_NR, H_RT)
+    sigma = math.sqrt(math.log(2.0)) / (2 * math.pi * H_F3DB)
+    dS = 4 * math.pi * H_ROUT ** 2 / H_NOUT
+    cols = np.arange(1, H_NOUT + 1, dtype=np.int64)
+    ctx.set_kernel_timing(True)
+    ctx.kernel_timing(reset=True)
+    t0 = time.perf_counter()
+    out = A.run_fdtd_kh(d, f, g, cp, m, cols, op, on, rp, sigma, -RHO * dS * d.dt, -dS * d.dt,
+                        ctx=ctx)
+    wall = time.perf_counter() - t0
+    k_ms, k_n = ctx.kernel_timing(reset=True)
+    ctx.set_kernel_timing(False)
+    run_ms, _ = ctx.last_timing()
+    kh_ms = ctx.last_kh_ms()
+    per = k_ms / max(k_n, 1)
+    byt = algorithmic_bytes_per_solve_step(H_N, H_NPML)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs") or 6650.0
+    taps = math.ceil(12 * sigma / d.dt)
+    flop = 4.0 * taps * H_NOUT * H_NR * nt  # 2 channels x taps x 2 FLOP per pair-sample
+    gbs = byt / (per / 1e3) / 1e9
+    return {"workload": f"512^3 (dx=5 mm air), 12-cell CPML, rigid ellipsoid 80/60/40 cells; "
+                        f"C_f/C_q injection at {H_NIN} Fibonacci points r=100 cells (seeded "
+                        f"band-limited noise traces), {H_NOUT}-point shell r=130 cells, {nt} "
+                        f"steps; KH pressure of the shell to {H_NR} targets on a 2 m sphere "
+                        f"(f_3db 20 kHz, {taps} taps)",
+            "wall_s": wall, "run_ms": run_ms, "gcell_upd_per_s": H_N ** 3 * nt / run_ms / 1e6,
+            "step_kernel": {"mean_launch_ms": per, "launches": k_n,
+                            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak,
+                                         "unit": "GB/s", "frac": gbs / peak,
+                                         "frac_of_nominal_8000": gbs / 8000.0,
+                                         "bytes_per_launch": byt}},
+            "kh": {"kernel_ms": kh_ms, "tflops": flop / (kh_ms / 1e3) / 1e12,
+                   "flop": flop, "traces": "recorded shell, handed over in HBM"},
+            "shell_p_rms": float(np.sqrt(np.mean(g.rec[0][:, :H_NOUT].astype(np.float64) ** 2))),
+            "kh_out_rms": float(np.sqrt(np.mean(out.astype(np.float64) ** 2)))}
+
+
+# ---------------------------------------------------------------------------
 # In-loop GF extrapolation (run_fdtd! gf_map = PVFromPin) on a 128^3 run
 # ---------------------------------------------------------------------------
 def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
@@ -682,6 +765,8 @@ def b200_arm(args):
         extra["gf_map"] = gf_section(A, ctx)
     if world == 1 and not args.no_step512:
         extra["step512"] = step512_section(A, ctx)
+    if world == 1 and not args.no_hologram:
+        extra["hologram512"] = hologram_section(A, ctx)
     if world == 1 and not args.no_serving:
         extra["serving"] = serving_section(A, ctx, args.serving_requests,
                                            args.serving_resident)
@@ -762,6 +847,17 @@ def kh_only(args):
     return 0
 
 
+def hologram_only(args):
+    import acoustic_disguising_b200 as A
+
+    if not os.path.exists(A.LIB_PATH):
+        A.build()
+    ctx = A.Context(0)
+    print(json.dumps({"hologram512": hologram_section(A, ctx, nt=args.hologram_nt)}), flush=True)
+    ctx.close()
+    return 0
+
+
 def gf_only(args):
     import acoustic_disguising_b200 as A
 
@@ -782,6 +878,8 @@ def main():
         return kh_only(args)
     if args.gf_only:
         return gf_only(args)
+    if args.hologram_only:
+        return hologram_only(args)
     return b200_arm(args)
 
 

@@ -314,6 +314,23 @@ int adf_kh_pressure(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
 int adf_kh_velocity(adf_ctx* ctx, const adf_kh_desc* desc, const float* in_q,
                     const float* in_f, float* out);
 
+/* Hologram synthesis and its extrapolation in one call: build_hologram's
+ * run_fdtd! (src/hologram.jl:141, 248) with a distributed C_f / C_q
+ * injection already written into txs's sources
+ * (diagnostics/_check_inject_kh/fdtd_runners.jl:39-45), followed by the
+ * two-way KH pressure of part3_kh_extrapolation.jl:168-185 on the recorded
+ * shell: in_q = the v_n traces and in_f = the p traces of the transceivers
+ * kh_cols[0..kh->ns-1] (1-based), rows 1..kh->nt.  Everything of
+ * adf_run_fdtd is returned as there; the recorded traces go from HBM into
+ * the KH kernel without a host round trip.  kh->dt must equal d->dt and
+ * kh->nt <= stop_step; kh_out is (kh->nt, kh->nr) Float32.                 */
+int adf_run_fdtd_kh(adf_ctx* ctx, const adf_domain* d, float* field, adf_txgrid* txs,
+                    adf_cpml* cpml, const uint8_t* mask, int64_t start_step, int64_t stop_step,
+                    int flags, const adf_kh_desc* kh, const int64_t* kh_cols, float* kh_out);
+/* Kernel time (ms) of the last KH extrapolation on ctx; a measurement
+ * helper with no reference counterpart.                                   */
+int adf_last_kh_ms(adf_ctx* ctx, double* ms);
+
 /* Measured FP32 FMA throughput of the device (TFLOP/s, 2 FLOP per FMA): the
  * roofline denominator of adf_kh_pressure.  Measurement helper with no
  * reference counterpart; ms (optional) receives the probe's duration.      */
