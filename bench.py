@@ -273,9 +273,12 @@ def parity_section(A, ctx, steps=200, arith="promote"):
     O.run_fdtd64(d, f64, g64, O.CpmlState64(d, NPML, 1e-4, PML_FC), m)
     del f64
     fp64 = {"p": rel(req.p, g64.rec[0][:, 1:]), "vn": rel(req.vn, g64.vn_rec[:, 1:])}
+    ref64 = {"p": rel(g.rec[0][:, 1:], g64.rec[0][:, 1:]),
+             "vn": rel(g.vn_rec[:, 1:], g64.vn_rec[:, 1:])}
     return {"workload": f"source 0 of the headline workload, first {steps} of its {NT} steps, "
                         "p and v_n traces of the 2048-point shell",
             f"rel_l2_vs_{arith}_oracle": same, "rel_l2_vs_fp64_oracle": fp64,
+            f"{arith}_oracle_rel_l2_vs_fp64_oracle": ref64,
             "tolerance": 1e-5, "pass": max(same.values()) <= 1e-5}
 
 

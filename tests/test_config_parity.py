@@ -33,8 +33,17 @@ pytestmark = pytest.mark.gpu
 DX = 0.005
 C0, RHO = 343.0, 1.2
 DT = 0.5 * DX / C0 / np.sqrt(3.0)
-TOL = 1e-5        # trace / field bar against the oracle in the same arithmetic
-FP64_BOUND = 1e-3  # sanity bound of the stated FP64 errors (Float32 storage)
+TOL = 1e-5  # trace / field bar against the oracle in the same arithmetic
+
+
+def no_worse_than_reference(e64, e64_ref):
+    """The GPU's error against the FP64 run stays within that of the
+    reference arithmetic (the promote oracle, Float32 storage) against the
+    same run: the stated error is the storage precision's, not the kernel's.
+    (Late in a run the field has decayed to a residual whose Float32
+    rounding is large relative to its norm; the traces stay near 1e-7.)"""
+    bad = {k: (v, e64_ref[k]) for k, v in e64.items() if not v <= 1.05 * e64_ref[k] + 1e-7}
+    assert not bad, f"GPU less accurate than the reference arithmetic: {bad}"
 
 
 def rel_l2(a, b):
@@ -113,13 +122,13 @@ def test_plain_solve_96cube_800_steps(adf, oracle, ctx):
     f64 = np.zeros((n, n, n, 4), np.float64, order="F")
     oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, npml, 1e-4, 2000.0), None)
     e64 = {**trace_errors(g, g64), **field_errors(f, f64)}
-    e64_oracle = trace_errors(go, g64)  # the promote oracle itself against FP64
+    e64_oracle = {**trace_errors(go, g64), **field_errors(fo, f64)}  # the reference arithmetic
     record("96^3 plain solve, 800 steps", vs_promote=errs, vs_fp64=e64,
            promote_oracle_vs_fp64=e64_oracle)
     assert np.abs(go.rec[0][:, 1:]).max() > 0 and np.abs(co.mv[0]).max() > 0
     bad = {k: v for k, v in errs.items() if not v <= TOL}
     assert not bad, f"against the promote oracle: {bad}; all {errs}"
-    assert max(e64.values()) < FP64_BOUND, e64
+    no_worse_than_reference(e64, e64_oracle)
 
 
 def gf_request(adf, d, n_rec=2048):
@@ -160,12 +169,13 @@ def test_gf_solve_256cube_shell_2048(adf, oracle, ctx):
     oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, 10, 1e-4, 2000.0), mo)
     del f64
     e64 = {"p": rel_l2(req.p, g64.rec[0][:, 1:]), "vn": rel_l2(req.vn, g64.vn_rec[:, 1:])}
+    e64_oracle = {"p": rel_l2(go.rec[0][:, 1:], g64.rec[0][:, 1:]),
+                  "vn": rel_l2(go.vn_rec[:, 1:], g64.vn_rec[:, 1:])}
     record("256^3 GF solve, 2048-point shell, 400 steps", vs_promote=errs, vs_fp64=e64,
-           promote_oracle_vs_fp64={"p": rel_l2(go.rec[0][:, 1:], g64.rec[0][:, 1:]),
-                                   "vn": rel_l2(go.vn_rec[:, 1:], g64.vn_rec[:, 1:])})
+           promote_oracle_vs_fp64=e64_oracle)
     assert np.abs(go.rec[0][:, 1:]).max() > 0
     assert max(errs.values()) <= TOL, errs
-    assert max(e64.values()) < FP64_BOUND, e64
+    no_worse_than_reference(e64, e64_oracle)
 
 
 def test_hologram_grid_512cube_ellipsoid(adf, oracle, ctx):
@@ -193,11 +203,12 @@ def test_hologram_grid_512cube_ellipsoid(adf, oracle, ctx):
     for a in range(3):
         errs[f"mv{a}"] = rel_l2(cp.mv[a], co.mv[a])
         errs[f"mp{a}"] = rel_l2(cp.mp[a], co.mp[a])
-    del fo
     g64 = oracle.transceivers_to_grid64(o, pts, dirs, tfs)
     oracle.run_fdtd64(o, f64, g64, oracle.CpmlState64(o, npml, 1e-4, 2000.0), mo)
     e64 = {**trace_errors(g, g64), **field_errors(f, f64)}
-    record("512^3 ellipsoid, random initial field, 20 steps", vs_promote=errs, vs_fp64=e64)
+    e64_oracle = {**trace_errors(go, g64), **field_errors(fo, f64)}
+    record("512^3 ellipsoid, random initial field, 20 steps", vs_promote=errs, vs_fp64=e64,
+           promote_oracle_vs_fp64=e64_oracle)
     bad = {k: v for k, v in errs.items() if not v <= TOL}
     assert not bad, f"against the promote oracle: {bad}; all {errs}"
-    assert max(e64.values()) < FP64_BOUND, e64
+    no_worse_than_reference(e64, e64_oracle)
