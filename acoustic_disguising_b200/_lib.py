@@ -139,6 +139,8 @@ SIGNATURES = [
     ("adf_server_poll", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int),
                                   C.POINTER(C.c_double)]),
     ("adf_server_cancel", C.c_int, [C.c_void_p, C.c_int64]),
+    ("adf_server_set_work_cap", C.c_int, [C.c_void_p, C.c_int64]),
+    ("adf_step_resident_ctas", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("adf_server_drain", C.c_int, [C.c_void_p]),
     ("adf_server_stop", C.c_int, [C.c_void_p]),
     ("adf_kh_pressure", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,

@@ -60,6 +60,12 @@ class Context:
         L.check(L.lib().adf_last_timing(self.h, C.byref(ms), C.byref(n)), "adf_last_timing")
         return ms.value, n.value
 
+    def step_resident_ctas(self) -> int:
+        """Step-kernel CTAs the GPU holds at once (one wave)."""
+        n = C.c_int64()
+        L.check(L.lib().adf_step_resident_ctas(self.h, C.byref(n)), "step_resident_ctas")
+        return n.value
+
     def last_kh_ms(self) -> float:
         """Kernel time of the last KH extrapolation on this context."""
         ms = C.c_double()
@@ -744,13 +750,21 @@ def impulsive_gfs(d: L.Domain, src_positions, src_normals, rec_positions, rec_no
 class Server:
     """Continuous-batching serving loop (adf_server_*)."""
 
-    def __init__(self, hbm_budget: int = 0, max_resident: int = 0, ctx: Context | None = None):
+    def __init__(self, hbm_budget: int = 0, max_resident: int = 0, ctx: Context | None = None,
+                 work_waves: float = 0.0):
+        """work_waves > 0 admits requests only while the resident solves' step
+        work stays within that many waves of the GPU's resident CTAs
+        (adf_server_set_work_cap); 0 = HBM budget and max_resident only."""
         self.ctx = ctx or default_context()
         h = C.c_void_p()
         L.check(L.lib().adf_server_start(self.ctx.h, hbm_budget, max_resident, C.byref(h)),
                 "server_start")
         self.h = h
         self._keep = {}
+        self.work_cap = 0
+        if work_waves > 0:
+            self.work_cap = int(work_waves * self.ctx.step_resident_ctas())
+            L.check(L.lib().adf_server_set_work_cap(self.h, self.work_cap), "server_set_work_cap")
 
     def submit(self, req: GfRequest) -> int:
         rc = req._c()

@@ -117,6 +117,7 @@ struct EpiParams {
 cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t s);
 int step_max_ty();
 int step_x_tile();  // cells per x tile of a step work item
+cudaError_t step_ctas_per_sm(int* n);  // resident step-kernel CTAs per SM (occupancy)
 cudaError_t launch_epilogue(const EpiParams& p, int max_ntx, cudaStream_t s);
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc, bool reduce,
                                   cudaStream_t s);

@@ -1067,6 +1067,10 @@ cudaError_t launch_step(const StepParams& p, int grid, int max_ty, cudaStream_t 
 }
 
 int step_max_ty() { return kMaxTy; }
+cudaError_t step_ctas_per_sm(int* n) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, adf_fdtd_step_kernel, kStepThreads,
+                                                       kStepDynSmem);
+}
 int step_x_tile() { return kXT; }
 
 cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_nsrc, bool reduce,

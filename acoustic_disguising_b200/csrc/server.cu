@@ -63,7 +63,17 @@ struct GfJob {
   bool cancel = false;
   std::unique_ptr<Solve> solve;
   size_t est = 0;
+  long long items = 0;  // step-kernel work items (CTAs per step launch)
 };
+
+// Work items one step launch runs for this request's grid (as solve_finalize
+// builds them: x tiles x y tiles x z chunks).
+static long long gf_items(const adf_gf_request& r) {
+  int nxp, ty, nzc, mw;
+  choose_tiles((int)r.dom.nx, (int)r.dom.ny, (int)r.dom.nz, nxp, ty, nzc, mw);
+  const long long xt = step_x_tile();
+  return (nxp + xt - 1) / xt * ((r.dom.ny + ty - 1) / ty) * ((r.dom.nz + nzc - 1) / nzc);
+}
 
 static size_t gf_bytes(const adf_gf_request& r) {
   int nxp, ty, nzc, mw;
@@ -219,6 +229,9 @@ class Engine {
       : ctx_(ctx), budget_(budget), max_resident_(max_resident), chunk_(chunk) {}
 
   void enqueue(GfJob* j) { pending_.push_back(j); }
+  // Admission by work: a request joins only while the resident solves' step
+  // work items stay within max_items (one solve is always admitted); 0 = no cap.
+  void set_work_cap(long long max_items) { max_items_.store(max_items); }
   bool idle() const { return pending_.empty() && resident_.empty(); }
   size_t resident() const { return resident_.size(); }
 
@@ -268,6 +281,9 @@ class Engine {
         continue;
       }
       if (used_ + j->est > budget_) break;  // wait for memory to free up
+      if (!j->items) j->items = gf_items(j->req);
+      const long long cap = max_items_.load();
+      if (cap > 0 && !resident_.empty() && items_ + j->items > cap) break;  // GPU full
       pending_.pop_front();
       int rc = gf_setup(ctx_, *j);
       if (rc) {
@@ -278,6 +294,7 @@ class Engine {
         continue;
       }
       used_ += j->est;
+      items_ += j->items;
       j->status = 1;
       resident_.push_back(j);
       dirty_ = true;
@@ -292,6 +309,7 @@ class Engine {
         int rc = j->cancel ? ADF_E_CANCELLED : gf_extract(ctx_, *j);
         j->solve.reset();
         used_ -= j->est;
+        items_ -= j->items;
         j->status = rc ? rc : 2;
         j->t_done = std::chrono::steady_clock::now();
         finished->push_back(j);
@@ -308,6 +326,8 @@ class Engine {
   int max_resident_;
   int chunk_;
   size_t used_ = 0;
+  std::atomic<long long> max_items_{0};
+  long long items_ = 0;
   std::deque<GfJob*> pending_;
   std::vector<GfJob*> resident_;
   Batch batch_;
@@ -440,6 +460,21 @@ int adf_server_start(adf_ctx* ctx, size_t hbm_budget, int max_resident, adf_serv
   s->eng.reset(new Engine(ctx, budget, max_resident > 0 ? max_resident : 1 << 20, kGraphChunk));
   s->th = std::thread(server_loop, s);
   *out = s;
+  return ADF_OK;
+}
+
+int adf_server_set_work_cap(adf_server* s, int64_t max_items) {
+  if (!s || max_items < 0) return fail(ADF_E_ARG, "adf_server_set_work_cap: bad arguments");
+  s->eng->set_work_cap((long long)max_items);
+  return ADF_OK;
+}
+
+int adf_step_resident_ctas(adf_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return fail(ADF_E_ARG, "NULL argument");
+  int per_sm = 0;
+  const cudaError_t e = step_ctas_per_sm(&per_sm);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  *n = (int64_t)per_sm * ctx->nsm;
   return ADF_OK;
 }
 

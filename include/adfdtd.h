@@ -273,6 +273,14 @@ typedef struct adf_server adf_server;
 int adf_server_start(adf_ctx* ctx, size_t hbm_budget, int max_resident, adf_server** out);
 /* The request's pointers (src_tf, points, outputs) must stay valid until the
  * request completes.  *id receives a request id.                          */
+/* Admission by work, with no reference counterpart: a queued request joins
+ * only while the resident solves' step-kernel work items (CTAs per step
+ * launch) stay within max_items, so that each step launch keeps the GPU
+ * full without spreading it over more solves than that needs; one solve is
+ * always admitted.  0 (the default) = HBM budget and slot count only.
+ * adf_step_resident_ctas gives the CTAs the GPU runs at once (one wave).  */
+int adf_server_set_work_cap(adf_server* s, int64_t max_items);
+int adf_step_resident_ctas(adf_ctx* ctx, int64_t* n);
 int adf_server_submit(adf_server* s, const adf_gf_request* req, int64_t* id);
 /* status: 0 pending/running, 1 done (outputs written), <0 error code.
  * latency_ms (optional): submit-to-completion wall time once done.        */

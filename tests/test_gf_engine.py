@@ -148,6 +148,30 @@ def test_server_continuous_batching(adf, ctx):
         assert np.array_equal(a.p, b.p) and np.array_equal(a.vn, b.vn)
 
 
+def test_server_work_cap_admission(adf, ctx):
+    """Admission by work (a cap of a fraction of one wave of step CTAs): the
+    solves still all complete, each with the result it gives alone; a solve
+    bigger than the cap is admitted on its own."""
+    specs = [(36, 60, "none", 0), (64, 50, "sphere", 1), (40, 70, "none", 2),
+             (36, 40, "cube", 3), (44, 30, "sphere", 4)]
+    alone = []
+    for s in specs:
+        r = make_req(adf, *s)
+        adf.gf_solve_batch([r], batched=False)
+        alone.append(r)
+    waves = 64 / ctx.step_resident_ctas()  # 64 work items: a few small solves at a time
+    srv = adf.Server(work_waves=waves)
+    assert srv.work_cap == 64
+    reqs = [make_req(adf, *s) for s in specs]
+    ids = [srv.submit(r) for r in reqs]
+    srv.drain()
+    for i in ids:
+        assert srv.poll(i)[0] == 1
+    srv.stop()
+    for a, b in zip(alone, reqs):
+        assert np.array_equal(a.p, b.p) and np.array_equal(a.vn, b.vn)
+
+
 def test_server_cancel_and_bad_request(adf, ctx):
     srv = adf.Server(max_resident=1)
     r1 = make_req(adf, 40, 400, "none", 0)
