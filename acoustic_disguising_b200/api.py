@@ -763,7 +763,7 @@ class Server:
         self._keep = {}
         self.work_cap = 0
         if work_waves > 0:
-            self.work_cap = int(work_waves * self.ctx.step_resident_ctas())
+            self.work_cap = max(1, int(round(work_waves * self.ctx.step_resident_ctas())))
             L.check(L.lib().adf_server_set_work_cap(self.h, self.work_cap), "server_set_work_cap")
 
     def submit(self, req: GfRequest) -> int:
