@@ -553,6 +553,10 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
       return fail(ADF_E_DEVICE, "graph launch failed");
     ctx->launches += per_step * chunk + 1 + (max_gf_far_blocks > 0 ? 2 * chunk / kGfBlock : 0);
     done += chunk;
+    if (ctx->kernel_timing) {  // measurement mode: the replay's per-launch events, before reuse
+      cudaStreamSynchronize(ctx->stream);
+      collect_kernel_times(ctx, chunk);
+    }
   }
   for (int s = 0; s < nsteps - done; ++s) {
     int rc = launch_step(ctx, s);

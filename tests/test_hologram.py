@@ -27,12 +27,14 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def band_noise(nt, n, seed, fc_cells=12.0):
-    """Seeded Gaussian noise, low-passed to a few cells per wavelength."""
+def band_noise(nt, n, seed, half=12):
+    """Seeded Gaussian noise, low-passed by a Hann window of 2*half+1 samples
+    (zero-padded at the ends, so the trace keeps its nt samples)."""
     rng = np.random.default_rng(seed)
-    x = rng.standard_normal((nt, n))
-    w = np.hanning(int(fc_cells) * 2 + 1)
-    y = np.apply_along_axis(lambda c: np.convolve(c, w / w.sum(), mode="same"), 0, x)
+    x = rng.standard_normal((nt + 2 * half, n))
+    w = np.hanning(2 * half + 1)
+    w /= w.sum()
+    y = sum(w[k] * x[k:k + nt] for k in range(2 * half + 1))
     return np.asfortranarray(y.astype(np.float32))
 
 
@@ -78,11 +80,12 @@ def run_pair(adf, oracle, c, cols, r_pts, sigma, aq, af):
 def test_hologram_128cube_injection_shell_kh(adf, oracle, ctx):
     """A reduced configuration with the full structure: 128^3, 8-cell CPML,
     rigid ellipsoid 20/15/10 cells, 512 injection points at 25 cells, a
-    512-point shell at 32 cells, 260 steps, KH to 64 targets at 1 m."""
+    512-point shell at 32 cells, 260 steps, KH to 64 targets at 0.4 m (their
+    delays from the shell, 165-390 samples, overlap the record)."""
     n_in = n_out = 512
     c = hologram_case(adf, oracle, 128, 260, 8, (20, 15, 10), 25, 32, n_in, n_out)
     cols = np.arange(1, n_out + 1, dtype=np.int64)
-    rp, _ = adf.fibonacci_sphere(64, 1.0)
+    rp, _ = adf.fibonacci_sphere(64, 0.4)
     sigma = np.sqrt(np.log(2.0)) / (2 * np.pi * 20e3)
     dS = 4 * np.pi * (32 * DX) ** 2 / n_out
     aq, af = -RHO * dS * DT, -dS * DT
@@ -96,7 +99,7 @@ def test_hologram_128cube_injection_shell_kh(adf, oracle, ctx):
     # the device hand-off equals the host path on the downloaded traces, bit for bit
     host = adf.kh_pressure(sp, sn, rp, g.vn_rec[:, shell], g.rec[0][:, shell], DT, sigma, C0,
                            aq, af, rho=RHO)
-    assert np.array_equal(out, host)
+    assert np.abs(host).max() > 0 and np.array_equal(out, host)
     # and the KH sum against the FP64 oracle on the oracle's own recorded traces
     ref = oracle.kh_pressure(sp, sn, rp, go.vn_rec[:, shell], go.rec[0][:, shell], DT, sigma,
                              C0, aq, af, mode=1)
@@ -108,11 +111,12 @@ def test_hologram_512cube_16384_transceivers(adf, oracle, ctx):
     """The full hologram grid and transceiver counts: 512^3, 12-cell CPML,
     ellipsoid 80/60/40 cells, 8192 injection points at 100 cells and an
     8192-point shell at 130 cells, 24 steps (the entry lists of all 16384
-    transceivers at full size), KH of the injection surface's own records."""
+    transceivers at full size), KH of the injection surface's own records to
+    targets 4 cells outside it (delays from 14 samples, inside the record)."""
     n_in = n_out = 8192
     c = hologram_case(adf, oracle, 512, 24, 12, (80, 60, 40), 100, 130, n_in, n_out)
     cols = np.arange(n_out + 1, n_out + n_in + 1, dtype=np.int64)
-    rp, _ = adf.fibonacci_sphere(128, 2.0)
+    rp, _ = adf.fibonacci_sphere(128, 104 * DX)
     sigma = np.sqrt(np.log(2.0)) / (2 * np.pi * 20e3)
     dS = 4 * np.pi * (100 * DX) ** 2 / n_in
     f, fo, out, sp, sn = run_pair(adf, oracle, c, cols, rp, sigma, -RHO * dS * DT, -dS * DT)
@@ -124,4 +128,4 @@ def test_hologram_512cube_16384_transceivers(adf, oracle, ctx):
     assert rel_l2(g.vn_rec[:, inner], go.vn_rec[:, inner]) <= TOL
     host = adf.kh_pressure(sp, sn, rp, g.vn_rec[:, inner], g.rec[0][:, inner], DT, sigma, C0,
                            -RHO * dS * DT, -dS * DT, rho=RHO)
-    assert np.array_equal(out, host)
+    assert np.abs(host).max() > 0 and np.array_equal(out, host)
