@@ -18,7 +18,7 @@ namespace adf {
 // Staged planes of the step kernel: x range xb-4 .. xb+kXT+3 of a 64-cell
 // tile (the halo column xb-1 and Vx at xb+64 included), rows j0-1 .. j0+ty.
 constexpr int kStageW = 72;
-constexpr int kStepRing = 3;  // planes k, k+1 resident while k+2 lands
+constexpr int kStepRing = 2;  // the stage of plane k in use while k+1 lands
 
 enum : int {
   SF_MASK = 1,      // solve has a scatterer mask
@@ -50,8 +50,10 @@ struct SolveDev {
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;
-  // two CUtensorMaps (128 B each) over field buffers 0 and 1: 4D (x: nxp,
-  // y: ny, z: nz, channel: 4), box (kStageW, ty + 2, 1, 4), zero fill
+  // four CUtensorMaps (128 B each) over the field: per buffer 0, 1 one with
+  // box (kStageW, ty + 2, 1, 3) (P, Vx, Vy of a plane) and one with box
+  // (kStageW, ty + 2, 1, 1) (Vz); 4D (x: nxp, y: ny, z: nz, channel: 4),
+  // zero fill outside the grid
   const void* fmap;
   long long buf_stride;   // floats per field buffer (4*nz*ny*nxp)
   long long chan_stride;  // floats per channel (nz*ny*nxp)

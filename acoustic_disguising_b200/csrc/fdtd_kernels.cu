@@ -187,12 +187,12 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
 }
 
 // The same update for one cell (the halo column x = xb-1 of an x tile), from
-// the staged planes: `st` is plane k, `stn` plane k+1, `c` the cell's offset
-// in a channel of a stage and `cst` the channel stride.
+// the staged plane `st` (P, Vx, Vy of plane k; `c` the cell's offset in a
+// channel, `cst` the channel stride) and Vz of planes k and k+1 (Z0, Z1).
 template <typename R>
 __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
-                                               const float* co, const float* st, const float* stn,
-                                               int c, int cst, int x) {
+                                               const float* co, const float* st, float Z0,
+                                               float Z1, int c, int cst, int x) {
   using A = Arith<R>;
   const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, j = rc.j, k = rc.k, nxp = rc.nxp;
   const bool rigid_y = j == ny - 1, rigid_z = k == nz - 1;
@@ -201,9 +201,9 @@ __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& 
   const float P = st[c];
   if (!upd) return P;
   const float X0 = st[cst + c], X1 = st[cst + c + 1];
-  const float Y0 = st[2 * cst + c], Z0 = st[3 * cst + c];
+  const float Y0 = st[2 * cst + c];
   const float dy = rigid_y ? __fmul_rn(-2.0f, Y0) : __fsub_rn(st[2 * cst + c + kStageW], Y0);
-  const float dz = rigid_z ? __fmul_rn(-2.0f, Z0) : __fsub_rn(stn[3 * cst + c], Z0);
+  const float dz = rigid_z ? __fmul_rn(-2.0f, Z0) : __fsub_rn(Z1, Z0);
   R dvx = A::mul(A::cv(__fsub_rn(X1, X0)), g.rdx);
   R dvy = A::mul(A::cv(dy), g.rdy);
   R dvz = A::mul(A::cv(dz), g.rdz);
@@ -460,11 +460,17 @@ constexpr int kXT = 64;             // cells per x tile (4 warps)
 constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..] = cells
 constexpr int kStepThreads = 32 * kXT / 16;  // warps of 4 quads x 8 rows
 
-constexpr int kStageFloats = 4 * (kMaxTy + 2) * kStageW;  // one staged plane, 4 channels
+// One stage: P, Vx, Vy of a plane ([3][ty+2][kStageW]) and, from the next
+// 128-B boundary on (TMA destinations must be 128-B aligned), Vz of the next
+// plane ([ty+2][kStageW]).
+__host__ __device__ constexpr int stage_vz_offset(int cst) { return (3 * cst + 31) / 32 * 32; }
+constexpr int kStageFloats =
+    (stage_vz_offset((kMaxTy + 2) * kStageW) + (kMaxTy + 2) * kStageW + 31) / 32 * 32;
 // Polls of a staged plane's bounded wait: a plane lands within microseconds,
 // so a limit far below kWaitLimit keeps a lost copy from stalling the GPU
 constexpr uint32_t kStepWaitLimit = 1u << 20;
 static_assert((kStageFloats * 4) % 128 == 0, "stages stay 128-B aligned");
+static_assert((stage_vz_offset(5 * kStageW) * 4) % 128 == 0, "Vz boxes start 128-B aligned");
 
 template <typename R>
 __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
@@ -523,21 +529,25 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   const int pq = r * kPnPitch + 4 + 4 * qx;  // this quad in a shared new-P plane
   const int z0 = item.z, z1 = item.w;
   const int kfirst = z0 > 0 ? z0 - 1 : z0;
-  // Planes kfirst .. klast are staged by TMA into a ring of kStepRing slots
-  // (the last one only for Vz of plane z1-1; plane nz would be all zeros,
-  // which the loop supplies itself).  A stage holds channels P, Vx, Vy, Vz of
-  // rows j0-1 .. j0+ty and x = xb-4 .. xb+67 (zero outside the grid).
-  const int klast = min(z1, nz - 1);
+  // The stage of plane k, staged by TMA into a ring of kStepRing slots, holds
+  // P, Vx, Vy of plane k and Vz of plane k+1 (channel slot 3; not loaded for
+  // k = nz-1, where the loop supplies the zeros itself), rows j0-1 .. j0+ty,
+  // x = xb-4 .. xb+67, zero outside the grid.  Vz of plane k is carried in
+  // registers from the previous stage.
   const int cst = (ty + 2) * kStageW;         // channel stride in a stage
+  const int vzo = stage_vz_offset(cst);       // Vz of the next plane in a stage
   const int so = r * kStageW + 4 + 4 * qx;    // this quad in a stage channel
-  const void* fmap = static_cast<const char*>(S.fmap) + rb * 128;
+  const char* maps = static_cast<const char*>(S.fmap) + rb * 256;  // {P,Vx,Vy box; Vz box}
   auto slot_of = [&](int k) { return (k - kfirst) % kStepRing; };
   auto issue = [&](int k) {  // one thread
     const int sl = slot_of(k);
     fence_proxy_async_smem();  // the slot was last read through the generic proxy
     const uint32_t bar = smem_u32(rbar + sl);
-    mbar_expect_tx(bar, (uint32_t)(16 * cst));
-    tma_load_4d(smem_u32(ring + sl * kStageFloats), fmap, xb - 4, j0 - 1, k, 0, bar);
+    const bool vz = k + 1 < nz;
+    mbar_expect_tx(bar, (uint32_t)((vz ? 16 : 12) * cst));
+    float* dst = ring + sl * kStageFloats;
+    tma_load_4d(smem_u32(dst), maps, xb - 4, j0 - 1, k, 0, bar);
+    if (vz) tma_load_4d(smem_u32(dst + vzo), maps + 128, xb - 4, j0 - 1, k + 1, 3, bar);
   };
   auto wait = [&](int k) {
     const int u = k - kfirst;
@@ -545,18 +555,24 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
       atomicOr(S.err, 4);  // reported as ADF_E_TIMEOUT; the values read are wrong
   };
   if (tid == 0)
-    for (int k = kfirst; k <= min(klast, kfirst + kStepRing - 1); ++k) issue(k);
-  wait(kfirst);
+    for (int k = kfirst; k < min(z1, kfirst + kStepRing); ++k) issue(k);
+  // Vz of plane kfirst (the stages carry the next plane's), and of the halo
+  // column for its single-cell update
   float4 Z0 = make_float4(0.f, 0.f, 0.f, 0.f), Pzm = Z0;
-  if (act) Z0 = ld4(ring + slot_of(kfirst) * kStageFloats + 3 * cst + so);
+  const bool hcol = qx == 0 && r >= 1 && row_ok && xb > 0;
+  float Zh = 0.f;
+  {
+    const float* vz0 = S.field + rb * S.buf_stride + 3 * cs + kfirst * plane + rowoff;
+    if (act) Z0 = ldg4(vz0);
+    if (hcol) Zh = __ldg(vz0 - 1);
+  }
   const int* tp = S.tp_off + (long long)T * nz * 4;
   for (int k = kfirst; k < z1; ++k) {
     const bool prologue = k < z0;
     rc.k = k;
     float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
     const float* st = ring + slot_of(k) * kStageFloats;
-    const float* stn = ring + slot_of(k + 1) * kStageFloats;
-    if (k + 1 <= klast) wait(k + 1);
+    wait(k);
     const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
     const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
     const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
@@ -569,7 +585,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
       Y0 = ld4(st + 2 * cst + so);
       const float X5 = st[cst + so + 4];
       const float4 Y1 = ld4(st + 2 * cst + so + kStageW);
-      Z1 = k + 1 < nz ? ld4(stn + 3 * cst + so) : Pn;
+      Z1 = k + 1 < nz ? ld4(st + vzo + so) : Pn;
       if (has_mask)
         nib = (__ldg(S.mask_bits + ((long long)k * ny + j) * S.mw + (x0 >> 3)) >> ((x0 & 4) * 4)) &
               0xFFFFu;
@@ -580,11 +596,14 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
         Pn = p_update_quad<R>(S, rc, g, co, x0, vrow && !prologue, P4, X4, X5, Y0, Y1, Z0, Z1, nib);
       st4(pn + pq, Pn);
     }
-    if (qx == 0 && r >= 1 && row_ok && xb > 0)
-      pn[pq - 1] = p_update_cell<R>(S, rc, g, co, st, stn, so - 1, cst, xb - 1);
+    if (hcol) {
+      const float Zh1 = k + 1 < nz ? st[vzo + so - 1] : 0.f;
+      pn[pq - 1] = p_update_cell<R>(S, rc, g, co, st, Zh, Zh1, so - 1, cst, xb - 1);
+      Zh = Zh1;
+    }
     __syncthreads();
     // every read of plane k's stage is done: refill its slot
-    if (tid == 0 && k + kStepRing <= klast) issue(k + kStepRing);
+    if (tid == 0 && k + kStepRing < z1) issue(k + kStepRing);
     // ---- q channel: inject/record on the new P (forward.jl:92) ----
     if (off0 < off1) {
       apply_entries(S, off0, off1, 0, nxp, xb - 1, xb + kXT, xb, !prologue, it, tid, nthr,
@@ -651,8 +670,12 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
 
 // Shared memory: the staged-plane ring (dynamic, kStepRing * kStageFloats
 // floats) plus the new-P planes, the f-channel staging and the descriptor:
-// 43.4 KB per CTA, five CTAs per SM.
-constexpr int kStepCtasPerSm = 5;
+// 33.4 KB per CTA; five CTAs per SM (the register budget: 102 per thread,
+// no spills; six CTAs at 80 registers spill and measured slower).
+#ifndef ADF_STEP_CTAS_PER_SM
+#define ADF_STEP_CTAS_PER_SM 5
+#endif
+constexpr int kStepCtasPerSm = ADF_STEP_CTAS_PER_SM;  // register budget: 65536 / (128 x this)
 // (+128 B so that the ring can start on a 128-B boundary, as TMA destinations must)
 constexpr size_t kStepDynSmem = sizeof(float) * kStepRing * kStageFloats + 128;
 

@@ -237,9 +237,9 @@ template float* solve_dalloc<float>(Solve&, size_t, int&);
 template int* solve_dalloc<int>(Solve&, size_t, int&);
 template double* solve_dalloc<double>(Solve&, size_t, int&);
 
-// The step kernel's TMA descriptors of the two field buffers: a 4D tiled map
-// (x: nxp, y: ny, z: nz, channel: 4) with the staged box (kStageW, ty+2, 1, 4)
-// and zero fill outside the grid.  cuTensorMapEncodeTiled comes from the
+// The step kernel's TMA descriptors of the two field buffers: 4D tiled maps
+// (x: nxp, y: ny, z: nz, channel: 4) with the staged boxes (kStageW, ty+2, 1, 3)
+// for P, Vx, Vy and (kStageW, ty+2, 1, 1) for Vz, zero fill outside the grid.  cuTensorMapEncodeTiled comes from the
 // driver through the runtime's entry-point query (no link against libcuda).
 static int make_field_maps(Solve& s) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -258,10 +258,12 @@ static int make_field_maps(Solve& s) {
   const cuuint64_t dims[4] = {(cuuint64_t)d.nxp, (cuuint64_t)d.ny, (cuuint64_t)d.nz, 4};
   const cuuint64_t strides[3] = {(cuuint64_t)d.nxp * 4, (cuuint64_t)d.nxp * d.ny * 4,
                                  (cuuint64_t)d.chan_stride * 4};
-  const cuuint32_t box[4] = {(cuuint32_t)kStageW, (cuuint32_t)(d.ty + 2), 1, 4};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  for (int b = 0; b < 2; ++b) {
-    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(s.fmap_host + 128 * b);
+  for (int m4 = 0; m4 < 4; ++m4) {  // buffer b = m4 / 2; box of 3 channels or of Vz
+    const int b = m4 / 2;
+    const cuuint32_t box[4] = {(cuuint32_t)kStageW, (cuuint32_t)(d.ty + 2), 1,
+                               (cuuint32_t)(m4 % 2 ? 1 : 3)};
+    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(s.fmap_host + 128 * m4);
     const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d.field + b * d.buf_stride,
                               dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
