@@ -148,6 +148,7 @@ SIGNATURES = [
     ("adf_kh_velocity", C.c_int, [C.c_void_p, C.POINTER(KhDescC), C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     ("adf_fp32_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("adf_fp64_fma_peak", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("adf_kh_test_fault", C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
     ("adf_run_fdtd_kh", C.c_int, [C.c_void_p, C.POINTER(Domain), C.c_void_p,
                                   C.POINTER(TxGridC), C.POINTER(CpmlC), C.c_void_p, C.c_int64,

@@ -598,6 +598,14 @@ def fp32_fma_peak(ctx: Context | None = None):
     return tf.value, ms.value
 
 
+def fp64_fma_peak(ctx: Context | None = None):
+    """Measured FP64 FMA throughput (TFLOP/s, ms of the probe)."""
+    ctx = ctx or default_context()
+    tf, ms = C.c_double(), C.c_double()
+    L.check(L.lib().adf_fp64_fma_peak(ctx.h, C.byref(tf), C.byref(ms)), "fp64_fma_peak")
+    return tf.value, ms.value
+
+
 # ---------------------------------------------------------------------------
 # Impulsive Green's-function solves (src/greens.jl:48-234)
 # ---------------------------------------------------------------------------

@@ -394,6 +394,25 @@ __global__ void __launch_bounds__(256) adf_fma_peak_kernel(float* out, int iters
   if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains live
 }
 
+// FP64 FMA throughput probe (the roofline of the in-loop GF contraction,
+// which accumulates in Float64): the same chains in double.
+__global__ void __launch_bounds__(256) adf_fma64_peak_kernel(double* out, int iters, double a,
+                                                             double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1234.5) out[blockIdx.x] = s;  // keeps the chains live
+}
+
 namespace {
 
 template <typename T>
@@ -679,6 +698,27 @@ extern "C" int adf_kh_test_fault(adf_ctx* ctx, int skip_chunk, uint32_t poll_lim
     return fail(ADF_E_ARG, "adf_kh_test_fault: skip_chunk >= -1 and poll_limit > 0");
   ctx->kh_skip_chunk = skip_chunk;
   ctx->kh_wait_limit = poll_limit;
+  return ADF_OK;
+}
+
+extern "C" int adf_fp64_fma_peak(adf_ctx* ctx, double* tflops, double* ms_out) {
+  if (!ctx || !tflops) return fail(ADF_E_ARG, "adf_fp64_fma_peak: null argument");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  const int blocks = ctx->nsm * 8, iters = 1024;
+  DevBuf<double> o(ctx);
+  if (!o.alloc((size_t)blocks)) return fail(ADF_E_NOMEM, "adf_fp64_fma_peak: allocation failed");
+  adf_fma64_peak_kernel<<<blocks, 256, 0, ctx->stream>>>(o.p, 16, 0.999, 1e-4);  // warm-up
+  cudaEventRecord(ctx->ev0, ctx->stream);
+  adf_fma64_peak_kernel<<<blocks, 256, 0, ctx->stream>>>(o.p, iters, 0.999, 1e-4);
+  cudaEventRecord(ctx->ev1, ctx->stream);
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  const double flop = 2.0 * 128.0 * iters * (double)blocks * 256;
+  *tflops = flop / (ms * 1e-3) / 1e12;
+  if (ms_out) *ms_out = ms;
   return ADF_OK;
 }
 

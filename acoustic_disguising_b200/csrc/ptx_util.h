@@ -62,6 +62,15 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int x
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(c), "r"(mbar)
       : "memory");
 }
+// The same for a three-dimensional map.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int x, int y, int z,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(mbar)
+      : "memory");
+}
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

@@ -687,11 +687,21 @@ def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
     gf_ms = times[False] - times[True]
     lags = sum(min(it, nt_gf) for it in range(1, nt))
     byts = 2.0 * 4 * n_io * n_io * lags  # both tensors' lag slices, read once per step
+    flop = 2.0 * 2 * n_io * n_io * lags  # 2 tensors x sources x receivers x lags, FMA = 2
+    peak64, _ = A.fp64_fma_peak(ctx)
+    achieved = flop / (gf_ms / 1e3) / 1e12 if gf_ms > 0 else None
     return {"workload": f"{n}^3 run_fdtd!, {nt} steps, PVFromPin map {nt_gf} lags x {n_io} "
                         f"sources x {n_io} receivers",
             "run_ms_without_map": times[True], "run_ms_with_map": times[False],
             "gf_ms_per_step": gf_ms / (nt - 1),
-            "gf_tensor_gbs": byts / (gf_ms / 1e3) / 1e9 if gf_ms > 0 else None}
+            "gf_tensor_gbs": byts / (gf_ms / 1e3) / 1e9 if gf_ms > 0 else None,
+            "roofline": {"bound": "fp64 fma (Float64 accumulation, as the reference's)",
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64 if achieved else None,
+                         "peak_source": "measured in this run (adf_fp64_fma_peak)",
+                         "flop": flop, "time": "run with the map minus the run with it "
+                                               "discarded (every GF kernel, per step and "
+                                               "per block)"}}
 
 
 # ---------------------------------------------------------------------------

@@ -343,6 +343,9 @@ int adf_last_kh_ms(adf_ctx* ctx, double* ms);
  * roofline denominator of adf_kh_pressure.  Measurement helper with no
  * reference counterpart; ms (optional) receives the probe's duration.      */
 int adf_fp32_fma_peak(adf_ctx* ctx, double* tflops, double* ms);
+/* The same probe in Float64: the roofline denominator of the in-loop GF
+ * extrapolation's contraction, which accumulates in Float64.             */
+int adf_fp64_fma_peak(adf_ctx* ctx, double* tflops, double* ms);
 
 /* Test hook with no reference counterpart: arms the next adf_kh_pressure /
  * adf_kh_velocity call on ctx (one shot) so that its bounded waits give up
