@@ -294,21 +294,23 @@ def reference_arm(args):
     threads = os.cpu_count() or 1
     per = []
     t_all = time.perf_counter()
+    sample = max(2, args.cpu_steps // 10)  # time steps of one solve per bench step
     for i in range(args.warmup + args.steps):
-        s = cpu_sample(max(2, args.cpu_steps // 10), threads)
+        s = cpu_sample(sample, threads)
         if i >= args.warmup:
             per.append(s)
-    sec_per_step = statistics.mean(per)
-    sps = 1.0 / (NT * sec_per_step)
+    sec_per_step = statistics.mean(per)  # per FDTD time step
+    sps = 1.0 / (NT * sec_per_step)      # solve-equivalents of 2000 steps per second
     line = {
         "impl": "reference", "metric": METRIC, "value": sps, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": sec_per_step * 1e3 * NT, "higher_is_better": True, "scaling": "weak",
+        # one bench step = the timed sample (`sample` time steps), as measured
+        "ms_per_step": sec_per_step * 1e3 * sample, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 intermediates, f32 storage", "data": "synthetic",
         "config": workload_config(1, 1),
         "cpu_baseline": {"value": sps, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{max(2, args.cpu_steps // 10)} time steps of one solve per "
-                                   "bench step, extrapolated to 2000 steps"},
+                         "sample": f"{sample} time steps of one solve per bench step (the "
+                                   "bench step); solves/s = its rate over a 2000-step solve"},
         "e2e": {"value": sps, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": "CPU restatement (oracle/) of the reference's Threads path; the reference is "
@@ -442,12 +444,12 @@ SERVE_SIZES = (96, 128, 160, 192, 256)
 SERVE_BUDGET = 120 * 10 ** 9
 
 
-def serving_requests(A, n_req, seed):
+def serving_requests(A, n_req, seed, sizes=SERVE_SIZES, steps_range=(500, 3001)):
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n_req):
-        n = int(rng.choice(SERVE_SIZES))
-        steps = int(rng.integers(500, 3001))
+        n = int(rng.choice(sizes))
+        steps = int(rng.integers(*steps_range))
         xmax = (n - 1) * DX / 2
         d = A.Domain(tmax=tmax_of(steps), xmax=xmax, nx=n, c0=C0, r0=RHO, cf=0.5)
         tf, _ = A.impulsive_wavelet(d, F3DB)
@@ -469,18 +471,17 @@ def serving_requests(A, n_req, seed):
     return out
 
 
-def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
-    """The mixed request stream served twice in real time on the same Poisson
+def serve_stream(A, ctx, n_req, make, max_resident=0, waves=2.0, load=4.0, seed=20261203):
+    """One request stream served twice in real time on the same Poisson
     arrivals, offered at `load` times the plain path's capacity (estimated
     from 8 calibration requests of another seed, then measured): the plain
     path runs one solve at a time (FIFO, one launch sequence per solve); the
     continuous-batching server admits by HBM budget and by work (resident
     step work within `waves` waves of the GPU's resident CTAs).  Latency =
     completion - arrival; solves/s = requests / (last completion - first
-    arrival)."""
-    seed = 20261203
+    arrival).  `make(n, seed)` builds n requests."""
     svc = []
-    for r in serving_requests(A, 8, seed + 7):  # calibration (and warm-up)
+    for r in make(8, seed + 7):  # calibration (and warm-up)
         t0 = time.perf_counter()
         A.gf_solve_batch([r], batched=False, ctx=ctx)
         svc.append(time.perf_counter() - t0)
@@ -488,7 +489,7 @@ def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
     arr = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / lam, n_req))
     arr -= arr[0]
     # plain arm: one solve at a time, in real time on the arrivals
-    reqs = serving_requests(A, n_req, seed)
+    reqs = make(n_req, seed)
     done, busy = [], 0.0
     t0 = time.perf_counter()
     for a, r in zip(arr, reqs):
@@ -503,7 +504,7 @@ def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
     plain_sps = n_req / (done[-1] - arr[0])
     plain_cap = n_req / busy
     # batched arm: the server fed the same arrivals in real time
-    reqs = serving_requests(A, n_req, seed)
+    reqs = make(n_req, seed)
     srv = A.Server(hbm_budget=SERVE_BUDGET, max_resident=max_resident, ctx=ctx, work_waves=waves)
     ids = []
     t0 = time.perf_counter()
@@ -530,11 +531,6 @@ def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
     b_sps = n_req / (max(done_at.values()) - arr[0])
     pct = lambda x, q: float(np.percentile(x, q))
     return {
-        "workload": f"{n_req} impulsive GF solves, grids {{96,128,160,192,256}}^3 drawn "
-                    "uniformly, 500-3000 steps, scatterer none/sphere/cube/ellipsoid (random "
-                    "centre, size <= 30% of the domain), 10-cell CPML, 256-point shell; "
-                    f"Poisson arrivals offered at {load:g}x the plain path's estimated "
-                    "capacity; 120 GB HBM budget; both arms served in real time",
         "batched": {"solves_per_s": b_sps, "p50_ms": pct(b_lat, 50) * 1e3,
                     "p99_ms": pct(b_lat, 99) * 1e3,
                     "admission": f"HBM budget + work cap {cap_items} step work items "
@@ -546,6 +542,25 @@ def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
         "speedup_solves_per_s": b_sps / plain_sps, "offered_per_s": lam,
         "offered_over_plain_capacity": lam / plain_cap, "requests": n_req,
     }
+
+
+def serving_section(A, ctx, n_req, max_resident=0, waves=2.0, load=4.0):
+    """The mixed stream of the serving workload, and the same stream drawn
+    from its two smallest grids (where one solve fills a fraction of the GPU
+    and batching pays most)."""
+    out = serve_stream(A, ctx, n_req, lambda n, sd: serving_requests(A, n, sd), max_resident,
+                       waves, load)
+    out["workload"] = (f"{n_req} impulsive GF solves, grids {{96,128,160,192,256}}^3 drawn "
+                       "uniformly, 500-3000 steps, scatterer none/sphere/cube/ellipsoid (random "
+                       "centre, size <= 30% of the domain), 10-cell CPML, 256-point shell; "
+                       f"Poisson arrivals offered at {load:g}x the plain path's estimated "
+                       "capacity; 120 GB HBM budget; both arms served in real time")
+    small = serve_stream(A, ctx, 64, lambda n, sd: serving_requests(A, n, sd, sizes=(96, 128)),
+                         max_resident, waves, load, seed=20261205)
+    small["workload"] = ("64 requests of the same stream restricted to 96^3 and 128^3 grids "
+                         "(one solve fills 23-41 % of the GPU's resident CTAs)")
+    out["small_grids"] = small
+    return out
 
 # ---------------------------------------------------------------------------
 # The 512^3 step: 12-cell CPML, rigid ellipsoid (semi-axes 80/60/40 cells)
