@@ -50,11 +50,10 @@ struct SolveDev {
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;
-  // five CUtensorMaps (128 B each): per field buffer 0, 1 one with box
-  // (kStageW, ty + 2, 1, 3) (P, Vx, Vy of a plane) and one with box
-  // (kStageW, ty + 2, 1, 1) (Vz), 4D (x: nxp, y: ny, z: nz, channel: 4); then
-  // the mask, 3D (word: mw, y: ny, z: nz) uint32 with box (16, ty + 1, 1)
-  // (solves with a mask only); zero fill outside the arrays
+  // four CUtensorMaps (128 B each) over the field: per buffer 0, 1 one with
+  // box (kStageW, ty + 2, 1, 3) (P, Vx, Vy of a plane) and one with box
+  // (kStageW, ty + 2, 1, 1) (Vz); 4D (x: nxp, y: ny, z: nz, channel: 4),
+  // zero fill outside the grid
   const void* fmap;
   long long buf_stride;   // floats per field buffer (4*nz*ny*nxp)
   long long chan_stride;  // floats per channel (nz*ny*nxp)

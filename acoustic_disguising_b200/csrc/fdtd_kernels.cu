@@ -192,7 +192,7 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
 template <typename R>
 __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& rc, const Sc<R>& g,
                                                const float* co, const float* st, float Z0,
-                                               float Z1, int c, int cst, int x, bool open_p) {
+                                               float Z1, int c, int cst, int x) {
   using A = Arith<R>;
   const int nx = rc.nx, ny = rc.ny, nz = rc.nz, npml = rc.npml, j = rc.j, k = rc.k, nxp = rc.nxp;
   const bool rigid_y = j == ny - 1, rigid_z = k == nz - 1;
@@ -209,7 +209,7 @@ __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& 
   R dvz = A::mul(A::cv(dz), g.rdz);
   bool open = true;
   if (!plain_rigid) {
-    open = open_p;
+    if (S.flags & SF_MASK) open = (S.mask_bits[((long long)k * ny + j) * S.mw + (x >> 3)] >> (4 * (x & 7))) & 1u;
     if (rc.pcpml) {
       const int xs = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
       if (xs >= 0) {
@@ -432,18 +432,17 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 // The step kernel.  One CTA per work item {solve, y tile | x tile << 16, z0,
 // z1}: a tile of ty <= 7 rows j0..j0+ty-1 and the kXT = 64 cells
 // xb..xb+63 of one solve, and the planes z0..z1-1.  blockDim = (32, 4): warp
-// w holds the quads w, w+4, w+8, w+12 of all 8 tile rows
-// r = j - j0 + 1 = 0..7 (lane = 4r + i holds quad w + 4i).  Row r = 0 is the
-// halo row j0-1, whose new P the Vy update of row j0 needs: it is
-// recomputed, not exchanged.  The lanes of quad 0 also recompute the halo
-// column x = xb-1 (for Vx at xb).  The interleaving spreads the x-slab quads
-// of an x-edge tile over three warps, so that no warp carries all of a
-// tile's x-slab CPML work to the per-plane barrier.
+// w holds the 4 quads 4w..4w+3 (16 cells) of all 8 tile rows
+// r = j - j0 + 1 = 0..7 (lane = 4r + quad).  Row r = 0 is the halo row
+// j0-1, whose new P the Vy update of row j0 needs: it is recomputed, not
+// exchanged.  The lanes of quad 0 also recompute the halo column x = xb-1
+// (for Vx at xb).  With this shape the x-slab quads of a grid sit in one
+// warp of each x-edge tile and the tiles between hold none, so few warps
+// take the CPML branch and few CTAs wait for such a warp at their barrier.
 // Per plane, after a prologue plane z0-1 (new P only, for Vz at z0) when
 // z0 > 0:
-//   stage  : P, Vx, Vy of plane k, Vz of plane k+1 and the mask words,
-//            staged by TMA (one plane ahead) into a shared ring; Vz of plane
-//            k and the new P of plane k-1 are carried in registers;
+//   loads  : P, Vx, Vy of plane k and Vz of plane k+1 (Vz of plane k and the
+//            new P of plane k-1 are carried in registers), 128-bit, coalesced;
 //   P      : new P into a double-buffered shared plane; barrier;
 //   q      : injection/recording on P (only planes with entries; barrier);
 //   V      : Vx/Vy/Vz from the new P (x-1 and y-1 neighbours from shared
@@ -454,25 +453,19 @@ __device__ __forceinline__ void v_plain_quad(const Sc<R>& g, float4 Pc, float Px
 // A warp whose quads are all plain for this plane (the bulk of the grid)
 // takes the plain functions (warp-uniform branch); the rest the general
 // ones.  Several CTAs per SM keep enough independent warps in flight to
-// cover the latency of the float/double chains and of the CPML memory.
+// cover the latency of the float/double chains and of HBM.
 // ---------------------------------------------------------------------------
 constexpr int kMaxTy = 7;           // rows per tile (plus the halo row: 8 per warp)
 constexpr int kXT = 64;             // cells per x tile (4 warps)
 constexpr int kPnPitch = kXT + 4;   // shared new-P row: [3] = halo column, [4..] = cells
-constexpr int kStepThreads = 32 * kXT / 16;  // 4 warps of 4 quads x 8 rows
+constexpr int kStepThreads = 32 * kXT / 16;  // warps of 4 quads x 8 rows
 
 // One stage: P, Vx, Vy of a plane ([3][ty+2][kStageW]) and, from the next
 // 128-B boundary on (TMA destinations must be 128-B aligned), Vz of the next
 // plane ([ty+2][kStageW]).
 __host__ __device__ constexpr int stage_vz_offset(int cst) { return (3 * cst + 31) / 32 * 32; }
-// then the mask words of rows j0-1 .. j0+ty-1 (kMaskW words per row, from
-// word xb/8 - 4), again from a 128-B boundary
-constexpr int kMaskW = 16;
-__host__ __device__ constexpr int stage_mask_offset(int cst) {
-  return (stage_vz_offset(cst) + cst + 31) / 32 * 32;
-}
 constexpr int kStageFloats =
-    (stage_mask_offset((kMaxTy + 2) * kStageW) + kMaskW * (kMaxTy + 1) + 31) / 32 * 32;
+    (stage_vz_offset((kMaxTy + 2) * kStageW) + (kMaxTy + 2) * kStageW + 31) / 32 * 32;
 // Polls of a staged plane's bounded wait: a plane lands within microseconds,
 // so a limit far below kWaitLimit keeps a lost copy from stalling the GPU
 constexpr uint32_t kStepWaitLimit = 1u << 20;
@@ -489,12 +482,8 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   const int T = item.y & 0xFFFF, X = item.y >> 16;
   const int j0 = T * ty, xb = X * kXT;
   // this thread's tile row r (0 = halo row) and quad qx; its warp's quads
-  // quads interleaved across the warps: warp w holds quads w, w+4, w+8, w+12,
-  // so the x-slab quads at a grid edge (the first or last three of a row)
-  // fall into three different warps instead of one, and no single warp
-  // carries a tile's whole x-slab CPML work to the per-plane barrier
-  const int qx = wid + 4 * (lane & 3), r = lane >> 2;
-  const int wr0 = 0, wnr = kMaxTy + 1;
+  const int qx = 4 * wid + (lane & 3), r = lane >> 2;
+  const int wq0 = 4 * wid, wnq = 4, wr0 = 0, wnr = kMaxTy + 1;
   const int j = j0 - 1 + r, x0 = xb + 4 * qx;
   const bool row_ok = r <= ty && j >= 0 && j < ny;
   const bool act = row_ok && x0 < nxp;  // this thread updates a quad
@@ -526,7 +515,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   bool wplain_rx;
   {
     const int wj0 = j0 - 1 + wr0, wj1 = wj0 + wnr - 1;  // rows: P on all, V from wj0 + 1
-    const int wx0 = xb + 4 * wid, wx1 = xb + 4 * (wid + 12) + 3;  // the warp's x extent
+    const int wx0 = xb + 4 * wq0, wx1 = wx0 + 4 * wnq - 1;
     const int p_xmin = pcp ? npml : 0, p_xmax = pcp ? min(nx - 2, nx - npml - 1) : nx - 2;
     const int v_xmin = vcp ? npml + 1 : 1, v_xmax = vcp ? nx - npml - 2 : nx - 1;
     bool ok = wr0 + wnr - 1 <= ty && wj0 >= 0 && wx1 < nxp;
@@ -547,7 +536,6 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
   // registers from the previous stage.
   const int cst = (ty + 2) * kStageW;         // channel stride in a stage
   const int vzo = stage_vz_offset(cst);       // Vz of the next plane in a stage
-  const int mko = stage_mask_offset(cst);     // mask words of the plane in a stage
   const int so = r * kStageW + 4 + 4 * qx;    // this quad in a stage channel
   const char* maps = static_cast<const char*>(S.fmap) + rb * 256;  // {P,Vx,Vy box; Vz box}
   auto slot_of = [&](int k) { return (k - kfirst) % kStepRing; };
@@ -556,13 +544,10 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     fence_proxy_async_smem();  // the slot was last read through the generic proxy
     const uint32_t bar = smem_u32(rbar + sl);
     const bool vz = k + 1 < nz;
-    mbar_expect_tx(bar, (uint32_t)((vz ? 16 : 12) * cst + (has_mask ? 4 * kMaskW * (ty + 1) : 0)));
+    mbar_expect_tx(bar, (uint32_t)((vz ? 16 : 12) * cst));
     float* dst = ring + sl * kStageFloats;
     tma_load_4d(smem_u32(dst), maps, xb - 4, j0 - 1, k, 0, bar);
     if (vz) tma_load_4d(smem_u32(dst + vzo), maps + 128, xb - 4, j0 - 1, k + 1, 3, bar);
-    if (has_mask)
-      tma_load_3d(smem_u32(dst + mko), static_cast<const char*>(S.fmap) + 4 * 128, xb / 8 - 4,
-                  j0 - 1, k, bar);
   };
   auto wait = [&](int k) {
     const int u = k - kfirst;
@@ -582,21 +567,13 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     if (hcol) Zh = __ldg(vz0 - 1);
   }
   const int* tp = S.tp_off + (long long)T * nz * 4;
-  // entry-list offsets of the next plane, loaded a plane ahead
-  int n0 = __ldg(tp + 4 * kfirst), n1 = __ldg(tp + 4 * kfirst + 1), n4 = __ldg(tp + 4 * kfirst + 4);
   for (int k = kfirst; k < z1; ++k) {
     const bool prologue = k < z0;
     rc.k = k;
     float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
     const float* st = ring + slot_of(k) * kStageFloats;
-    const uint32_t* mk = reinterpret_cast<const uint32_t*>(st + mko) + r * kMaskW;
-    const int off0 = n0, off1 = n1, off4 = n4;
-    if (k + 1 < z1) {
-      n0 = __ldg(tp + 4 * k + 4);
-      n1 = __ldg(tp + 4 * k + 5);
-      n4 = __ldg(tp + 4 * k + 8);
-    }
     wait(k);
+    const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
     const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
     const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
     const bool wplain = wplain_rx && pplane && (prologue || vplane);
@@ -609,8 +586,8 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
       const float X5 = st[cst + so + 4];
       const float4 Y1 = ld4(st + 2 * cst + so + kStageW);
       Z1 = k + 1 < nz ? ld4(st + vzo + so) : Pn;
-      if (has_mask)  // cell x0's word is x0/8 - (xb/8 - 4) of the staged row
-        nib = (mk[4 + (qx >> 1)] >> ((qx & 1) * 16)) &
+      if (has_mask)
+        nib = (__ldg(S.mask_bits + ((long long)k * ny + j) * S.mw + (x0 >> 3)) >> ((x0 & 4) * 4)) &
               0xFFFFu;
       if (wplain)
         Pn = has_mask ? p_plain_quad<R, true>(g, P4, X4, X5, Y0, Y1, Z0, Z1, nib)
@@ -621,8 +598,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     }
     if (hcol) {
       const float Zh1 = k + 1 < nz ? st[vzo + so - 1] : 0.f;
-      const bool open_p = !has_mask || ((mk[3] >> 28) & 1u) != 0;  // x = xb-1: word 3, nibble 7
-      pn[pq - 1] = p_update_cell<R>(S, rc, g, co, st, Zh, Zh1, so - 1, cst, xb - 1, open_p);
+      pn[pq - 1] = p_update_cell<R>(S, rc, g, co, st, Zh, Zh1, so - 1, cst, xb - 1);
       Zh = Zh1;
     }
     __syncthreads();

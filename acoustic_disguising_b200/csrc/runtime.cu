@@ -239,8 +239,7 @@ template double* solve_dalloc<double>(Solve&, size_t, int&);
 
 // The step kernel's TMA descriptors of the two field buffers: 4D tiled maps
 // (x: nxp, y: ny, z: nz, channel: 4) with the staged boxes (kStageW, ty+2, 1, 3)
-// for P, Vx, Vy and (kStageW, ty+2, 1, 1) for Vz, zero fill outside the grid;
-// and, for a masked solve, the mask's 3D map (words, rows, planes).  cuTensorMapEncodeTiled comes from the
+// for P, Vx, Vy and (kStageW, ty+2, 1, 1) for Vz, zero fill outside the grid.  cuTensorMapEncodeTiled comes from the
 // driver through the runtime's entry-point query (no link against libcuda).
 static int make_field_maps(Solve& s) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -271,20 +270,6 @@ static int make_field_maps(Solve& s) {
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
       return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  }
-  if (d.mask_bits) {  // the mask words of a plane's rows, 16 words from xb/8 - 4
-    const cuuint64_t mdims[3] = {(cuuint64_t)d.mw, (cuuint64_t)d.ny, (cuuint64_t)d.nz};
-    const cuuint64_t mstr[2] = {(cuuint64_t)d.mw * 4, (cuuint64_t)d.mw * d.ny * 4};
-    const cuuint32_t mbox[3] = {16, (cuuint32_t)(d.ty + 1), 1};
-    CUtensorMap* m = reinterpret_cast<CUtensorMap*>(s.fmap_host + 4 * 128);
-    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3,
-                              const_cast<uint32_t*>(d.mask_bits), mdims, mstr, mbox, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS)
-      return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled (mask) failed (" +
-                                    std::to_string((int)r) + ")");
   }
   int rc = ADF_OK;
   void* dm = dalloc<unsigned char>(s, sizeof(s.fmap_host), rc);
