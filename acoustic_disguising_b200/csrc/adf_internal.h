@@ -46,7 +46,11 @@ struct SolveDev {
   int it_first;      // step whose input field sits in buffer 0
   int ntx, mw;
   int src_ntx;            // columns of src[] (transceivers that inject)
-  int npp, nvp;           // x-slab psi row pitch (npml, npml+1 rounded up to 4)
+  // x-slab psi rows, quad-aligned: side 0 holds cell x at x, side 1 at
+  // x - xs1 (xs1p = (nx-npml) & ~3, xs1v = (nx-npml-1) & ~3), so that a quad's
+  // memory is one aligned float4 per side; npp, nvp: the row pitch
+  int npp, nvp;
+  int xs1p, xs1v;
   double fq, fv, rdx, rdy, rdz;
   float fqf, fvf, rdxf, rdyf, rdzf;
   float* field;

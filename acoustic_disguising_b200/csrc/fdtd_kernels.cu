@@ -137,19 +137,26 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
     upd[e] = x0 + e <= nx - 2 && !corner;
   }
   if (rc.pcpml && !plain_rigid) {
-    if (x0 < npml || x0 + 3 >= nx - npml) {  // x slab
+    const bool s0 = x0 < npml, s1 = x0 + 3 >= nx - npml;
+    // x slab: the quad's memory of a side is one aligned float4 (both sides
+    // only on grids narrower than two slabs and a quad: one after the other)
+    const long long row = ((long long)k * ny + j) * S.npp;
+    for (int sd = 0; sd < 2; ++sd) {
+      if (!(sd == 0 ? s0 : s1)) continue;
+      const long long o = sd == 0 ? row + x0 : S.psi_p_side[0] + row + (x0 - S.xs1p);
+      const float4 t = ld4(S.psi_p[0] + rc.rb * S.psi_p_buf[0] + o);
+      float m[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int x = x0 + e;
         const int side = x < npml ? 0 : (x >= nx - npml ? 1 : -1);
-        if (side >= 0 && upd[e]) {
+        if (side == sd && upd[e]) {
           const int l = side == 0 ? x : x - (nx - npml);
-          const long long o = side * S.psi_p_side[0] + ((long long)k * ny + j) * S.npp + l;
-          float m = S.psi_p[0][rc.rb * S.psi_p_buf[0] + o];
-          cpml_apply<R>(dvx[e], m, co[side * npml + l], co[4 * npml + 2 + side * npml + l]);
-          if (owned) S.psi_p[0][rc.wb * S.psi_p_buf[0] + o] = m;
+          cpml_apply<R>(dvx[e], m[e], co[side * npml + l], co[4 * npml + 2 + side * npml + l]);
         }
       }
+      // cells outside the slab or not updated write back what they read
+      if (owned) st4(S.psi_p[0] + rc.wb * S.psi_p_buf[0] + o, make_float4(m[0], m[1], m[2], m[3]));
     }
     const int ysd = j < npml ? 0 : (j >= ny - npml ? 1 : -1);
     if (ysd >= 0) {  // y slab: the whole quad, cells that are not updated keep their memory
@@ -215,7 +222,7 @@ __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& 
       if (xs >= 0) {
         const int l = xs == 0 ? x : x - (nx - npml);
         float m = S.psi_p[0][rc.rb * S.psi_p_buf[0] + xs * S.psi_p_side[0] +
-                             ((long long)k * ny + j) * S.npp + l];
+                             ((long long)k * ny + j) * S.npp + (xs == 0 ? x : x - S.xs1p)];
         cpml_apply<R>(dvx, m, co[xs * npml + l], co[4 * npml + 2 + xs * npml + l]);
       }
       const int ysd = j < npml ? 0 : (j >= ny - npml ? 1 : -1);
@@ -268,19 +275,24 @@ __device__ __forceinline__ void v_update_quad(const SolveDev& S, const RowCtx& r
     in[e] = x0 + e < nx;
   }
   if (rc.vcpml) {
-    if (x0 <= npml || x0 + 3 >= nx - npml - 1) {  // x slab
+    const bool s0 = x0 <= npml, s1 = x0 + 3 >= nx - npml - 1;
+    // x slab: one aligned float4 per side, the sides one after the other
+    const long long row = ((long long)k * ny + j) * S.nvp;
+    for (int sd = 0; sd < 2; ++sd) {
+      if (!(sd == 0 ? s0 : s1)) continue;
+      const long long o = sd == 0 ? row + x0 : S.psi_v_side[0] + row + (x0 - S.xs1v);
+      const float4 t = ld4(S.psi_v[0] + rc.rb * S.psi_v_buf[0] + o);
+      float m[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int x = x0 + e;
         const int side = x <= npml ? 0 : (x >= nx - npml - 1 ? 1 : -1);
-        if (side >= 0 && in[e] && x >= 1) {
+        if (side == sd && in[e] && x >= 1) {
           const int l = side == 0 ? x : x - (nx - npml - 1);
-          const long long o = side * S.psi_v_side[0] + ((long long)k * ny + j) * S.nvp + l;
-          float m = S.psi_v[0][rc.rb * S.psi_v_buf[0] + o];
-          cpml_apply<R>(dx[e], m, co[2 * npml + side * nm + l], co[6 * npml + 2 + side * nm + l]);
-          S.psi_v[0][rc.wb * S.psi_v_buf[0] + o] = m;
+          cpml_apply<R>(dx[e], m[e], co[2 * npml + side * nm + l], co[6 * npml + 2 + side * nm + l]);
         }
       }
+      st4(S.psi_v[0] + rc.wb * S.psi_v_buf[0] + o, make_float4(m[0], m[1], m[2], m[3]));
     }
     const int ysd = j < 1 ? -1 : (j <= npml ? 0 : (j >= ny - npml - 1 ? 1 : -1));
     if (ysd >= 0) {

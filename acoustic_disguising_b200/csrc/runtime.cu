@@ -323,8 +323,11 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
   rc = make_field_maps(s);
   if (rc) return rc;
   const long long n = npml, nm = npml + 1, nxp = d.nxp, ny = d.ny, nz = d.nz;
-  d.npp = (npml + 3) / 4 * 4;
-  d.nvp = (npml + 1 + 3) / 4 * 4;
+  // x-slab rows: side 1 starts at the quad holding its first cell
+  d.xs1p = std::max(0, d.nx - npml) / 4 * 4;
+  d.xs1v = std::max(0, d.nx - npml - 1) / 4 * 4;
+  d.npp = std::max((npml + 3) / 4 * 4, d.nxp - d.xs1p);
+  d.nvp = std::max((npml + 1 + 3) / 4 * 4, d.nxp - d.xs1v);
   const long long ps[3] = {nz * ny * d.npp, nz * n * nxp, n * ny * nxp};
   const long long vs[3] = {nz * ny * d.nvp, nz * nm * nxp, nm * ny * nxp};
   for (int a = 0; a < 3; ++a) {
@@ -731,14 +734,23 @@ static cudaError_t psi_copy(Solve& s, int axis, bool vside, float* host, bool up
   float* base = vside ? d.psi_v[axis] : d.psi_p[axis];
   const long long side = vside ? d.psi_v_side[axis] : d.psi_p_side[axis];
   float* dev = base + (long long)buffer * 2 * side;
-  if (axis == 0) {  // rows of n values, device pitch padded to npp / nvp
+  if (axis == 0) {  // rows of n values per side; device pitch npp / nvp, side 1 offset
     const size_t pitch = (size_t)(vside ? d.nvp : d.npp) * 4;
-    const size_t rows = (size_t)d.ny * d.nz * 2;
-    if (upload)
-      return cudaMemcpy2DAsync(dev, pitch, host, (size_t)n * 4, (size_t)n * 4, rows,
-                               cudaMemcpyHostToDevice, st);
-    return cudaMemcpy2D(host, (size_t)n * 4, dev, pitch, (size_t)n * 4, rows,
-                        cudaMemcpyDeviceToHost);
+    const size_t rows = (size_t)d.ny * d.nz;
+    const long long first1 = vside ? d.nx - d.npml - 1 : d.nx - d.npml;  // side 1's first cell
+    // (a grid narrower than npml+1 cells never uses side 1: any in-row offset does)
+    const long long off1 = first1 < 0 ? 0 : first1 - (vside ? d.xs1v : d.xs1p);
+    for (int sd = 0; sd < 2; ++sd) {
+      float* dv = dev + sd * side + (sd ? off1 : 0);
+      float* hs = host + (size_t)sd * rows * n;
+      const cudaError_t e =
+          upload ? cudaMemcpy2DAsync(dv, pitch, hs, (size_t)n * 4, (size_t)n * 4, rows,
+                                     cudaMemcpyHostToDevice, st)
+                 : cudaMemcpy2D(hs, (size_t)n * 4, dv, pitch, (size_t)n * 4, rows,
+                                cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
   }
   const size_t rows = axis == 1 ? (size_t)n * d.nz * 2 : (size_t)d.ny * n * 2;
   if (upload)
