@@ -57,9 +57,7 @@ struct SolveDev {
   // four CUtensorMaps (128 B each) over the field: per buffer 0, 1 one with
   // box (kStageW, ty + 2, 1, 3) (P, Vx, Vy of a plane) and one with box
   // (kStageW, ty + 2, 1, 1) (Vz); 4D (x: nxp, y: ny, z: nz, channel: 4),
-  // zero fill outside the grid; then (npml > 0) the y- and z-slab CPML
-  // memory psi_p[1], psi_v[1], psi_p[2], psi_v[2] as 4D maps (x, row or y,
-  // plane or slab plane, buffer*2 + side) with box (kStageW, ty + 1, 1, 1)
+  // zero fill outside the grid
   const void* fmap;
   long long buf_stride;   // floats per field buffer (4*nz*ny*nxp)
   long long chan_stride;  // floats per channel (nz*ny*nxp)

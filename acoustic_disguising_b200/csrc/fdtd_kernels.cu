@@ -29,7 +29,6 @@
 namespace adf {
 
 constexpr int kMaxCoef = 8 * 63 + 4;  // CPML coefficients for npml <= 63
-constexpr int kPsiBox = kStageW * 8;    // a staged CPML memory box: kStageW x (kMaxTy + 1)
 
 // ---------------------------------------------------------------------------
 // Arithmetic policies
@@ -93,13 +92,6 @@ struct Sc {  // per-solve update scalars in registers
 struct RowCtx {
   int nx, ny, nz, npml, nxp, j, k, rb, wb;
   bool pcpml, vcpml;
-  // y/z-slab CPML memory staged for this plane: the p- and v-side boxes
-  // (rows j0-1 .. j0+ty-1, x = xb-4 .. xb+67), which slab each holds
-  // (0/1: y side 0/1, 2/3: z side 0/1, -1: none, read from global memory)
-  // and the shared-window address of this quad in the p-side box (the
-  // v-side box follows at + 4 kPsiBox bytes)
-  uint32_t pbox;
-  int pcode, vcode;
 };
 
 // ---------------------------------------------------------------------------
@@ -170,8 +162,7 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
     if (ysd >= 0) {  // y slab: the whole quad, cells that are not updated keep their memory
       const int yl = ysd == 0 ? j : j - (ny - npml);
       const long long o = ysd * S.psi_p_side[1] + ((long long)k * npml + yl) * rc.nxp + x0;
-      const float4 m4 =
-          rc.pcode == ysd ? lds4(rc.pbox) : ld4(S.psi_p[1] + rc.rb * S.psi_p_buf[1] + o);
+      const float4 m4 = ld4(S.psi_p[1] + rc.rb * S.psi_p_buf[1] + o);
       float m[4] = {m4.x, m4.y, m4.z, m4.w};
       const float a = co[ysd * npml + yl], b = co[4 * npml + 2 + ysd * npml + yl];
 #pragma unroll
@@ -183,8 +174,7 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
     if (zsd >= 0) {
       const int zl = zsd == 0 ? k : k - (nz - npml);
       const long long o = zsd * S.psi_p_side[2] + ((long long)zl * ny + j) * rc.nxp + x0;
-      const float4 m4 =
-          rc.pcode == 2 + zsd ? lds4(rc.pbox) : ld4(S.psi_p[2] + rc.rb * S.psi_p_buf[2] + o);
+      const float4 m4 = ld4(S.psi_p[2] + rc.rb * S.psi_p_buf[2] + o);
       float m[4] = {m4.x, m4.y, m4.z, m4.w};
       const float a = co[zsd * npml + zl], b = co[4 * npml + 2 + zsd * npml + zl];
 #pragma unroll
@@ -238,18 +228,15 @@ __device__ __forceinline__ float p_update_cell(const SolveDev& S, const RowCtx& 
       const int ysd = j < npml ? 0 : (j >= ny - npml ? 1 : -1);
       if (ysd >= 0) {
         const int yl = ysd == 0 ? j : j - (ny - npml);
-        float m = rc.pcode == ysd ? lds1(rc.pbox - 4)
-                                  : S.psi_p[1][rc.rb * S.psi_p_buf[1] + ysd * S.psi_p_side[1] +
-                                               ((long long)k * npml + yl) * nxp + x];
+        float m = S.psi_p[1][rc.rb * S.psi_p_buf[1] + ysd * S.psi_p_side[1] +
+                             ((long long)k * npml + yl) * nxp + x];
         cpml_apply<R>(dvy, m, co[ysd * npml + yl], co[4 * npml + 2 + ysd * npml + yl]);
       }
       const int zsd = k < npml ? 0 : (k >= nz - npml ? 1 : -1);
       if (zsd >= 0) {
         const int zl = zsd == 0 ? k : k - (nz - npml);
-        float m = rc.pcode == 2 + zsd
-                      ? lds1(rc.pbox - 4)
-                      : S.psi_p[2][rc.rb * S.psi_p_buf[2] + zsd * S.psi_p_side[2] +
-                                   ((long long)zl * ny + j) * nxp + x];
+        float m = S.psi_p[2][rc.rb * S.psi_p_buf[2] + zsd * S.psi_p_side[2] +
+                             ((long long)zl * ny + j) * nxp + x];
         cpml_apply<R>(dvz, m, co[zsd * npml + zl], co[4 * npml + 2 + zsd * npml + zl]);
       }
     }
@@ -311,8 +298,7 @@ __device__ __forceinline__ void v_update_quad(const SolveDev& S, const RowCtx& r
     if (ysd >= 0) {
       const int yl = ysd == 0 ? j : j - (ny - npml - 1);
       const long long o = ysd * S.psi_v_side[1] + ((long long)k * nm + yl) * rc.nxp + x0;
-      const float4 m4 = rc.vcode == ysd ? lds4(rc.pbox + 4 * kPsiBox)
-                                         : ld4(S.psi_v[1] + rc.rb * S.psi_v_buf[1] + o);
+      const float4 m4 = ld4(S.psi_v[1] + rc.rb * S.psi_v_buf[1] + o);
       float m[4] = {m4.x, m4.y, m4.z, m4.w};
       const float a = co[2 * npml + ysd * nm + yl], b = co[6 * npml + 2 + ysd * nm + yl];
 #pragma unroll
@@ -324,8 +310,7 @@ __device__ __forceinline__ void v_update_quad(const SolveDev& S, const RowCtx& r
     if (zsd >= 0) {
       const int zl = zsd == 0 ? k : k - (nz - npml - 1);
       const long long o = zsd * S.psi_v_side[2] + ((long long)zl * ny + j) * rc.nxp + x0;
-      const float4 m4 = rc.vcode == 2 + zsd ? lds4(rc.pbox + 4 * kPsiBox)
-                                             : ld4(S.psi_v[2] + rc.rb * S.psi_v_buf[2] + o);
+      const float4 m4 = ld4(S.psi_v[2] + rc.rb * S.psi_v_buf[2] + o);
       float m[4] = {m4.x, m4.y, m4.z, m4.w};
       const float a = co[2 * npml + zsd * nm + zl], b = co[6 * npml + 2 + zsd * nm + zl];
 #pragma unroll
@@ -581,61 +566,8 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     if (!mbar_wait(smem_u32(rbar + u % kStepRing), (uint32_t)(u / kStepRing) & 1u, kStepWaitLimit))
       atomicOr(S.err, 4);  // reported as ADF_E_TIMEOUT; the values read are wrong
   };
-  // The y/z-slab CPML memory of plane k: one p-side and one v-side box
-  // (rows j0-1 .. j0+ty-1, the stage's x range), each holding the slab the
-  // tile's rows or the plane lie in (a y slab first; a tile in two y sides
-  // or in a y and a z slab reads the other one from global memory).  The
-  // boxes have a two-slot ring of their own, refilled a plane later than the
-  // field's, since the v-side box is read after the plane's barrier.
-  float* pring = ring + kStepRing * kStageFloats;
-  const char* fm = static_cast<const char*>(S.fmap);
-  auto pcode_of = [&](int k) {
-    if (!pcp) return -1;
-    if (j0 - 1 < npml) return 0;
-    if (j0 + ty - 1 >= ny - npml) return 1;
-    return k < npml ? 2 : (k >= nz - npml ? 3 : -1);
-  };
-  auto vcode_of = [&](int k) {
-    if (!vcp || k < z0) return -1;  // the prologue plane has no velocity update
-    if (j0 <= npml) return 0;
-    if (j0 + ty - 1 >= ny - npml - 1) return 1;
-    return k < 1 ? -1 : (k <= npml ? 2 : (k >= nz - npml - 1 ? 3 : -1));
-  };
-  const uint32_t box_bytes = (uint32_t)(4 * kStageW * (ty + 1));
-  auto issue_psi = [&](int k) {  // one thread; zero bytes completes the phase at once
-    const int sl = (k - kfirst) & 1, pc = pcode_of(k), vc = vcode_of(k);
-    fence_proxy_async_smem();
-    const uint32_t bar = smem_u32(rbar + kStepRing + sl);
-    mbar_expect_tx(bar, (pc >= 0 ? box_bytes : 0u) + (vc >= 0 ? box_bytes : 0u));
-    float* dst = pring + sl * 2 * kPsiBox;
-    if (pc >= 0) {
-      const int sd = pc & 1;
-      if (pc < 2)
-        tma_load_4d(smem_u32(dst), fm + 4 * 128, xb - 4, j0 - 1 - (sd ? ny - npml : 0), k,
-                    2 * rb + sd, bar);
-      else
-        tma_load_4d(smem_u32(dst), fm + 6 * 128, xb - 4, j0 - 1, sd ? k - (nz - npml) : k,
-                    2 * rb + sd, bar);
-    }
-    if (vc >= 0) {
-      const int sd = vc & 1;
-      if (vc < 2)
-        tma_load_4d(smem_u32(dst + kPsiBox), fm + 5 * 128, xb - 4,
-                    j0 - 1 - (sd ? ny - npml - 1 : 0), k, 2 * rb + sd, bar);
-      else
-        tma_load_4d(smem_u32(dst + kPsiBox), fm + 7 * 128, xb - 4, j0 - 1,
-                    sd ? k - (nz - npml - 1) : k, 2 * rb + sd, bar);
-    }
-  };
-  auto wait_psi = [&](int k) {
-    const int u = k - kfirst;
-    if (!mbar_wait(smem_u32(rbar + kStepRing + (u & 1)), (uint32_t)(u >> 1) & 1u, kStepWaitLimit))
-      atomicOr(S.err, 4);
-  };
-  if (tid == 0) {
+  if (tid == 0)
     for (int k = kfirst; k < min(z1, kfirst + kStepRing); ++k) issue(k);
-    issue_psi(kfirst);
-  }
   // Vz of plane kfirst (the stages carry the next plane's), and of the halo
   // column for its single-cell update
   float4 Z0 = make_float4(0.f, 0.f, 0.f, 0.f), Pzm = Z0;
@@ -653,10 +585,6 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
     const float* st = ring + slot_of(k) * kStageFloats;
     wait(k);
-    wait_psi(k);
-    rc.pcode = pcode_of(k);
-    rc.vcode = vcode_of(k);
-    rc.pbox = smem_u32(pring + ((k - kfirst) & 1) * 2 * kPsiBox + so);
     const int off0 = __ldg(tp + 4 * k), off1 = __ldg(tp + 4 * k + 1), off4 = __ldg(tp + 4 * k + 4);
     const bool pplane = k != nz - 1 && (!pcp || (k >= npml && k < nz - npml));
     const bool vplane = k >= 1 && (!vcp || (k > npml && k < nz - npml - 1));
@@ -687,11 +615,7 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     }
     __syncthreads();
     // every read of plane k's stage is done: refill its slot
-    if (tid == 0) {
-      if (k + kStepRing < z1) issue(k + kStepRing);
-      // plane k-1's CPML slot: its velocity update finished before this barrier
-      if (k + 1 < z1) issue_psi(k + 1);
-    }
+    if (tid == 0 && k + kStepRing < z1) issue(k + kStepRing);
     // ---- q channel: inject/record on the new P (forward.jl:92) ----
     if (off0 < off1) {
       apply_entries(S, off0, off1, 0, nxp, xb - 1, xb + kXT, xb, !prologue, it, tid, nthr,
@@ -765,17 +689,13 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
 #endif
 constexpr int kStepCtasPerSm = ADF_STEP_CTAS_PER_SM;  // register budget: 65536 / (128 x this)
 // (+128 B so that the ring can start on a 128-B boundary, as TMA destinations must)
-constexpr size_t kStepDynSmem =
-    sizeof(float) * (kStepRing * kStageFloats + 2 * 2 * kPsiBox) + 128;
-static_assert(kPsiBox == kStageW * (kMaxTy + 1), "CPML boxes hold a tile's rows");
-static_assert((kStageFloats * 4) % 128 == 0 && (kPsiBox * 4) % 128 == 0,
-              "CPML boxes start 128-B aligned");
+constexpr size_t kStepDynSmem = sizeof(float) * kStepRing * kStageFloats + 128;
 
 __global__ void __launch_bounds__(kStepThreads, kStepCtasPerSm) adf_fdtd_step_kernel(const StepParams p) {
   extern __shared__ __align__(128) float dyn_smem[];
   float* ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dyn_smem) + 127) &
                                          ~static_cast<uintptr_t>(127));
-  __shared__ __align__(8) uint64_t rbar[kStepRing + 2];  // field ring, then CPML ring
+  __shared__ __align__(8) uint64_t rbar[kStepRing];
   __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
   __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
   __shared__ float s_co[kMaxCoef];
@@ -792,7 +712,7 @@ __global__ void __launch_bounds__(kStepThreads, kStepCtasPerSm) adf_fdtd_step_ke
     const int ncoef = 8 * G.npml + 4;
     for (int w = tid; w < ncoef; w += nthr) s_co[w] = G.coef[w];
     if (tid == 0) {
-      for (int q = 0; q < kStepRing + 2; ++q) mbar_init(smem_u32(rbar + q), 1);
+      for (int q = 0; q < kStepRing; ++q) mbar_init(smem_u32(rbar + q), 1);
       fence_mbar_init();
     }
   }

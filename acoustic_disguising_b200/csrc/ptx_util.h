@@ -71,20 +71,6 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int x
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(mbar)
       : "memory");
 }
-// Loads through a 32-bit shared-window address.
-__device__ __forceinline__ float4 lds4(uint32_t a) {
-  float4 v;
-  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "r"(a)
-               : "memory");
-  return v;
-}
-__device__ __forceinline__ float lds1(uint32_t a) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
-  return v;
-}
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

@@ -271,28 +271,6 @@ static int make_field_maps(Solve& s) {
     if (r != CUDA_SUCCESS)
       return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   }
-  // y- and z-slab CPML memory, [2 buffers][2 sides][...][...][nxp] each, as
-  // 4D maps (x, slab row or y, z or slab plane, buffer*2 + side) with the
-  // box (kStageW, ty + 1, 1, 1): rows j0-1 .. j0+ty-1 of one plane
-  if (d.npml > 0) {
-    const long long n = d.npml;
-    const long long e[4][3] = {{n, d.nz, 0}, {n + 1, d.nz, 0}, {d.ny, n, 0}, {d.ny, n + 1, 0}};
-    float* base[4] = {d.psi_p[1], d.psi_v[1], d.psi_p[2], d.psi_v[2]};
-    const cuuint32_t pbox[4] = {(cuuint32_t)kStageW, (cuuint32_t)(d.ty + 1), 1, 1};
-    for (int q = 0; q < 4; ++q) {
-      const cuuint64_t pd[4] = {(cuuint64_t)d.nxp, (cuuint64_t)e[q][0], (cuuint64_t)e[q][1], 4};
-      const cuuint64_t pst[3] = {(cuuint64_t)d.nxp * 4, (cuuint64_t)(d.nxp * e[q][0]) * 4,
-                                 (cuuint64_t)(d.nxp * e[q][0] * e[q][1]) * 4};
-      CUtensorMap* m = reinterpret_cast<CUtensorMap*>(s.fmap_host + 128 * (4 + q));
-      const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base[q], pd, pst, pbox,
-                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return fail(ADF_E_DEVICE, "cuTensorMapEncodeTiled (CPML) failed (" +
-                                      std::to_string((int)r) + ")");
-    }
-  }
   int rc = ADF_OK;
   void* dm = dalloc<unsigned char>(s, sizeof(s.fmap_host), rc);
   if (rc) return rc;
@@ -342,6 +320,8 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
     if (rc) return rc;
     d.mask_bits = s.mask_bits;
   }
+  rc = make_field_maps(s);
+  if (rc) return rc;
   const long long n = npml, nm = npml + 1, nxp = d.nxp, ny = d.ny, nz = d.nz;
   // x-slab rows: side 1 starts at the quad holding its first cell
   d.xs1p = std::max(0, d.nx - npml) / 4 * 4;
@@ -363,8 +343,6 @@ int solve_alloc(adf_ctx* ctx, Solve& s, const hm::Dom& dom, int npml, bool has_m
       cudaMemsetAsync(d.psi_v[a], 0, (size_t)4 * vs[a] * 4, s.stream);
     }
   }
-  rc = make_field_maps(s);
-  if (rc) return rc;
   float* coef = dalloc<float>(s, (size_t)8 * n + 4, rc);
   if (rc) return rc;
   cudaMemsetAsync(coef, 0, ((size_t)8 * n + 4) * 4, s.stream);

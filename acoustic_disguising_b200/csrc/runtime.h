@@ -69,7 +69,7 @@ void tune_force(Tune t);  // {0,0} releases
 
 struct Solve {
   SolveDev dev;
-  unsigned char fmap_host[8 * 128];  // the tensor maps of dev.fmap (copied to the device)
+  unsigned char fmap_host[4 * 128];  // the tensor maps of dev.fmap (copied to the device)
   std::vector<void*> allocs;
   size_t bytes = 0;
   int nzc = 32;
