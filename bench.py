@@ -101,6 +101,8 @@ def parse():
     ap.add_argument("--no-gf", action="store_true", help="skip the in-loop GF section")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity section")
     ap.add_argument("--no-hologram", action="store_true", help="skip the 512^3 hologram section")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="use the tune table / default tile shape (profiling runs)")
     ap.add_argument("--hologram-only", action="store_true",
                     help="run only the 512^3 hologram section and print it (profiling runs)")
     ap.add_argument("--hologram-nt", type=int, default=H_NT)
@@ -675,6 +677,26 @@ def hologram_section(A, ctx, nt=H_NT):
             "kh_out_rms": float(np.sqrt(np.mean(out.astype(np.float64) ** 2)))}
 
 
+def fp32_section(A, ctx, batch, nt=96):
+    """The headline launch (batch x 256^3 GF solves) with Float32 arithmetic
+    instead of the reference's Float64 promotion: what the promotion costs.
+    Not the headline: the reference computes in Float64."""
+    _, reqs = make_requests(A, 0, batch, "fp32", nt)
+    A.gf_solve_batch(reqs, batched=True, ctx=ctx)  # warm
+    ctx.set_kernel_timing(True)
+    ctx.kernel_timing(reset=True)
+    _, reqs = make_requests(A, 0, batch, "fp32", nt)
+    A.gf_solve_batch(reqs, batched=True, ctx=ctx)
+    k_ms, k_n = ctx.kernel_timing(reset=True)
+    ctx.set_kernel_timing(False)
+    per = k_ms / max(k_n, 1)
+    return {"workload": f"{batch} x 256^3 GF solves as the headline, {nt} steps, Float32 "
+                        "arithmetic (all updates in Float32, as ParallelStencil would compute "
+                        "them if it narrowed the Float64 Domain scalars)",
+            "mean_launch_ms": per,
+            "achieved_gbs": batch * algorithmic_bytes_per_solve_step() / (per / 1e3) / 1e9}
+
+
 # ---------------------------------------------------------------------------
 # In-loop GF extrapolation (run_fdtd! gf_map = PVFromPin) on a 128^3 run
 # ---------------------------------------------------------------------------
@@ -767,6 +789,10 @@ def b200_arm(args):
             dist.barrier()
 
     B = args.batch
+    # the product's tuner picks this grid's tile shape (stored in the tune
+    # table beside the library, which every later solve of the size reads)
+    tuned = (A.autotune(N, N, N, npml=NPML, n_solves=B, steps=32, ctx=ctx) if not args.no_tune
+             else ("table/default", "table/default"))
     step_ix = 0
     # the caller's result buffers (p and v_n traces of every solve), page-locked
     # once and reused by every step, as a serving caller keeps its buffers
@@ -817,6 +843,8 @@ def b200_arm(args):
         extra["gf_map"] = gf_section(A, ctx)
     if world == 1 and not args.no_step512:
         extra["step512"] = step512_section(A, ctx)
+    if world == 1 and args.arith == "promote":
+        extra["arith_fp32"] = fp32_section(A, ctx, B)
     if world == 1 and not args.no_hologram:
         extra["hologram512"] = hologram_section(A, ctx)
     if world == 1 and not args.no_serving:
@@ -875,6 +903,7 @@ def b200_arm(args):
         "gcell_upd_per_s": cells * NT * solves / (dev_total / 1e3) / 1e9,
         "clocks": clk,
         "region_wall_s": region,
+        "tile": {"ty": tuned[0], "nzc": tuned[1], "chosen_by": "adf_autotune"},
     }
     line.update(extra)
     if world == 1 and not args.no_cpu_baseline:
