@@ -92,10 +92,6 @@ struct Sc {  // per-solve update scalars in registers
 struct RowCtx {
   int nx, ny, nz, npml, nxp, j, k, rb, wb;
   bool pcpml, vcpml;
-  // this quad's x-slab CPML memory of the plane, prefetched into shared
-  // memory (p side at xpre, v side at xpre + 16) when xp / xv
-  bool xp, xv;
-  uint32_t xpre;
 };
 
 // ---------------------------------------------------------------------------
@@ -148,7 +144,7 @@ __device__ __forceinline__ float4 p_update_quad(const SolveDev& S, const RowCtx&
     for (int sd = 0; sd < 2; ++sd) {
       if (!(sd == 0 ? s0 : s1)) continue;
       const long long o = sd == 0 ? row + x0 : S.psi_p_side[0] + row + (x0 - S.xs1p);
-      const float4 t = rc.xp ? lds4(rc.xpre) : ld4(S.psi_p[0] + rc.rb * S.psi_p_buf[0] + o);
+      const float4 t = ld4(S.psi_p[0] + rc.rb * S.psi_p_buf[0] + o);
       float m[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -285,8 +281,7 @@ __device__ __forceinline__ void v_update_quad(const SolveDev& S, const RowCtx& r
     for (int sd = 0; sd < 2; ++sd) {
       if (!(sd == 0 ? s0 : s1)) continue;
       const long long o = sd == 0 ? row + x0 : S.psi_v_side[0] + row + (x0 - S.xs1v);
-      const float4 t =
-          rc.xv ? lds4(rc.xpre + 16) : ld4(S.psi_v[0] + rc.rb * S.psi_v_buf[0] + o);
+      const float4 t = ld4(S.psi_v[0] + rc.rb * S.psi_v_buf[0] + o);
       float m[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -492,7 +487,7 @@ static_assert((stage_vz_offset(5 * kStageW) * 4) % 128 == 0, "Vz boxes start 128
 template <typename R>
 __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S, int4 item, int it,
                                           float* sPn, float* sV, const float* co, float* ring,
-                                          uint64_t* rbar, float4* sXP) {
+                                          uint64_t* rbar) {
   const int lane = threadIdx.x, wid = threadIdx.y;
   const int tid = wid * 32 + lane, nthr = blockDim.x * blockDim.y;
   const int nx = S.nx, ny = S.ny, nz = S.nz, nxp = S.nxp, ty = S.ty, npml = S.npml;
@@ -583,42 +578,8 @@ __device__ __forceinline__ void step_item(const StepParams& p, const SolveDev& S
     if (act) Z0 = ldg4(vz0);
     if (hcol) Zh = __ldg(vz0 - 1);
   }
-  // The quad's x-slab CPML memory (one float4 per side and update) of the
-  // next plane is prefetched by cp.async into this thread's slot of a
-  // two-plane shared buffer, when the quad lies in exactly one side of the
-  // slab: the boundary warp's two dependent global loads per plane leave
-  // the critical path.  Only the issuing thread reads its slot (no barrier).
-  const bool xpf = act && pcp && ((x0 < npml) != (x0 + 3 >= nx - npml));
-  const bool xvf = vrow && vcp && ((x0 <= npml) != (x0 + 3 >= nx - npml - 1));
-  auto xslot = [&](int kk) { return smem_u32(sXP + ((kk & 1) * kStepThreads + tid) * 2); };
-  auto xprefetch = [&](int kk) {
-    const uint32_t d = xslot(kk);
-    if (xpf) {
-      const long long o = (x0 < npml ? (long long)x0 : S.psi_p_side[0] + x0 - S.xs1p) +
-                          ((long long)kk * ny + j) * S.npp;
-      cp_async16(d, S.psi_p[0] + rb * S.psi_p_buf[0] + o);
-    }
-    if (xvf) {
-      const long long o = (x0 <= npml ? (long long)x0 : S.psi_v_side[0] + x0 - S.xs1v) +
-                          ((long long)kk * ny + j) * S.nvp;
-      cp_async16(d + 16, S.psi_v[0] + rb * S.psi_v_buf[0] + o);
-    }
-    cp_async_commit();
-  };
-  rc.xp = xpf;
-  rc.xv = xvf;
-  if (xpf || xvf) xprefetch(kfirst);
   const int* tp = S.tp_off + (long long)T * nz * 4;
   for (int k = kfirst; k < z1; ++k) {
-    if (xpf || xvf) {
-      if (k + 1 < z1) {
-        xprefetch(k + 1);
-        cp_async_wait<1>();  // plane k's copies are done
-      } else {
-        cp_async_wait<0>();
-      }
-      rc.xpre = xslot(k);
-    }
     const bool prologue = k < z0;
     rc.k = k;
     float* pn = sPn + (k & 1) * (kMaxTy + 1) * kPnPitch;
@@ -736,7 +697,6 @@ __global__ void __launch_bounds__(kStepThreads, kStepCtasPerSm) adf_fdtd_step_ke
                                          ~static_cast<uintptr_t>(127));
   __shared__ __align__(8) uint64_t rbar[kStepRing];
   __shared__ __align__(16) float sPn[2 * (kMaxTy + 1) * kPnPitch];
-  __shared__ __align__(16) float4 sXP[2 * kStepThreads * 2];  // prefetched x-slab CPML memory
   __shared__ __align__(16) float sV[3 * kMaxTy * kXT];
   __shared__ float s_co[kMaxCoef];
   __shared__ __align__(16) SolveDev S;  // the solve descriptor, read in the hot loop
@@ -758,9 +718,9 @@ __global__ void __launch_bounds__(kStepThreads, kStepCtasPerSm) adf_fdtd_step_ke
   }
   __syncthreads();
   if (S.flags & SF_FP32)
-    step_item<float>(p, S, item, it, sPn, sV, s_co, ring, rbar, sXP);
+    step_item<float>(p, S, item, it, sPn, sV, s_co, ring, rbar);
   else
-    step_item<double>(p, S, item, it, sPn, sV, s_co, ring, rbar, sXP);
+    step_item<double>(p, S, item, it, sPn, sV, s_co, ring, rbar);
 }
 
 // Per-step trace assembly (derivatives.jl:51-56 record sums in corner order,

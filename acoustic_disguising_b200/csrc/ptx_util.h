@@ -71,26 +71,6 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void* map, int x
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(mbar)
       : "memory");
 }
-// Per-thread asynchronous 16-B copy global -> shared (both 16-B aligned),
-// completed by cp_async_wait<n>: all but the n most recent committed groups.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-__device__ __forceinline__ float4 lds4(uint32_t a) {
-  float4 v;
-  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "r"(a)
-               : "memory");
-  return v;
-}
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
