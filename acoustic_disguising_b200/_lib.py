@@ -89,10 +89,11 @@ class GfMapC(C.Structure):
     _fields_ = [("kind", C.c_int), ("nt_gf", C.c_int64), ("n1", C.c_int64), ("n2", C.c_int64),
                 ("t", C.c_void_p * 4), ("i_src", C.c_void_p), ("n_src", C.c_int64),
                 ("i_rec", C.c_void_p), ("n_rec", C.c_int64), ("z0", C.c_double),
-                ("discard", C.c_int)]
+                ("discard", C.c_int), ("contraction", C.c_int)]
 
 
 GF_KINDS = {"PVFromPin": 0, "PFromPin": 1, "PVFromPV": 2}
+GF_CONTRACTIONS = {"fp64": 0, "tf32x3": 1}  # ADF_GF_CONTRACT_*
 
 
 STEP_CB = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_void_p)

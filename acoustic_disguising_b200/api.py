@@ -368,13 +368,18 @@ class GfMap:
     kind "PVFromPV": (pp, pv, vp, vv), each (nt_gf, #iRec, #iSrc).
     i_src / i_rec are 1-based transceiver indices.  discard=True reproduces
     the reference as shipped, whose extrapolate! writes into slice copies so
-    the sources never change."""
+    the sources never change.  contraction "fp64" (default) sums every lag
+    with Float64 FMAs, as the reference accumulates; "tf32x3" sums the lags
+    older than the current 32-step block on the tensor cores (the two
+    *FromPin kinds; TF32 split into three products, within about 1e-6 of the
+    Float64 sums), keeping the map a second time as operand tiles."""
 
     kind: str
     tensors: tuple
     i_src: np.ndarray
     i_rec: np.ndarray
     discard: bool = False
+    contraction: str = "fp64"
 
     def _c(self, z0: float):
         self._t = [np.asfortranarray(t, np.float32) for t in self.tensors]
@@ -387,18 +392,19 @@ class GfMap:
         g = L.GfMapC(kind=L.GF_KINDS[self.kind], nt_gf=self._t[0].shape[0],
                      n1=self._t[0].shape[1], n2=self._t[0].shape[2], i_src=self._is.ctypes.data,
                      n_src=self._is.size, i_rec=self._ir.ctypes.data, n_rec=self._ir.size,
-                     z0=float(z0), discard=int(bool(self.discard)))
+                     z0=float(z0), discard=int(bool(self.discard)),
+                     contraction=L.GF_CONTRACTIONS[self.contraction])
         for k, t in enumerate(self._t):
             g.t[k] = t.ctypes.data
         return g
 
 
-def PVFromPin(p_pin, v_pin, i_src, i_rec, discard=False) -> GfMap:
-    return GfMap("PVFromPin", (p_pin, v_pin), i_src, i_rec, discard)
+def PVFromPin(p_pin, v_pin, i_src, i_rec, discard=False, contraction="fp64") -> GfMap:
+    return GfMap("PVFromPin", (p_pin, v_pin), i_src, i_rec, discard, contraction)
 
 
-def PFromPin(pos, neg, i_src, i_rec, discard=False) -> GfMap:
-    return GfMap("PFromPin", (pos, neg), i_src, i_rec, discard)
+def PFromPin(pos, neg, i_src, i_rec, discard=False, contraction="fp64") -> GfMap:
+    return GfMap("PFromPin", (pos, neg), i_src, i_rec, discard, contraction)
 
 
 def PVFromPV(pp, pv, vp, vv, i_src, i_rec, discard=False) -> GfMap:

@@ -26,6 +26,7 @@ enum : int {
   SF_VCPML = 4,     // v-side CPML active (npml>=1)
   SF_FP32 = 8,      // Float32 arithmetic instead of Float64 intermediates
   SF_GF = 32,       // in-loop GF extrapolation between v2vn and vn2v
+  SF_GF_TC = 64,    // its far lags on the tensor cores (TF32 split, gf_tc)
 };
 
 // Steps per block of the in-loop GF extrapolation: lags older than the block
@@ -100,7 +101,9 @@ struct SolveDev {
   int gf_ks;              // receiver splits per driven source (per-step kernel)
   int gf_rs;              // receiver splits of the far-lag kernel, 0 = no blocking
   int gf_nl;              // lags held in gf_near: min(kGfBlock, nt_gf)
-  int gf_pad_;
+  int gf_tc_nch;          // 16-lag chunks of gf_tc
+  const float* gf_tc;     // SF_GF_TC: the two tensors packed as tensor-core operand tiles
+                          // [n_in][gf_tc_nch][128-source tiles][2][16 lags x 128 sources]
 };
 
 // work item: {solve index, y tile | x tile << 16, z0, z1}
@@ -131,5 +134,12 @@ cudaError_t launch_gf_extrapolate(const EpiParams& p, int max_blocks, int max_ns
 // that starts at launch-step p.step
 cudaError_t launch_gf_near_pack(const SolveDev& d, float* near, cudaStream_t s);
 cudaError_t launch_gf_far(const EpiParams& p, int max_blocks, int max_nsrc, cudaStream_t s);
+// the same on the tensor cores for SF_GF_TC solves (gf_tc_kernel.cu): blocks =
+// 128-source tiles x gf_rs; launch_gf_far's combine step then adds the splits
+cudaError_t launch_gf_far_tc(const EpiParams& p, int max_blocks, cudaStream_t s);
+cudaError_t launch_gf_tc_pack(const SolveDev& d, float* out, cudaStream_t s);
+int64_t gf_tc_chunks(int64_t nt_gf);  // 16-lag chunks of lags 1 .. nt_gf-1
+size_t gf_tc_packed_floats(int64_t nt_gf, int64_t n_src, int64_t n_rec);
+int gf_tc_sources_per_tile();
 
 }  // namespace adf

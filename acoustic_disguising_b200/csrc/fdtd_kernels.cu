@@ -972,7 +972,8 @@ constexpr int kGfOT = 64;  // sources per tile (two per thread)
 __global__ void __launch_bounds__(256) adf_gf_far_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it0 = S.it_base + p.step;
-  if (S.gf_rs <= 0 || it0 > S.it_stop || it0 >= S.nt || !(S.flags & SF_GF)) return;
+  if (S.gf_rs <= 0 || it0 > S.it_stop || it0 >= S.nt || !(S.flags & SF_GF) || (S.flags & SF_GF_TC))
+    return;  // (tensor-core solves: adf_gf_far_tc_kernel)
   const int rsn = S.gf_rs, nout = S.gf_nout;
   const int ot = blockIdx.x / rsn, rsi = blockIdx.x - ot * rsn;
   if (ot * kGfOT >= nout) return;
@@ -1146,9 +1147,11 @@ cudaError_t launch_gf_near_pack(const SolveDev& d, float* near, cudaStream_t s) 
 }
 
 cudaError_t launch_gf_far(const EpiParams& p, int max_blocks, int max_nsrc, cudaStream_t s) {
-  adf_gf_far_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), 256, 0, s>>>(p);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if (max_blocks > 0) {  // 0: every blocked solve of the batch is on the tensor cores
+    adf_gf_far_kernel<<<dim3(max_blocks, p.n_solves), 256, 0, s>>>(p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   adf_gf_far_combine_kernel<<<dim3((max_nsrc * kGfBlock + 255) / 256, p.n_solves), 256, 0, s>>>(p);
   return cudaGetLastError();
 }

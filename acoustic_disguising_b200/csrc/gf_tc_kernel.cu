@@ -1,0 +1,377 @@
+// gf_tc_kernel.cu -- the far-lag part of the in-loop GF extrapolation on the
+// tensor cores (tcgen05.mma, kind::tf32, accumulators in tensor memory).
+//
+// extrapolate_pv_from_pin! and extrapolate_p_from_pin
+// (src/kernels/extrapolation.jl:139-193) sum, for step it and driven source o,
+//     sum_r sum_lag G[lag, o, r] * pin[it-1-lag, r].
+// In the block-causal form (adf_gf_far_kernel in fdtd_kernels.cu) the lags
+// older than the current block of kGfBlock steps are summed once per block.
+// Per receiver r that is a matrix product: the source x lag slice of the map
+// (A: 128 sources x 16 lags per chunk) times the block's masked Toeplitz
+// window of the input history (B: 32 steps x 16 lags, B[b][l] =
+// pin[it0-1+b-lag, r] on the far lags of step b, zero elsewhere).  Here that
+// product runs on tcgen05.mma with FP32 accumulation in tensor memory.  Every
+// Float32 map entry and Float64 history sample is split into a TF32 part
+// (rounded to nearest) and the remainder, and hi*hi + hi*lo + lo*hi is
+// accumulated (the dropped lo*lo term is below 2^-22 of the product).  After
+// the last chunk of a receiver its accumulator is added into per-thread
+// Float64 sums (two accumulator sets in tensor memory alternate, so one is
+// drained while the next receiver's products run), so the sum over receivers
+// stays in Float64.  The result agrees with the Float64 sum to about 1e-6
+// relative, Float32 level: an opt-in contraction (ADF_GF_CONTRACT_TF32X3);
+// the default path keeps the Float64 FMAs of the reference's accumulation.
+//
+// Data path: the two tensors of the map are packed once per map
+// (adf_gf_tc_pack_kernel) into 16 KB tiles (receiver, 16-lag chunk,
+// 128-source tile) laid out as the MMA's K-major, no-swizzle operand (8-row x
+// 16-byte core matrices), so one bulk copy (cp.async.bulk, completing on an
+// mbarrier, no multicast) stages a chunk; four chunks are in flight.  The
+// CTA's 128 threads split the staged tile and build the history window into
+// a double-buffered operand area, one thread issues the 12 MMAs of the chunk
+// and commits them to the buffer's mbarrier.  One CTA (128 threads, 137 KB of
+// shared memory, 128 tensor-memory columns) per SM and (source tile,
+// receiver split); every wait is bounded and a wait that gives up sets the
+// solve's error word (ADF_E_TIMEOUT), lets the copies and products in flight
+// land, frees the tensor memory and leaves the partials unwritten.
+#include "adf_internal.h"
+#include "ptx_util.h"
+
+namespace adf {
+
+constexpr int kTcM = 128;              // sources per CTA = tensor-memory lanes
+constexpr int kTcL = 16;               // lags per chunk (two MMA k-steps of 8)
+constexpr int kTcN = kGfBlock;         // steps of a block (MMA N)
+constexpr int kTcStages = 4;           // staged map tiles in flight
+constexpr int kTcTile = kTcL * kTcM;   // floats of one tensor's tile (8 KB)
+constexpr int kTcBTile = kTcN * kTcL;  // floats of one history window (2 KB)
+// shared memory, in floats: staged tiles [kTcStages][2 tensors][kTcTile],
+// A operands [2 buffers][t0 hi, t0 lo, t1 hi, t1 lo][kTcTile], B operands
+// [2 buffers][hi, lo][kTcBTile]
+constexpr int kTcAOff = kTcStages * 2 * kTcTile;
+constexpr int kTcBOff = kTcAOff + 2 * 4 * kTcTile;
+constexpr int kTcSmemFloats = kTcBOff + 2 * 2 * kTcBTile;
+constexpr size_t kTcDynSmem = sizeof(float) * kTcSmemFloats + 1024;  // + alignment to 1 KB
+constexpr uint32_t kTcCols = 128;  // tensor-memory columns: 2 sets x 2 tensors x 32 steps
+static_assert(kTcM == 128 && kTcN % 16 == 0 && kTcN <= 256, "MMA shape M=128, N=32");
+static_assert(kTcCols >= 4 * kTcN, "two accumulator sets of two tensors");
+// Instruction descriptor of kind::tf32: D Float32 (bit 4), A and B TF32
+// (bits 7-9, 10-12), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                              ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+// Operand layouts (K-major, no swizzle): core matrix (row group g, k-block
+// kb of 4 lags) at byte (kb * groups + g) * 128, its 8 rows 16 B apart.
+constexpr uint32_t kTcALbo = (kTcM / 8) * 128;  // next k-block of A
+constexpr uint32_t kTcBLbo = (kTcN / 8) * 128;  // next k-block of B
+constexpr uint32_t kTcSbo = 128;                // next row group
+constexpr uint32_t kTcWaitLimit = 1u << 22;     // polls of a bounded wait
+
+// Shared-memory matrix descriptor (tcgen05): start, leading and stride byte
+// offsets (>> 4), descriptor version 1 at bit 46, no swizzle, base offset 0.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   mbar)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 16 consecutive 32-bit columns of this warp's 32 tensor-memory lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Packs the two tensors of an input-history map (layout as in
+// adf_gf_far_kernel: PVFromPin element lag + ngf*(o + n1*r), PFromPin
+// lag + ngf*(r + n1*o)) into tiles (r, chunk c, source tile ot) of
+// [tensor][kb][g][row][4]: source ot*128 + 8g + row, lag 16c + 1 + 4kb + col,
+// zero beyond the map.  Set-up, once per map.
+__global__ void adf_gf_tc_pack_kernel(const float* t0, const float* t1, float* out, int kind,
+                                      int ngf, int n1, int nout, int nin, int nch, int notile) {
+  const long long per_tile = 2LL * kTcTile;
+  const long long total = (long long)nin * nch * notile * per_tile;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % per_tile);
+    long long tile = i / per_tile;
+    const int ot = (int)(tile % notile);
+    tile /= notile;
+    const int c = (int)(tile % nch);
+    const int r = (int)(tile / nch);
+    const int t = e / kTcTile, w = e - t * kTcTile;
+    const int kb = w / (kTcM * 4), rem = w - kb * (kTcM * 4);
+    const int g = rem >> 5, row = (rem >> 2) & 7, col = rem & 3;
+    const int o = ot * kTcM + g * 8 + row, lag = kTcL * c + 1 + 4 * kb + col;
+    float v = 0.f;
+    if (o < nout && lag < ngf) {
+      const long long idx = kind == ADF_GF_PV_FROM_PIN_ ? lag + (long long)ngf * (o + (long long)n1 * r)
+                                                        : lag + (long long)ngf * (r + (long long)n1 * o);
+      v = (t == 0 ? t0 : t1)[idx];
+    }
+    out[i] = v;
+  }
+}
+
+// Far-lag sums of the block of kGfBlock steps that starts at this launch-step
+// (the same partials as adf_gf_far_kernel: gf_far[o][receiver split][step of
+// the block][2], added over the splits by adf_gf_far_combine_kernel).
+// blockIdx.x = source tile * gf_rs + receiver split, blockIdx.y = solve.
+__global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p) {
+  const SolveDev& S = p.solves[blockIdx.y];
+  const int it0 = S.it_base + p.step;
+  if (!(S.flags & SF_GF) || !(S.flags & SF_GF_TC) || S.gf_rs <= 0 || it0 > S.it_stop ||
+      it0 >= S.nt)
+    return;
+  const int rsn = S.gf_rs, nout = S.gf_nout;
+  const int ot = blockIdx.x / rsn, rsi = blockIdx.x - ot * rsn;
+  if (ot * kTcM >= nout) return;
+  const int nt = S.nt, ngf = S.gf_nt, nin = S.gf_nin, notile = (nout + kTcM - 1) / kTcM;
+  const int r0 = (int)((long long)nin * rsi / rsn), r1 = (int)((long long)nin * (rsi + 1) / rsn);
+  const int lag_hi = min(it0 + kGfBlock - 1, ngf) - 1;  // largest lag any step of the block uses
+  const int nch = lag_hi >= 1 ? (lag_hi + kTcL - 1) / kTcL : 0;  // chunks this block needs
+  const int Q = (r1 - r0) * nch;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int o = ot * kTcM + tid;  // this thread's source = its tensor-memory lane
+  double acc[2][kTcN];
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+#pragma unroll
+    for (int b = 0; b < kTcN; ++b) acc[t][b] = 0.0;
+  auto write_out = [&]() {
+    if (o >= nout) return;
+    double* pp = S.gf_far + ((long long)o * rsn + rsi) * kGfBlock * 2;
+#pragma unroll
+    for (int b = 0; b < kTcN; ++b) {
+      pp[2 * b] = acc[0][b];
+      pp[2 * b + 1] = acc[1][b];
+    }
+  };
+  if (Q == 0) {  // no far lag in this block (uniform across the CTA)
+    write_out();
+    return;
+  }
+
+  extern __shared__ unsigned char tc_smem_raw[];
+  float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) &
+                                       ~static_cast<uintptr_t>(1023));
+  __shared__ __align__(8) uint64_t full[kTcStages];  // staged tile landed
+  __shared__ __align__(8) uint64_t mmad[2];          // products of an operand buffer done
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&full[s]), 1);
+    for (int s = 0; s < 2; ++s) mbar_init(smem_u32(&mmad[s]), 1);
+    fence_mbar_init();
+    s_abort = 0;
+  }
+  if (warp == 0) {  // one warp allocates (and later frees) the accumulators
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = s_tmem;
+
+  const float* tiles = S.gf_tc;
+  auto tile_src = [&](int q) {
+    const int rr = q / nch, c = q - rr * nch;
+    return tiles + (((long long)(r0 + rr) * S.gf_tc_nch + c) * notile + ot) * (2LL * kTcTile);
+  };
+  int staged = 0;  // chunks whose bulk copy was issued (thread 0)
+  auto stage = [&](int q) {
+    const int s = q % kTcStages;
+    fence_proxy_async_smem();  // the slot was last read through the generic proxy
+    mbar_expect_tx(smem_u32(&full[s]), (uint32_t)(2 * kTcTile * sizeof(float)));
+    bulk_load(smem_u32(sm + s * 2 * kTcTile), tile_src(q), (uint32_t)(2 * kTcTile * sizeof(float)),
+              smem_u32(&full[s]));
+    staged = q + 1;
+  };
+  if (tid == 0)
+    for (int q = 0; q < min(Q, kTcStages); ++q) stage(q);
+  auto bounded = [&](uint64_t* bar, int phase) {
+    if (!mbar_wait(smem_u32(bar), (uint32_t)phase & 1u, kTcWaitLimit)) {
+      atomicOr(S.err, 4);  // reported as ADF_E_TIMEOUT
+      s_abort = 1;         // read by every thread after the next barrier
+    }
+  };
+  // adds accumulator set `set` (lanes of this warp) into the Float64 sums
+  auto drain = [&](int set) {
+    const uint32_t ta = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(set * 2 * kTcN);
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+      for (int h = 0; h < kTcN / 16; ++h) {
+        uint32_t v[16];
+        tmem_ld16(ta + t * kTcN + h * 16, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          acc[t][h * 16 + j] = __dadd_rn(acc[t][h * 16 + j], (double)__uint_as_float(v[j]));
+      }
+  };
+
+  int q = 0;
+  bool aborted = false;
+  for (; q < Q; ++q) {
+    const int s = q % kTcStages, buf = q & 1;
+    const int rr = q / nch, c = q - rr * nch, r = r0 + rr;
+    if (c == 0 && q > 0) {  // the previous receiver's products (last chunk q-1) into Float64
+      bounded(&mmad[(q - 1) & 1], (q - 1) >> 1);
+      tc_fence_after();
+      drain((rr - 1) & 1);
+    }
+    if (q >= 2) bounded(&mmad[buf], (q - 2) >> 1);  // operand buffer read by chunk q-2
+    bounded(&full[s], q / kTcStages);
+    // the staged tile -> TF32 high parts and remainders
+    {
+      const float* stg = sm + s * 2 * kTcTile;
+      float* A = sm + kTcAOff + buf * 4 * kTcTile;
+#pragma unroll 2
+      for (int i = tid; i < 2 * kTcTile / 4; i += kTcM) {
+        const float4 x = *reinterpret_cast<const float4*>(stg + 4 * i);
+        const int t = (4 * i) / kTcTile, e = 4 * i - t * kTcTile;
+        float4 hi, lo;
+        hi.x = tf32_rna(x.x);
+        hi.y = tf32_rna(x.y);
+        hi.z = tf32_rna(x.z);
+        hi.w = tf32_rna(x.w);
+        lo.x = __fsub_rn(x.x, hi.x);
+        lo.y = __fsub_rn(x.y, hi.y);
+        lo.z = __fsub_rn(x.z, hi.z);
+        lo.w = __fsub_rn(x.w, hi.w);
+        *reinterpret_cast<float4*>(A + (2 * t) * kTcTile + e) = hi;
+        *reinterpret_cast<float4*>(A + (2 * t + 1) * kTcTile + e) = lo;
+      }
+    }
+    // the block's far-lag window of receiver r's input history: thread ->
+    // step b = tid/4, lags 4(tid%4) .. +3 of the chunk (one core-matrix row)
+    {
+      const int b = tid >> 2, kb = tid & 3;
+      const double* hist = S.gf_pin + (long long)r * nt;
+      const int lim = min(it0 + b, ngf);
+      float hv[4], lv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int lag = kTcL * c + 1 + 4 * kb + j;
+        const double h = (lag > b && lag < lim) ? hist[it0 - 1 + b - lag] : 0.0;
+        hv[j] = tf32_rna((float)h);
+        lv[j] = (float)(h - (double)hv[j]);
+      }
+      float* B = sm + kTcBOff + buf * 2 * kTcBTile;
+      const int off = (kb * (kTcN / 8) + (b >> 3)) * 32 + (b & 7) * 4;
+      *reinterpret_cast<float4*>(B + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+      *reinterpret_cast<float4*>(B + kTcBTile + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+    }
+    fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
+    tc_fence_before();
+    __syncthreads();
+    if (s_abort) {
+      aborted = true;
+      break;
+    }
+    if (tid == 0) {
+      tc_fence_after();
+      if (q + kTcStages < Q) stage(q + kTcStages);  // slot s was consumed by the split
+      const uint32_t set = (uint32_t)((rr & 1) * 2 * kTcN);
+      const uint32_t a0 = smem_u32(sm + kTcAOff + buf * 4 * kTcTile);
+      const uint32_t b0 = smem_u32(sm + kTcBOff + buf * 2 * kTcBTile);
+#pragma unroll
+      for (int ks = 0; ks < kTcL / 8; ++ks) {
+        const uint64_t bh = umma_desc(b0 + ks * 2 * kTcBLbo, kTcBLbo, kTcSbo);
+        const uint64_t bl = umma_desc(b0 + kTcBTile * 4 + ks * 2 * kTcBLbo, kTcBLbo, kTcSbo);
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const uint32_t d = tbase + set + (uint32_t)(t * kTcN);
+          const uint64_t ah = umma_desc(a0 + (2 * t) * kTcTile * 4 + ks * 2 * kTcALbo, kTcALbo, kTcSbo);
+          const uint64_t al =
+              umma_desc(a0 + (2 * t + 1) * kTcTile * 4 + ks * 2 * kTcALbo, kTcALbo, kTcSbo);
+          tc_mma_tf32(d, ah, bh, (c > 0 || ks > 0) ? 1u : 0u);  // a receiver's first product overwrites
+          tc_mma_tf32(d, ah, bl, 1u);
+          tc_mma_tf32(d, al, bh, 1u);
+        }
+      }
+      tc_commit(smem_u32(&mmad[buf]));
+    }
+  }
+  if (!aborted) {  // the last receiver's products
+    bounded(&mmad[(Q - 1) & 1], (Q - 1) >> 1);
+    tc_fence_after();
+    drain(((Q - 1) / nch) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (aborted || s_abort) {
+    // let the copies and products in flight land before the CTA exits
+    // (bounded again); no partial is written, the host reports the error
+    if (tid == 0) {
+      for (int k = q; k < staged; ++k)
+        mbar_wait(smem_u32(&full[k % kTcStages]), (uint32_t)(k / kTcStages) & 1u, kTcWaitLimit);
+      if (q > 0) mbar_wait(smem_u32(&mmad[(q - 1) & 1]), (uint32_t)((q - 1) >> 1) & 1u, kTcWaitLimit);
+    }
+  } else {
+    write_out();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcCols)
+                 : "memory");
+  }
+}
+
+int64_t gf_tc_chunks(int64_t nt_gf) { return nt_gf > 1 ? (nt_gf - 1 + kTcL - 1) / kTcL : 1; }
+size_t gf_tc_packed_floats(int64_t nt_gf, int64_t n_src, int64_t n_rec) {
+  return (size_t)n_rec * gf_tc_chunks(nt_gf) * ((n_src + kTcM - 1) / kTcM) * 2 * kTcTile;
+}
+int gf_tc_sources_per_tile() { return kTcM; }
+
+cudaError_t launch_gf_tc_pack(const SolveDev& d, float* out, cudaStream_t s) {
+  const int notile = (d.gf_nout + kTcM - 1) / kTcM;
+  adf_gf_tc_pack_kernel<<<8 * 148, 256, 0, s>>>(d.gf_t[0], d.gf_t[1], out, d.gf_kind, d.gf_nt,
+                                                d.gf_n1, d.gf_nout, d.gf_nin, d.gf_tc_nch, notile);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gf_far_tc(const EpiParams& p, int max_blocks, cudaStream_t s) {
+  static bool attr = false;  // the first launch of the process raises the shared-memory limit
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute((const void*)adf_gf_far_tc_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcDynSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  adf_gf_far_tc_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), kTcM, kTcDynSmem, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace adf

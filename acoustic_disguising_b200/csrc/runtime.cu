@@ -423,6 +423,7 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
   max_gf_nsrc = 0;
   max_gf_blocks = 0;
   max_gf_far_blocks = 0;
+  max_gf_tc_blocks = 0;
   gf_reduce = false;
   for (int i = 0; i < ns; ++i) {
     sd[i] = list[i]->dev;
@@ -430,7 +431,11 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
       max_gf_nsrc = std::max(max_gf_nsrc, sd[i].gf_nout);
       max_gf_blocks = std::max(max_gf_blocks, sd[i].gf_nout * sd[i].gf_ks);
       gf_reduce = gf_reduce || sd[i].gf_ks > 1;
-      if (sd[i].gf_rs > 0)
+      if (sd[i].gf_rs > 0 && (sd[i].flags & SF_GF_TC))
+        max_gf_tc_blocks = std::max(max_gf_tc_blocks,
+                                    (sd[i].gf_nout + gf_tc_sources_per_tile() - 1) /
+                                        gf_tc_sources_per_tile() * sd[i].gf_rs);
+      else if (sd[i].gf_rs > 0)
         max_gf_far_blocks = std::max(max_gf_far_blocks, (sd[i].gf_nout + 63) / 64 * sd[i].gf_rs);
     }
     const SolveDev& d = list[i]->dev;
@@ -513,7 +518,10 @@ int Batch::launch_step(adf_ctx* ctx, int step) {
     return fail(ADF_E_DEVICE, std::string("epilogue launch failed: ") + cudaGetErrorString(e2));
   if (max_gf_nsrc > 0) {  // in-loop GF extrapolation, then vn2v! of those solves
     // the far lags of a block of steps, at the block's first launch-step
-    if (max_gf_far_blocks > 0 && step % kGfBlock == 0 &&
+    if (max_gf_tc_blocks > 0 && step % kGfBlock == 0 &&
+        (e2 = launch_gf_far_tc(ep, max_gf_tc_blocks, ctx->stream)) != cudaSuccess)
+      return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
+    if ((max_gf_far_blocks > 0 || max_gf_tc_blocks > 0) && step % kGfBlock == 0 &&
         (e2 = launch_gf_far(ep, max_gf_far_blocks, max_gf_nsrc, ctx->stream)) != cudaSuccess)
       return fail(ADF_E_DEVICE, std::string("GF launch failed: ") + cudaGetErrorString(e2));
     if ((e2 = launch_gf_extrapolate(ep, max_gf_blocks, max_gf_nsrc, gf_reduce, ctx->stream)) !=
@@ -556,7 +564,7 @@ int Batch::run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk) {
   while (nsteps - done >= chunk) {
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += per_step * chunk + 1 + (max_gf_far_blocks > 0 ? 2 * chunk / kGfBlock : 0);
+    ctx->launches += per_step * chunk + 1 + far_launches() * chunk / kGfBlock;
     done += chunk;
     if (ctx->kernel_timing) {  // measurement mode: the replay's per-launch events, before reuse
       cudaStreamSynchronize(ctx->stream);
@@ -595,7 +603,7 @@ int Batch::run_chunk(adf_ctx* ctx, int n, int chunk) {
     }
     if (cudaGraphLaunch(graph_exec, ctx->stream) != cudaSuccess)
       return fail(ADF_E_DEVICE, "graph launch failed");
-    ctx->launches += per_step * chunk + 1 + (max_gf_far_blocks > 0 ? 2 * chunk / kGfBlock : 0);
+    ctx->launches += per_step * chunk + 1 + far_launches() * chunk / kGfBlock;
     return ADF_OK;
   }
   for (int s = 0; s < n; ++s) {
@@ -1025,6 +1033,12 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
       if (gf->i_rec[k] < 1 || gf->i_rec[k] > txs->ntx)
         return fail(ADF_E_ARG, "gf map iRec outside 1..ntx");
   }
+  if (use_gf && gf->contraction != ADF_GF_CONTRACT_FP64 &&
+      gf->contraction != ADF_GF_CONTRACT_TF32X3)
+    return fail(ADF_E_ARG, "gf map contraction must be ADF_GF_CONTRACT_FP64 or _TF32X3");
+  if (use_gf && gf->contraction == ADF_GF_CONTRACT_TF32X3 && gf->kind == ADF_GF_PV_FROM_PV)
+    return fail(ADF_E_ARG, "the tensor-core contraction applies to PVFromPin and PFromPin maps");
+  const bool use_tc = use_gf && gf->contraction == ADF_GF_CONTRACT_TF32X3;
   if (txs->nt != d->nt) return fail(ADF_E_ARG, "txs.nt must equal dom.nt");
   if (start_step < 1 || stop_step > d->nt) return fail(ADF_E_ARG, "step range outside 1..nt");
   if (d->nx < 4 || d->ny < 4 || d->nz < 4) return fail(ADF_E_ARG, "grid must be at least 4^3");
@@ -1043,6 +1057,7 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     if (gf->kind != ADF_GF_PV_FROM_PV)  // near-lag copy and history ring of the blocked kinds
       need += (size_t)4 * 2 * std::min<int64_t>(kGfBlock, gf->nt_gf) * gf->n1 * gf->n2 +
               (size_t)8 * kGfRing * gf->n_rec;
+    if (use_tc) need += sizeof(float) * gf_tc_packed_floats(gf->nt_gf, gf->n_src, gf->n_rec);
   }
   if (need > ctx->budget) return fail(ADF_E_BUDGET, "solve exceeds the context's HBM budget");
   auto s = std::make_unique<Solve>();
@@ -1109,10 +1124,17 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
     int rs = 0;
     double* far = nullptr;
     if (gf->kind != ADF_GF_PV_FROM_PV && !rc) {
-      const int64_t otiles = (gf->n_src + 63) / 64;
-      rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (2 * ctx->nsm + otiles - 1) / otiles));
+      if (use_tc) {  // one 128-source CTA per SM over the source tiles
+        const int64_t otiles = (gf->n_src + gf_tc_sources_per_tile() - 1) / gf_tc_sources_per_tile();
+        rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (ctx->nsm + otiles - 1) / otiles));
+      } else {
+        const int64_t otiles = (gf->n_src + 63) / 64;
+        rs = (int)std::max<int64_t>(1, std::min<int64_t>(gf->n_rec, (2 * ctx->nsm + otiles - 1) / otiles));
+      }
       far = solve_dalloc<double>(*s, (size_t)gf->n_src * rs * kGfBlock * 2, rc);
     }
+    float* tc = nullptr;
+    if (use_tc && !rc) tc = solve_dalloc<float>(*s, gf_tc_packed_floats(gf->nt_gf, gf->n_src, gf->n_rec), rc);
     // the blocked kinds' per-step sum reads lags 0..kGfBlock-1 from a
     // receiver-major copy and the recent history from a receiver-major ring
     float* near = nullptr;
@@ -1157,6 +1179,14 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
       if (e != cudaSuccess)
         return fail(ADF_E_DEVICE, std::string("GF pack launch failed: ") + cudaGetErrorString(e));
       sd.gf_near = near;
+    }
+    if (tc) {  // the far lags' operand tiles for the tensor cores
+      sd.gf_tc_nch = (int)gf_tc_chunks(gf->nt_gf);
+      cudaError_t e = launch_gf_tc_pack(sd, tc, ctx->stream);
+      if (e != cudaSuccess)
+        return fail(ADF_E_DEVICE, std::string("GF pack launch failed: ") + cudaGetErrorString(e));
+      sd.gf_tc = tc;
+      sd.flags |= SF_GF_TC;
     }
     // pin rows recorded before start_step (a resumed run) from the host traces
     if (start_step > 1 && gf->kind != ADF_GF_PV_FROM_PV) {

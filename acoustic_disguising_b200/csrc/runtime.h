@@ -98,6 +98,12 @@ struct Batch {
   int max_gf_nsrc = 0;       // > 0: some solve runs the in-loop GF extrapolation
   int max_gf_blocks = 0;     // (source, receiver split) blocks of the GF kernel
   int max_gf_far_blocks = 0; // (source tile, receiver split) blocks of the far-lag kernel
+  int max_gf_tc_blocks = 0;  // the same for the tensor-core far-lag kernel
+  // far-lag kernels launched per block of kGfBlock steps (FP64, tensor-core, combine)
+  int far_launches() const {
+    const int k = (max_gf_far_blocks > 0) + (max_gf_tc_blocks > 0);
+    return k > 0 ? k + 1 : 0;
+  }
   bool gf_reduce = false;    // some GF solve splits a source's receivers over blocks
   int per_step = 2;          // kernel launches per launch-step
   cudaGraphExec_t graph_exec = nullptr;

@@ -187,7 +187,16 @@ typedef struct {
                    copies, extrapolation.jl:215-216, 228-229, 246-247, so the
                    sources never change); 0: the documented intent, the
                    extrapolated samples are written into txs's sources     */
+  int contraction; /* ADF_GF_CONTRACT_FP64 (0): every lag summed with Float64
+                      FMAs, as the reference accumulates; ADF_GF_CONTRACT_TF32X3
+                      (1): the *FromPin kinds sum the lags older than the
+                      current 32-step block on the tensor cores (TF32 split
+                      into three products, FP32 per receiver, Float64 over
+                      receivers), within about 1e-6 of the Float64 sums; the
+                      map is kept a second time, packed as operand tiles  */
 } adf_gfmap;
+#define ADF_GF_CONTRACT_FP64 0
+#define ADF_GF_CONTRACT_TF32X3 1
 
 /* run_fdtd! with a gf_map (src/simulation.jl:542-557, forward.jl:123-128):
  * adf_run_fdtd plus, after v2vn! of each step it < nt, extrapolate!

@@ -106,6 +106,71 @@ def test_gf_map_matches_oracle(adf, oracle, ctx, kind, discard, tol, steps, nt_g
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["PVFromPin", "PFromPin"])
+def test_gf_map_tensor_core_contraction(adf, oracle, ctx, kind):
+    """contraction="tf32x3": the lags older than each 32-step block summed on
+    the tensor cores (TF32 split into three products).  160 sources (two
+    128-source tiles, the second mostly padding), 160 receivers, 100 lags
+    over 140 steps (five blocks, the later ones with far lags in every
+    16-lag chunk).  The driven sources, traces and fields stay within 1e-5
+    of the oracle's Float64 sums (the Float32-level bar the reference's own
+    PVFromPV accumulation sets), and so does the Float64 GPU path."""
+    case = make_case(adf, oracle, 40, 36, 32, steps=140, npml=5, shape="sphere", seed=9,
+                     n_rec=320)
+    d, o, g, cp, mask, field = case
+    ntx = g.dir.shape[1]
+    i_rec = np.arange(3, 163, dtype=np.int64)
+    i_src = np.arange(163, 323, dtype=np.int64)
+    assert i_src.max() <= ntx
+    nt_gf = 100
+    shape = (nt_gf, i_src.size, i_rec.size) if kind == "PVFromPin" else (nt_gf, i_rec.size,
+                                                                          i_src.size)
+    rng = np.random.default_rng(11)
+    ts = [(rng.standard_normal(shape) * 2.5e-4).astype(np.float32, order="F") for _ in range(2)]
+    runs = {}
+    for contraction in ("tf32x3", "fp64"):
+        gg = to_adf_grid(adf, g)
+        pc = _Cp(adf, cp)
+        f_gpu = field.copy(order="F")
+        adf.run_fdtd(d, f_gpu, gg, pc, mask,
+                     gf_map=adf.GfMap(kind, tuple(ts), i_src, i_rec, False, contraction))
+        runs[contraction] = (f_gpu, gg, pc)
+    f_cpu = field.copy(order="F")
+    go, co = g.copy(), cp.copy()
+    oracle.run_fdtd_gf(o, f_cpu, go, co, mask, kind, ts, i_src, i_rec, o.z0, discard=False)
+    tol = 1e-5
+    errs = assert_parity(runs["tf32x3"], (f_cpu, go, co), tol)
+    assert errs["rec0"] <= tol
+    tc, fp = runs["tf32x3"][1], runs["fp64"][1]
+    for k in i_src - 1:
+        b = go.src[0][:, k].astype(np.float64)
+        assert np.abs(b[40:]).max() > 0  # far lags drive the later blocks
+        for src in (tc.src[0][:, k], fp.src[0][:, k]):
+            a = src.astype(np.float64)
+            assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b)
+        a = tc.vn_src[:, k].astype(np.float64)
+        b = go.vn_src[:, k].astype(np.float64)
+        assert np.linalg.norm(a - b) <= tol * max(np.linalg.norm(b), 1e-30)
+
+
+def test_gf_map_unknown_contraction(adf):
+    ts, isr, irc = gf_inputs(40, "PVFromPin")
+    with pytest.raises(KeyError):
+        adf.GfMap("PVFromPin", tuple(ts), isr, irc, False, "bf16")._c(1.0)
+
+
+@pytest.mark.gpu
+def test_gf_map_tensor_core_contraction_rejects_pvfrompv(adf, oracle, ctx):
+    """The tensor-core contraction covers the input-history kinds only."""
+    case = make_case(adf, oracle, 24, 22, 20, steps=10, npml=4, shape="none", seed=1)
+    d, o, g, cp, mask, field = case
+    ts, isr, irc = gf_inputs(g.dir.shape[1], "PVFromPV", nt_gf=4)
+    with pytest.raises(adf.AdfError, match="tensor-core"):
+        adf.run_fdtd(d, field.copy(order="F"), to_adf_grid(adf, g), _Cp(adf, cp), mask,
+                     gf_map=adf.GfMap("PVFromPV", tuple(ts), isr, irc, False, "tf32x3"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["PVFromPin", "PFromPin"])
 def test_gf_map_resumed_run(adf, oracle, ctx, kind):
     """A run stopped after step 45 and resumed at step 46 matches one
     uninterrupted oracle run: the resumed call starts its 32-step blocks at
