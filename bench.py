@@ -25,6 +25,10 @@ time step over all of their tiles, graph-captured), and the p / v_n traces copie
           map of 256 lags x 256 sources x 256 receivers): device time per
           step of the map's work (the run minus the same run with the map
           discarded)
+  gf_map_tensor_core : the same with a 512-lag x 1024 x 1024 map on 96^3:
+          the Float64 far-lag kernel against the tensor-core contraction
+          (tcgen05 TF32 split), their per-step cost, speedup and agreement,
+          and the map bytes per second against the HBM peak
   step512 : one 512^3 solve (12-cell CPML, rigid ellipsoid): the step
           kernel's roofline on the largest single-solve grid
   serving : 100 GF solves of mixed grid sizes (96..256^3), step counts
@@ -585,12 +589,7 @@ def step512_section(A, ctx, nt=48, tune=True):
     ctx.set_kernel_timing(False)
     per = k_ms / max(k_n, 1)
     byt = algorithmic_bytes_per_solve_step(n, npml)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs") or 6650.0
+    peak = hbm_peak()[0]
     gbs = byt / (per / 1e3) / 1e9
     return {"workload": "one 512^3 solve (dx=5 mm air), 12-cell CPML, rigid ellipsoid 80/60/40 "
                         f"cells, point source, 256-point shell, {nt} steps",
@@ -651,12 +650,7 @@ def hologram_section(A, ctx, nt=H_NT):
     kh_ms = ctx.last_kh_ms()
     per = k_ms / max(k_n, 1)
     byt = algorithmic_bytes_per_solve_step(H_N, H_NPML)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs") or 6650.0
+    peak = hbm_peak()[0]
     taps = math.ceil(12 * sigma / d.dt)
     flop = 4.0 * taps * H_NOUT * H_NR * nt  # 2 channels x taps x 2 FLOP per pair-sample
     gbs = byt / (per / 1e3) / 1e9
@@ -700,7 +694,7 @@ def fp32_section(A, ctx, batch, nt=96):
 # ---------------------------------------------------------------------------
 # In-loop GF extrapolation (run_fdtd! gf_map = PVFromPin) on a 128^3 run
 # ---------------------------------------------------------------------------
-def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
+def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256, contraction="fp64"):
     d = A.Domain(tmax=tmax_of(nt), xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
     tf = A.ricker_wavelet(d, 2000.0, injection=False)
     rp, rn = A.fibonacci_sphere(n_io, 40 * DX)   # recording shell (iRec)
@@ -719,7 +713,8 @@ def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
         g = A.transceivers_to_grid(d, txs)
         cp = A.Cpml(d, NPML, 1e-4, PML_FC)
         f = np.zeros((n, n, n, 4), np.float32, order="F")
-        A.run_fdtd(d, f, g, cp, ctx=ctx, gf_map=A.PVFromPin(pp, vp, i_src, i_rec, discard))
+        A.run_fdtd(d, f, g, cp, ctx=ctx,
+                   gf_map=A.PVFromPin(pp, vp, i_src, i_rec, discard, contraction))
         times[discard] = ctx.last_timing()[0]
     gf_ms = times[False] - times[True]
     lags = sum(min(it, nt_gf) for it in range(1, nt))
@@ -739,6 +734,71 @@ def gf_section(A, ctx, n=128, nt=300, nt_gf=256, n_io=256):
                          "flop": flop, "time": "run with the map minus the run with it "
                                                "discarded (every GF kernel, per step and "
                                                "per block)"}}
+
+
+def hbm_peak():
+    """The HBM roofline denominator: MEASURED_PEAKS.json's measured copy
+    bandwidth when the file is present, else the pool's earlier measurement."""
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        peak = None
+    if peak:
+        return float(peak), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6650"
+
+
+def gf_tc_section(A, ctx, n=96, nt=700, nt_gf=512, n_io=1024):
+    """In-loop GF extrapolation with a map whose older lags dominate (512 lags
+    x 1024 sources x 1024 receivers, 4.3 GB): the Float64 far-lag kernel
+    against the tensor-core contraction (TF32 split into three products).
+    GF cost = run with the map minus the run with it discarded; the map bytes
+    are the algorithmic reads of both tensors (the far lags once per 32-step
+    block, the near lags every step)."""
+    d = A.Domain(tmax=tmax_of(nt), xmax=(n - 1) * DX / 2, nx=n, c0=C0, r0=RHO, cf=0.5)
+    tf = A.ricker_wavelet(d, 2000.0, injection=False)
+    rp, rn = A.fibonacci_sphere(n_io, 30 * DX)
+    ip, inn = A.fibonacci_sphere(n_io, 22 * DX)
+    txs = [A.Transceiver(np.zeros(3), np.array([1.0, 0, 0, 0]), tf * 1e3)]
+    txs += [A.Transceiver(rp[k], np.r_[0.0, rn[k]], np.zeros(d.nt)) for k in range(n_io)]
+    txs += [A.Transceiver(ip[k], np.r_[0.0, inn[k]], np.zeros(d.nt)) for k in range(n_io)]
+    i_rec = np.arange(2, 2 + n_io, dtype=np.int64)
+    i_src = np.arange(2 + n_io, 2 + 2 * n_io, dtype=np.int64)
+    rng = np.random.default_rng(12)
+    shape = (nt_gf, n_io, n_io)
+    pp = np.asfortranarray(rng.standard_normal(shape, dtype=np.float32) * np.float32(1e-6))
+    vp = np.asfortranarray(rng.standard_normal(shape, dtype=np.float32) * np.float32(1e-6))
+    times, srcs = {}, {}
+    for mode in ("discard", "fp64", "tf32x3"):
+        g = A.transceivers_to_grid(d, txs)
+        cp = A.Cpml(d, NPML, 1e-4, PML_FC)
+        f = np.zeros((n, n, n, 4), np.float32, order="F")
+        gm = A.PVFromPin(pp, vp, i_src, i_rec, mode == "discard",
+                         "fp64" if mode == "discard" else mode)
+        A.run_fdtd(d, f, g, cp, ctx=ctx, gf_map=gm)
+        times[mode] = ctx.last_timing()[0]
+        srcs[mode] = np.array(g.src[0][:, i_src - 1], np.float64)
+    del pp, vp
+    gf = {m: times[m] - times["discard"] for m in ("fp64", "tf32x3")}
+    B = 32
+    far = sum(min(it0 + B - 1, nt_gf) - 1 for it0 in range(1, nt, B))  # lags per block
+    near = sum(min(min(it, nt_gf), (it - 1) % B + 1) for it in range(1, nt))
+    byts = 2.0 * 4 * n_io * n_io * (far + near)
+    err = float(np.linalg.norm(srcs["tf32x3"] - srcs["fp64"]) / np.linalg.norm(srcs["fp64"]))
+    peak = hbm_peak()
+    gbs = byts / (gf["tf32x3"] / 1e3) / 1e9 if gf["tf32x3"] > 0 else None
+    return {"workload": f"{n}^3 run_fdtd!, {nt} steps, PVFromPin map {nt_gf} lags x {n_io} "
+                        f"sources x {n_io} receivers (seeded)",
+            "run_ms": times, "gf_ms_per_step": {m: gf[m] / (nt - 1) for m in gf},
+            "speedup_tensor_core": gf["fp64"] / gf["tf32x3"] if gf["tf32x3"] > 0 else None,
+            "rel_l2_driven_sources_tf32x3_vs_fp64": err,
+            "roofline_tf32x3": {"bound": "hbm (map tensors)", "achieved": gbs,
+                                "peak": peak[0], "unit": "GB/s",
+                                "frac": gbs / peak[0] if gbs else None,
+                                "peak_source": peak[1], "map_bytes": byts,
+                                "time": "run with the map minus the run with it discarded "
+                                        "(every GF kernel: near lags per step, far lags per "
+                                        "block on the tensor cores)"}}
 
 
 # ---------------------------------------------------------------------------
@@ -841,6 +901,8 @@ def b200_arm(args):
     if world == 1 and not args.no_gf:
         gf_section(A, ctx, nt=40)  # warm-up: graphs, pool blocks
         extra["gf_map"] = gf_section(A, ctx)
+        gf_tc_section(A, ctx, nt=80, nt_gf=64, n_io=256)  # warm-up of both contractions
+        extra["gf_map_tensor_core"] = gf_tc_section(A, ctx)
     if world == 1 and not args.no_step512:
         extra["step512"] = step512_section(A, ctx)
     if world == 1 and args.arith == "promote":
@@ -866,14 +928,7 @@ def b200_arm(args):
     e2e = solves / wall_total
     bytes_launch = B * algorithmic_bytes_per_solve_step()
     achieved = bytes_launch / (k_avg_ms / 1e3) / 1e9
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak = peaks.get("hbm_gbs")
-    peak_note = "measured (MEASURED_PEAKS.json hbm_gbs)" if peak else "fallback 6650"
-    peak = peak or 6650.0
+    peak, peak_note = hbm_peak()
     tpc = read_traffic()
     cells = N ** 3
     line = {
@@ -959,7 +1014,10 @@ def gf_only(args):
         A.build()
     ctx = A.Context(0)
     gf_section(A, ctx, nt=40)
-    print(json.dumps({"gf_map": gf_section(A, ctx)}), flush=True)
+    out = {"gf_map": gf_section(A, ctx)}
+    gf_tc_section(A, ctx, nt=80, nt_gf=64, n_io=256)
+    out["gf_map_tensor_core"] = gf_tc_section(A, ctx)
+    print(json.dumps(out), flush=True)
     ctx.close()
     return 0
 
