@@ -12,27 +12,31 @@
 // pin[it0-1+b-lag, r] on the far lags of step b, zero elsewhere).  Here that
 // product runs on tcgen05.mma with FP32 accumulation in tensor memory.  Every
 // Float32 map entry and Float64 history sample is split into a TF32 part
-// (rounded to nearest) and the remainder, and hi*hi + hi*lo + lo*hi is
-// accumulated (the dropped lo*lo term is below 2^-22 of the product).  After
-// the last chunk of a receiver its accumulator is added into per-thread
-// Float64 sums (two accumulator sets in tensor memory alternate, so one is
-// drained while the next receiver's products run), so the sum over receivers
-// stays in Float64.  The result agrees with the Float64 sum to about 1e-6
-// relative, Float32 level: an opt-in contraction (ADF_GF_CONTRACT_TF32X3);
-// the default path keeps the Float64 FMAs of the reference's accumulation.
+// (rounded to nearest, ties away) and the remainder, and hi*hi + hi*lo +
+// lo*hi is accumulated (the dropped lo*lo term is below 2^-22 of the
+// product).  After the last chunk of a receiver its accumulator is added
+// into Float64 sums in shared memory (two accumulator sets in tensor memory
+// alternate, so one is drained while the next receiver's products run), so
+// the sum over receivers stays in Float64.  The result agrees with the
+// Float64 sum to about 1e-6 relative, Float32 level: an opt-in contraction
+// (ADF_GF_CONTRACT_TF32X3); the default path keeps the Float64 FMAs of the
+// reference's accumulation.
 //
 // Data path: the two tensors of the map are packed once per map
 // (adf_gf_tc_pack_kernel) into 16 KB tiles (receiver, 16-lag chunk,
 // 128-source tile) laid out as the MMA's K-major, no-swizzle operand (8-row x
 // 16-byte core matrices), so one bulk copy (cp.async.bulk, completing on an
-// mbarrier, no multicast) stages a chunk; four chunks are in flight.  The
-// CTA's 128 threads split the staged tile and build the history window into
-// a double-buffered operand area, one thread issues the 12 MMAs of the chunk
-// and commits them to the buffer's mbarrier.  One CTA (128 threads, 137 KB of
-// shared memory, 128 tensor-memory columns) per SM and (source tile,
-// receiver split); every wait is bounded and a wait that gives up sets the
-// solve's error word (ADF_E_TIMEOUT), lets the copies and products in flight
-// land, frees the tensor memory and leaves the partials unwritten.
+// mbarrier, no multicast) stages a chunk, and a second one on the same
+// mbarrier brings the chunk's rows of the input history; four chunks are in
+// flight.  The CTA's 256 threads split the staged tile and build the history
+// window into a double-buffered operand area, one thread issues the 12 MMAs
+// of the chunk and commits them to the buffer's mbarrier, warps 0-3 (the
+// owners of the 128 tensor-memory lanes) drain the accumulators.  One CTA
+// (256 threads, 204 KB of shared memory, 128 tensor-memory columns) per SM
+// and (source tile, receiver split); every wait is bounded and a wait that
+// gives up sets the solve's error word (ADF_E_TIMEOUT), lets the copies and
+// products in flight land, frees the tensor memory and leaves the partials
+// unwritten.
 #include "adf_internal.h"
 #include "ptx_util.h"
 
@@ -43,14 +47,20 @@ constexpr int kTcL = 16;               // lags per chunk (two MMA k-steps of 8)
 constexpr int kTcN = kGfBlock;         // steps of a block (MMA N)
 constexpr int kTcStages = 4;           // staged map tiles in flight
 constexpr int kTcTile = kTcL * kTcM;   // floats of one tensor's tile (8 KB)
-constexpr int kTcBTile = kTcN * kTcL;  // floats of one history window (2 KB)
-// shared memory, in floats: staged tiles [kTcStages][2 tensors][kTcTile],
-// A operands [2 buffers][t0 hi, t0 lo, t1 hi, t1 lo][kTcTile], B operands
-// [2 buffers][hi, lo][kTcBTile]
-constexpr int kTcAOff = kTcStages * 2 * kTcTile;
-constexpr int kTcBOff = kTcAOff + 2 * 4 * kTcTile;
-constexpr int kTcSmemFloats = kTcBOff + 2 * 2 * kTcBTile;
-constexpr size_t kTcDynSmem = sizeof(float) * kTcSmemFloats + 1024;  // + alignment to 1 KB
+constexpr int kTcBTile = kTcN * kTcL;  // floats of one history window operand (2 KB)
+constexpr int kTcThreads = 256;        // 8 warps share the operand work; warps 0-3 own the lanes
+constexpr int kTcWinD = 64;            // doubles per staged history window (50 at most used)
+// shared memory (bytes): staged tiles [kTcStages][2 tensors][kTcTile] f32,
+// history windows [kTcStages][kTcWinD] f64, A operands [2 buffers][t0 hi,
+// t0 lo, t1 hi, t1 lo][kTcTile] f32, B operands [2 buffers][hi, lo][kTcBTile]
+// f32, Float64 sums [tensor x step][source]
+constexpr int kTcStgOff = 0;
+constexpr int kTcWinOff = kTcStgOff + kTcStages * 2 * kTcTile * 4;
+constexpr int kTcAOff = kTcWinOff + kTcStages * kTcWinD * 8;
+constexpr int kTcBOff = kTcAOff + 2 * 4 * kTcTile * 4;
+constexpr int kTcSumOff = kTcBOff + 2 * 2 * kTcBTile * 4;
+constexpr int kTcSmemBytes = kTcSumOff + 2 * kTcN * kTcM * 8;
+constexpr size_t kTcDynSmem = kTcSmemBytes + 1024;  // + alignment to 1 KB
 constexpr uint32_t kTcCols = 128;  // tensor-memory columns: 2 sets x 2 tensors x 32 steps
 static_assert(kTcM == 128 && kTcN % 16 == 0 && kTcN <= 256, "MMA shape M=128, N=32");
 static_assert(kTcCols >= 4 * kTcN, "two accumulator sets of two tensors");
@@ -101,10 +111,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+// x rounded to TF32 (10 stored mantissa bits, ties away from zero) by two
+// integer operations; x - tf32_hi(x) is exact in Float32
+__device__ __forceinline__ float tf32_hi(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // Packs the two tensors of an input-history map (layout as in
@@ -142,7 +152,7 @@ __global__ void adf_gf_tc_pack_kernel(const float* t0, const float* t1, float* o
 // (the same partials as adf_gf_far_kernel: gf_far[o][receiver split][step of
 // the block][2], added over the splits by adf_gf_far_combine_kernel).
 // blockIdx.x = source tile * gf_rs + receiver split, blockIdx.y = solve.
-__global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p) {
+__global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiParams p) {
   const SolveDev& S = p.solves[blockIdx.y];
   const int it0 = S.it_base + p.step;
   if (!(S.flags & SF_GF) || !(S.flags & SF_GF_TC) || S.gf_rs <= 0 || it0 > S.it_stop ||
@@ -157,33 +167,28 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
   const int nch = lag_hi >= 1 ? (lag_hi + kTcL - 1) / kTcL : 0;  // chunks this block needs
   const int Q = (r1 - r0) * nch;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int o = ot * kTcM + tid;  // this thread's source = its tensor-memory lane
-  double acc[2][kTcN];
-#pragma unroll
-  for (int t = 0; t < 2; ++t)
-#pragma unroll
-    for (int b = 0; b < kTcN; ++b) acc[t][b] = 0.0;
-  auto write_out = [&]() {
-    if (o >= nout) return;
-    double* pp = S.gf_far + ((long long)o * rsn + rsi) * kGfBlock * 2;
-#pragma unroll
-    for (int b = 0; b < kTcN; ++b) {
-      pp[2 * b] = acc[0][b];
-      pp[2 * b + 1] = acc[1][b];
-    }
-  };
+  const int o = ot * kTcM + tid;  // threads 0..127: this source = this tensor-memory lane
   if (Q == 0) {  // no far lag in this block (uniform across the CTA)
-    write_out();
+    if (tid < kTcM && o < nout) {
+      double* pp = S.gf_far + ((long long)o * rsn + rsi) * kGfBlock * 2;
+      for (int k = 0; k < 2 * kTcN; ++k) pp[k] = 0.0;
+    }
     return;
   }
 
   extern __shared__ unsigned char tc_smem_raw[];
-  float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) &
-                                       ~static_cast<uintptr_t>(1023));
-  __shared__ __align__(8) uint64_t full[kTcStages];  // staged tile landed
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  float* stg = reinterpret_cast<float*>(base + kTcStgOff);
+  double* win = reinterpret_cast<double*>(base + kTcWinOff);
+  float* opA = reinterpret_cast<float*>(base + kTcAOff);
+  float* opB = reinterpret_cast<float*>(base + kTcBOff);
+  double* sums = reinterpret_cast<double*>(base + kTcSumOff);
+  __shared__ __align__(8) uint64_t full[kTcStages];  // staged tile and window landed
   __shared__ __align__(8) uint64_t mmad[2];          // products of an operand buffer done
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
+  for (int i = tid; i < 2 * kTcN * kTcM; i += kTcThreads) sums[i] = 0.0;
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&full[s]), 1);
     for (int s = 0; s < 2; ++s) mbar_init(smem_u32(&mmad[s]), 1);
@@ -202,18 +207,36 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
   tc_fence_after();
   const uint32_t tbase = s_tmem;
 
-  const float* tiles = S.gf_tc;
+  // history window of chunk q: the input-history rows its far lags read,
+  // [max(0, it0-1-16(c+1)), min(it0-2, it0+29-16c)] of receiver r, copied
+  // from the even element at or below the first (16-B aligned source) for an
+  // even count of doubles; cnt = 0 when the chunk reads no row
+  auto win_of = [&](int q, long long& gs, int& cnt) {
+    const int rr = q / nch, c = q - rr * nch;
+    const int lo = max(0, it0 - 1 - kTcL * (c + 1)), hi = min(it0 - 2, it0 + kTcN - 3 - kTcL * c);
+    gs = 0;
+    cnt = 0;
+    if (hi < lo) return;
+    const long long g0 = (long long)(r0 + rr) * nt;
+    gs = (g0 + lo) & ~1LL;
+    cnt = (int)((g0 + hi - gs + 2) & ~1LL);
+  };
   auto tile_src = [&](int q) {
     const int rr = q / nch, c = q - rr * nch;
-    return tiles + (((long long)(r0 + rr) * S.gf_tc_nch + c) * notile + ot) * (2LL * kTcTile);
+    return S.gf_tc + (((long long)(r0 + rr) * S.gf_tc_nch + c) * notile + ot) * (2LL * kTcTile);
   };
-  int staged = 0;  // chunks whose bulk copy was issued (thread 0)
+  int staged = 0;  // chunks whose copies were issued (thread 0)
   auto stage = [&](int q) {
     const int s = q % kTcStages;
+    long long gs;
+    int cnt;
+    win_of(q, gs, cnt);
     fence_proxy_async_smem();  // the slot was last read through the generic proxy
-    mbar_expect_tx(smem_u32(&full[s]), (uint32_t)(2 * kTcTile * sizeof(float)));
-    bulk_load(smem_u32(sm + s * 2 * kTcTile), tile_src(q), (uint32_t)(2 * kTcTile * sizeof(float)),
-              smem_u32(&full[s]));
+    const uint32_t tb = (uint32_t)(2 * kTcTile * sizeof(float));
+    mbar_expect_tx(smem_u32(&full[s]), tb + (uint32_t)cnt * 8u);
+    bulk_load(smem_u32(stg + s * 2 * kTcTile), tile_src(q), tb, smem_u32(&full[s]));
+    if (cnt > 0)
+      bulk_load(smem_u32(win + s * kTcWinD), S.gf_pin + gs, (uint32_t)cnt * 8u, smem_u32(&full[s]));
     staged = q + 1;
   };
   if (tid == 0)
@@ -224,7 +247,8 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
       s_abort = 1;         // read by every thread after the next barrier
     }
   };
-  // adds accumulator set `set` (lanes of this warp) into the Float64 sums
+  // warps 0-3: adds accumulator set `set` of this warp's lanes into the
+  // Float64 sums (step-major, source fastest)
   auto drain = [&](int set) {
     const uint32_t ta = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(set * 2 * kTcN);
 #pragma unroll
@@ -234,62 +258,64 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
         uint32_t v[16];
         tmem_ld16(ta + t * kTcN + h * 16, v);
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          acc[t][h * 16 + j] = __dadd_rn(acc[t][h * 16 + j], (double)__uint_as_float(v[j]));
+        for (int j = 0; j < 16; ++j) {
+          double* a = sums + (t * kTcN + h * 16 + j) * kTcM + tid;
+          *a = __dadd_rn(*a, (double)__uint_as_float(v[j]));
+        }
       }
   };
+  const uint64_t descA = umma_desc(smem_u32(opA), kTcALbo, kTcSbo);
+  const uint64_t descB = umma_desc(smem_u32(opB), kTcBLbo, kTcSbo);
 
   int q = 0;
   bool aborted = false;
   for (; q < Q; ++q) {
     const int s = q % kTcStages, buf = q & 1;
     const int rr = q / nch, c = q - rr * nch, r = r0 + rr;
-    if (c == 0 && q > 0) {  // the previous receiver's products (last chunk q-1) into Float64
+    if (c == 0 && q > 0 && warp < 4) {  // the previous receiver's products into Float64
       bounded(&mmad[(q - 1) & 1], (q - 1) >> 1);
       tc_fence_after();
       drain((rr - 1) & 1);
     }
     if (q >= 2) bounded(&mmad[buf], (q - 2) >> 1);  // operand buffer read by chunk q-2
     bounded(&full[s], q / kTcStages);
-    // the staged tile -> TF32 high parts and remainders
+    // the staged tile -> TF32 parts and remainders (4 float4 per thread)
     {
-      const float* stg = sm + s * 2 * kTcTile;
-      float* A = sm + kTcAOff + buf * 4 * kTcTile;
-#pragma unroll 2
-      for (int i = tid; i < 2 * kTcTile / 4; i += kTcM) {
-        const float4 x = *reinterpret_cast<const float4*>(stg + 4 * i);
-        const int t = (4 * i) / kTcTile, e = 4 * i - t * kTcTile;
-        float4 hi, lo;
-        hi.x = tf32_rna(x.x);
-        hi.y = tf32_rna(x.y);
-        hi.z = tf32_rna(x.z);
-        hi.w = tf32_rna(x.w);
-        lo.x = __fsub_rn(x.x, hi.x);
-        lo.y = __fsub_rn(x.y, hi.y);
-        lo.z = __fsub_rn(x.z, hi.z);
-        lo.w = __fsub_rn(x.w, hi.w);
+      const float* st = stg + s * 2 * kTcTile;
+      float* A = opA + buf * 4 * kTcTile;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int t = k >> 1, e = 4 * tid + (kTcTile / 2) * (k & 1);
+        const float4 x = *reinterpret_cast<const float4*>(st + t * kTcTile + e);
+        const float4 hi = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+        const float4 lo = make_float4(__fsub_rn(x.x, hi.x), __fsub_rn(x.y, hi.y),
+                                      __fsub_rn(x.z, hi.z), __fsub_rn(x.w, hi.w));
         *reinterpret_cast<float4*>(A + (2 * t) * kTcTile + e) = hi;
         *reinterpret_cast<float4*>(A + (2 * t + 1) * kTcTile + e) = lo;
       }
     }
     // the block's far-lag window of receiver r's input history: thread ->
-    // step b = tid/4, lags 4(tid%4) .. +3 of the chunk (one core-matrix row)
+    // step b = tid/8, lags 2(tid%8), +1 of the chunk (half a core-matrix row)
     {
-      const int b = tid >> 2, kb = tid & 3;
-      const double* hist = S.gf_pin + (long long)r * nt;
+      long long gs;
+      int cnt;
+      win_of(q, gs, cnt);
+      const double* w = win + s * kTcWinD;
+      const long long row0 = (long long)r * nt - gs;  // window index of history row 0
+      const int b = tid >> 3, pr = tid & 7;
       const int lim = min(it0 + b, ngf);
-      float hv[4], lv[4];
+      float hv[2], lv[2];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int lag = kTcL * c + 1 + 4 * kb + j;
-        const double h = (lag > b && lag < lim) ? hist[it0 - 1 + b - lag] : 0.0;
-        hv[j] = tf32_rna((float)h);
+      for (int j = 0; j < 2; ++j) {
+        const int lag = kTcL * c + 1 + 2 * pr + j;
+        const double h = (lag > b && lag < lim) ? w[row0 + it0 - 1 + b - lag] : 0.0;
+        hv[j] = tf32_hi((float)h);
         lv[j] = (float)(h - (double)hv[j]);
       }
-      float* B = sm + kTcBOff + buf * 2 * kTcBTile;
-      const int off = (kb * (kTcN / 8) + (b >> 3)) * 32 + (b & 7) * 4;
-      *reinterpret_cast<float4*>(B + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-      *reinterpret_cast<float4*>(B + kTcBTile + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+      float* B = opB + buf * 2 * kTcBTile;
+      const int off = ((pr >> 1) * (kTcN / 8) + (b >> 3)) * 32 + (b & 7) * 4 + (pr & 1) * 2;
+      *reinterpret_cast<float2*>(B + off) = make_float2(hv[0], hv[1]);
+      *reinterpret_cast<float2*>(B + kTcBTile + off) = make_float2(lv[0], lv[1]);
     }
     fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
     tc_fence_before();
@@ -302,18 +328,17 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
       tc_fence_after();
       if (q + kTcStages < Q) stage(q + kTcStages);  // slot s was consumed by the split
       const uint32_t set = (uint32_t)((rr & 1) * 2 * kTcN);
-      const uint32_t a0 = smem_u32(sm + kTcAOff + buf * 4 * kTcTile);
-      const uint32_t b0 = smem_u32(sm + kTcBOff + buf * 2 * kTcBTile);
+      const uint64_t a0 = descA + (uint64_t)((buf * 4 * kTcTile * 4) >> 4);
+      const uint64_t b0 = descB + (uint64_t)((buf * 2 * kTcBTile * 4) >> 4);
 #pragma unroll
       for (int ks = 0; ks < kTcL / 8; ++ks) {
-        const uint64_t bh = umma_desc(b0 + ks * 2 * kTcBLbo, kTcBLbo, kTcSbo);
-        const uint64_t bl = umma_desc(b0 + kTcBTile * 4 + ks * 2 * kTcBLbo, kTcBLbo, kTcSbo);
+        const uint64_t bh = b0 + ((ks * 2 * kTcBLbo) >> 4);
+        const uint64_t bl = bh + ((kTcBTile * 4) >> 4);
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
           const uint32_t d = tbase + set + (uint32_t)(t * kTcN);
-          const uint64_t ah = umma_desc(a0 + (2 * t) * kTcTile * 4 + ks * 2 * kTcALbo, kTcALbo, kTcSbo);
-          const uint64_t al =
-              umma_desc(a0 + (2 * t + 1) * kTcTile * 4 + ks * 2 * kTcALbo, kTcALbo, kTcSbo);
+          const uint64_t ah = a0 + (((2 * t) * kTcTile * 4 + ks * 2 * kTcALbo) >> 4);
+          const uint64_t al = ah + ((kTcTile * 4) >> 4);
           tc_mma_tf32(d, ah, bh, (c > 0 || ks > 0) ? 1u : 0u);  // a receiver's first product overwrites
           tc_mma_tf32(d, ah, bl, 1u);
           tc_mma_tf32(d, al, bh, 1u);
@@ -322,7 +347,7 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
       tc_commit(smem_u32(&mmad[buf]));
     }
   }
-  if (!aborted) {  // the last receiver's products
+  if (!aborted && warp < 4) {  // the last receiver's products
     bounded(&mmad[(Q - 1) & 1], (Q - 1) >> 1);
     tc_fence_after();
     drain(((Q - 1) / nch) & 1);
@@ -337,8 +362,13 @@ __global__ void __launch_bounds__(128, 1) adf_gf_far_tc_kernel(const EpiParams p
         mbar_wait(smem_u32(&full[k % kTcStages]), (uint32_t)(k / kTcStages) & 1u, kTcWaitLimit);
       if (q > 0) mbar_wait(smem_u32(&mmad[(q - 1) & 1]), (uint32_t)((q - 1) >> 1) & 1u, kTcWaitLimit);
     }
-  } else {
-    write_out();
+  } else if (tid < kTcM && o < nout) {
+    double* pp = S.gf_far + ((long long)o * rsn + rsi) * kGfBlock * 2;
+#pragma unroll 4
+    for (int b = 0; b < kTcN; ++b) {
+      pp[2 * b] = sums[b * kTcM + tid];
+      pp[2 * b + 1] = sums[(kTcN + b) * kTcM + tid];
+    }
   }
   __syncthreads();
   if (warp == 0) {
@@ -370,7 +400,8 @@ cudaError_t launch_gf_far_tc(const EpiParams& p, int max_blocks, cudaStream_t s)
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  adf_gf_far_tc_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), kTcM, kTcDynSmem, s>>>(p);
+  adf_gf_far_tc_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), kTcThreads, kTcDynSmem,
+                         s>>>(p);
   return cudaGetLastError();
 }
 
