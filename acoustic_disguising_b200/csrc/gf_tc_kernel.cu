@@ -22,21 +22,22 @@
 // (ADF_GF_CONTRACT_TF32X3); the default path keeps the Float64 FMAs of the
 // reference's accumulation.
 //
-// Data path: the two tensors of the map are packed once per map
-// (adf_gf_tc_pack_kernel) into 16 KB tiles (receiver, 16-lag chunk,
-// 128-source tile) laid out as the MMA's K-major, no-swizzle operand (8-row x
-// 16-byte core matrices), so one bulk copy (cp.async.bulk, completing on an
-// mbarrier, no multicast) stages a chunk, and a second one on the same
-// mbarrier brings the chunk's rows of the input history; four chunks are in
-// flight.  The CTA's 256 threads split the staged tile and build the history
-// window into a double-buffered operand area, one thread issues the 12 MMAs
-// of the chunk and commits them to the buffer's mbarrier, warps 0-3 (the
-// owners of the 128 tensor-memory lanes) drain the accumulators.  One CTA
-// (256 threads, 204 KB of shared memory, 128 tensor-memory columns) per SM
-// and (source tile, receiver split); every wait is bounded and a wait that
-// gives up sets the solve's error word (ADF_E_TIMEOUT), lets the copies and
-// products in flight land, frees the tensor memory and leaves the partials
-// unwritten.
+// Data path: the two tensors of the map are split and packed once per map
+// (adf_gf_tc_pack_kernel) into 32 KB tiles (receiver, 16-lag chunk,
+// 128-source tile; TF32 parts and remainders of both tensors) laid out as
+// the MMA's K-major, no-swizzle operands (8-row x 16-byte core matrices), so
+// one bulk copy (cp.async.bulk, completing on an mbarrier, no multicast)
+// stages a chunk's A operands where the MMAs read them, and a second one on
+// the same mbarrier brings the chunk's rows of the input history; four chunks
+// are staged, the next two in flight while two are in use.  The CTA's 256
+// threads build the history window operand (double-buffered), one thread
+// issues the 12 MMAs of the chunk, commits them to the slot's mbarrier and
+// refills the slot of the chunk two back, warps 0-3 (the owners of the 128
+// tensor-memory lanes) drain the accumulators.  One CTA (256 threads, 204 KB
+// of shared memory, 128 tensor-memory columns) per SM and (source tile,
+// receiver split); every wait is bounded and a wait that gives up sets the
+// solve's error word (ADF_E_TIMEOUT), lets the copies and products in flight
+// land, frees the tensor memory and leaves the partials unwritten.
 #include "adf_internal.h"
 #include "ptx_util.h"
 
@@ -50,14 +51,13 @@ constexpr int kTcTile = kTcL * kTcM;   // floats of one tensor's tile (8 KB)
 constexpr int kTcBTile = kTcN * kTcL;  // floats of one history window operand (2 KB)
 constexpr int kTcThreads = 256;        // 8 warps share the operand work; warps 0-3 own the lanes
 constexpr int kTcWinD = 64;            // doubles per staged history window (50 at most used)
-// shared memory (bytes): staged tiles [kTcStages][2 tensors][kTcTile] f32,
-// history windows [kTcStages][kTcWinD] f64, A operands [2 buffers][t0 hi,
-// t0 lo, t1 hi, t1 lo][kTcTile] f32, B operands [2 buffers][hi, lo][kTcBTile]
-// f32, Float64 sums [tensor x step][source]
+// shared memory (bytes): staged operand tiles [kTcStages][tensor][hi, lo]
+// [kTcTile] f32 (read by the MMAs where they land), history windows
+// [kTcStages][kTcWinD] f64, B operands [2 buffers][hi, lo][kTcBTile] f32,
+// Float64 sums [tensor x step][source]
 constexpr int kTcStgOff = 0;
-constexpr int kTcWinOff = kTcStgOff + kTcStages * 2 * kTcTile * 4;
-constexpr int kTcAOff = kTcWinOff + kTcStages * kTcWinD * 8;
-constexpr int kTcBOff = kTcAOff + 2 * 4 * kTcTile * 4;
+constexpr int kTcWinOff = kTcStgOff + kTcStages * 4 * kTcTile * 4;
+constexpr int kTcBOff = kTcWinOff + kTcStages * kTcWinD * 8;
 constexpr int kTcSumOff = kTcBOff + 2 * 2 * kTcBTile * 4;
 constexpr int kTcSmemBytes = kTcSumOff + 2 * kTcN * kTcM * 8;
 constexpr size_t kTcDynSmem = kTcSmemBytes + 1024;  // + alignment to 1 KB
@@ -120,11 +120,11 @@ __device__ __forceinline__ float tf32_hi(float x) {
 // Packs the two tensors of an input-history map (layout as in
 // adf_gf_far_kernel: PVFromPin element lag + ngf*(o + n1*r), PFromPin
 // lag + ngf*(r + n1*o)) into tiles (r, chunk c, source tile ot) of
-// [tensor][kb][g][row][4]: source ot*128 + 8g + row, lag 16c + 1 + 4kb + col,
-// zero beyond the map.  Set-up, once per map.
+// [tensor][TF32 part, remainder][kb][g][row][4]: source ot*128 + 8g + row,
+// lag 16c + 1 + 4kb + col, zero beyond the map.  Set-up, once per map.
 __global__ void adf_gf_tc_pack_kernel(const float* t0, const float* t1, float* out, int kind,
                                       int ngf, int n1, int nout, int nin, int nch, int notile) {
-  const long long per_tile = 2LL * kTcTile;
+  const long long per_tile = 4LL * kTcTile;
   const long long total = (long long)nin * nch * notile * per_tile;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
@@ -134,7 +134,7 @@ __global__ void adf_gf_tc_pack_kernel(const float* t0, const float* t1, float* o
     tile /= notile;
     const int c = (int)(tile % nch);
     const int r = (int)(tile / nch);
-    const int t = e / kTcTile, w = e - t * kTcTile;
+    const int t = e / (2 * kTcTile), part = (e / kTcTile) & 1, w = e % kTcTile;
     const int kb = w / (kTcM * 4), rem = w - kb * (kTcM * 4);
     const int g = rem >> 5, row = (rem >> 2) & 7, col = rem & 3;
     const int o = ot * kTcM + g * 8 + row, lag = kTcL * c + 1 + 4 * kb + col;
@@ -144,7 +144,8 @@ __global__ void adf_gf_tc_pack_kernel(const float* t0, const float* t1, float* o
                                                         : lag + (long long)ngf * (r + (long long)n1 * o);
       v = (t == 0 ? t0 : t1)[idx];
     }
-    out[i] = v;
+    const float hi = tf32_hi(v);
+    out[i] = part == 0 ? hi : __fsub_rn(v, hi);
   }
 }
 
@@ -181,17 +182,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   float* stg = reinterpret_cast<float*>(base + kTcStgOff);
   double* win = reinterpret_cast<double*>(base + kTcWinOff);
-  float* opA = reinterpret_cast<float*>(base + kTcAOff);
   float* opB = reinterpret_cast<float*>(base + kTcBOff);
   double* sums = reinterpret_cast<double*>(base + kTcSumOff);
   __shared__ __align__(8) uint64_t full[kTcStages];  // staged tile and window landed
-  __shared__ __align__(8) uint64_t mmad[2];          // products of an operand buffer done
+  __shared__ __align__(8) uint64_t mmad[kTcStages];  // products of a staged chunk done
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   for (int i = tid; i < 2 * kTcN * kTcM; i += kTcThreads) sums[i] = 0.0;
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&full[s]), 1);
-    for (int s = 0; s < 2; ++s) mbar_init(smem_u32(&mmad[s]), 1);
+    for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&mmad[s]), 1);
     fence_mbar_init();
     s_abort = 0;
   }
@@ -207,12 +207,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
   tc_fence_after();
   const uint32_t tbase = s_tmem;
 
-  // history window of chunk q: the input-history rows its far lags read,
-  // [max(0, it0-1-16(c+1)), min(it0-2, it0+29-16c)] of receiver r, copied
-  // from the even element at or below the first (16-B aligned source) for an
-  // even count of doubles; cnt = 0 when the chunk reads no row
-  auto win_of = [&](int q, long long& gs, int& cnt) {
-    const int rr = q / nch, c = q - rr * nch;
+  // solve fields used in the loop, read once (the loop's fences would
+  // otherwise reload them from global memory every chunk)
+  const float* gtc = S.gf_tc;
+  const double* gpin = S.gf_pin;
+  int* gerr = S.err;
+  const long long cstride = (long long)notile * 4 * kTcTile;  // floats per 16-lag chunk
+  const long long rstride = (long long)S.gf_tc_nch * cstride;  // floats per receiver
+  // history window of chunk (receiver r0+rr, chunk c): the input-history
+  // rows its far lags read, [max(0, it0-1-16(c+1)), min(it0-2, it0+29-16c)],
+  // copied from the even element at or below the first (16-B aligned source)
+  // for an even count of doubles; cnt = 0 when the chunk reads no row
+  auto win_of = [&](int rr, int c, long long& gs, int& cnt) {
     const int lo = max(0, it0 - 1 - kTcL * (c + 1)), hi = min(it0 - 2, it0 + kTcN - 3 - kTcL * c);
     gs = 0;
     cnt = 0;
@@ -221,29 +227,32 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
     gs = (g0 + lo) & ~1LL;
     cnt = (int)((g0 + hi - gs + 2) & ~1LL);
   };
-  auto tile_src = [&](int q) {
-    const int rr = q / nch, c = q - rr * nch;
-    return S.gf_tc + (((long long)(r0 + rr) * S.gf_tc_nch + c) * notile + ot) * (2LL * kTcTile);
-  };
-  int staged = 0;  // chunks whose copies were issued (thread 0)
-  auto stage = [&](int q) {
-    const int s = q % kTcStages;
+  // thread 0: the next chunk to stage, as (receiver offset, chunk)
+  int staged = 0, srr = 0, sc = 0;
+  auto stage_next = [&]() {
+    const int s = staged % kTcStages;
     long long gs;
     int cnt;
-    win_of(q, gs, cnt);
+    win_of(srr, sc, gs, cnt);
     fence_proxy_async_smem();  // the slot was last read through the generic proxy
-    const uint32_t tb = (uint32_t)(2 * kTcTile * sizeof(float));
+    const uint32_t tb = (uint32_t)(4 * kTcTile * sizeof(float));
     mbar_expect_tx(smem_u32(&full[s]), tb + (uint32_t)cnt * 8u);
-    bulk_load(smem_u32(stg + s * 2 * kTcTile), tile_src(q), tb, smem_u32(&full[s]));
+    bulk_load(smem_u32(stg + s * 4 * kTcTile),
+              gtc + (long long)(r0 + srr) * rstride + sc * cstride + ot * (4LL * kTcTile), tb,
+              smem_u32(&full[s]));
     if (cnt > 0)
-      bulk_load(smem_u32(win + s * kTcWinD), S.gf_pin + gs, (uint32_t)cnt * 8u, smem_u32(&full[s]));
-    staged = q + 1;
+      bulk_load(smem_u32(win + s * kTcWinD), gpin + gs, (uint32_t)cnt * 8u, smem_u32(&full[s]));
+    ++staged;
+    if (++sc == nch) {
+      sc = 0;
+      ++srr;
+    }
   };
   if (tid == 0)
-    for (int q = 0; q < min(Q, kTcStages); ++q) stage(q);
+    while (staged < min(Q, kTcStages)) stage_next();
   auto bounded = [&](uint64_t* bar, int phase) {
     if (!mbar_wait(smem_u32(bar), (uint32_t)phase & 1u, kTcWaitLimit)) {
-      atomicOr(S.err, 4);  // reported as ADF_E_TIMEOUT
+      atomicOr(gerr, 4);  // reported as ADF_E_TIMEOUT
       s_abort = 1;         // read by every thread after the next barrier
     }
   };
@@ -264,42 +273,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
         }
       }
   };
-  const uint64_t descA = umma_desc(smem_u32(opA), kTcALbo, kTcSbo);
+  const uint64_t descA = umma_desc(smem_u32(stg), kTcALbo, kTcSbo);
   const uint64_t descB = umma_desc(smem_u32(opB), kTcBLbo, kTcSbo);
 
-  int q = 0;
+  int q = 0, rr = 0, c = 0;  // chunk q = chunk c of receiver r0 + rr
   bool aborted = false;
-  for (; q < Q; ++q) {
-    const int s = q % kTcStages, buf = q & 1;
-    const int rr = q / nch, c = q - rr * nch, r = r0 + rr;
+  for (; q < Q; ++q, c = (c + 1 == nch ? 0 : c + 1), rr += (c == 0)) {
+    const int s = q % kTcStages, buf = q & 1, r = r0 + rr;
     if (c == 0 && q > 0 && warp < 4) {  // the previous receiver's products into Float64
-      bounded(&mmad[(q - 1) & 1], (q - 1) >> 1);
+      bounded(&mmad[(q - 1) % kTcStages], (q - 1) / kTcStages);
       tc_fence_after();
       drain((rr - 1) & 1);
     }
-    if (q >= 2) bounded(&mmad[buf], (q - 2) >> 1);  // operand buffer read by chunk q-2
+    if (q >= 2) bounded(&mmad[(q - 2) % kTcStages], (q - 2) / kTcStages);  // B buffer of q-2
     bounded(&full[s], q / kTcStages);
-    // the staged tile -> TF32 parts and remainders (4 float4 per thread)
-    {
-      const float* st = stg + s * 2 * kTcTile;
-      float* A = opA + buf * 4 * kTcTile;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int t = k >> 1, e = 4 * tid + (kTcTile / 2) * (k & 1);
-        const float4 x = *reinterpret_cast<const float4*>(st + t * kTcTile + e);
-        const float4 hi = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
-        const float4 lo = make_float4(__fsub_rn(x.x, hi.x), __fsub_rn(x.y, hi.y),
-                                      __fsub_rn(x.z, hi.z), __fsub_rn(x.w, hi.w));
-        *reinterpret_cast<float4*>(A + (2 * t) * kTcTile + e) = hi;
-        *reinterpret_cast<float4*>(A + (2 * t + 1) * kTcTile + e) = lo;
-      }
-    }
     // the block's far-lag window of receiver r's input history: thread ->
     // step b = tid/8, lags 2(tid%8), +1 of the chunk (half a core-matrix row)
     {
       long long gs;
       int cnt;
-      win_of(q, gs, cnt);
+      win_of(rr, c, gs, cnt);
       const double* w = win + s * kTcWinD;
       const long long row0 = (long long)r * nt - gs;  // window index of history row 0
       const int b = tid >> 3, pr = tid & 7;
@@ -317,7 +310,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
       *reinterpret_cast<float2*>(B + off) = make_float2(hv[0], hv[1]);
       *reinterpret_cast<float2*>(B + kTcBTile + off) = make_float2(lv[0], lv[1]);
     }
-    fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
+    fence_proxy_async_smem();  // the B operand is read by the tensor cores (async proxy)
     tc_fence_before();
     __syncthreads();
     if (s_abort) {
@@ -326,9 +319,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
     }
     if (tid == 0) {
       tc_fence_after();
-      if (q + kTcStages < Q) stage(q + kTcStages);  // slot s was consumed by the split
       const uint32_t set = (uint32_t)((rr & 1) * 2 * kTcN);
-      const uint64_t a0 = descA + (uint64_t)((buf * 4 * kTcTile * 4) >> 4);
+      const uint64_t a0 = descA + (uint64_t)((s * 4 * kTcTile * 4) >> 4);
       const uint64_t b0 = descB + (uint64_t)((buf * 2 * kTcBTile * 4) >> 4);
 #pragma unroll
       for (int ks = 0; ks < kTcL / 8; ++ks) {
@@ -344,11 +336,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
           tc_mma_tf32(d, al, bh, 1u);
         }
       }
-      tc_commit(smem_u32(&mmad[buf]));
+      tc_commit(smem_u32(&mmad[s]));
+      // the slot of chunk q-2 is free once its products are done: chunk q+2
+      if (q >= 2 && staged < Q) {
+        bounded(&mmad[(q - 2) % kTcStages], (q - 2) / kTcStages);
+        stage_next();
+      }
     }
   }
   if (!aborted && warp < 4) {  // the last receiver's products
-    bounded(&mmad[(Q - 1) & 1], (Q - 1) >> 1);
+    bounded(&mmad[(Q - 1) % kTcStages], (Q - 1) / kTcStages);
     tc_fence_after();
     drain(((Q - 1) / nch) & 1);
   }
@@ -360,7 +357,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
     if (tid == 0) {
       for (int k = q; k < staged; ++k)
         mbar_wait(smem_u32(&full[k % kTcStages]), (uint32_t)(k / kTcStages) & 1u, kTcWaitLimit);
-      if (q > 0) mbar_wait(smem_u32(&mmad[(q - 1) & 1]), (uint32_t)((q - 1) >> 1) & 1u, kTcWaitLimit);
+      if (q > 0)
+        mbar_wait(smem_u32(&mmad[(q - 1) % kTcStages]), (uint32_t)((q - 1) / kTcStages) & 1u,
+                  kTcWaitLimit);
     }
   } else if (tid < kTcM && o < nout) {
     double* pp = S.gf_far + ((long long)o * rsn + rsi) * kGfBlock * 2;
@@ -380,7 +379,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
 
 int64_t gf_tc_chunks(int64_t nt_gf) { return nt_gf > 1 ? (nt_gf - 1 + kTcL - 1) / kTcL : 1; }
 size_t gf_tc_packed_floats(int64_t nt_gf, int64_t n_src, int64_t n_rec) {
-  return (size_t)n_rec * gf_tc_chunks(nt_gf) * ((n_src + kTcM - 1) / kTcM) * 2 * kTcTile;
+  return (size_t)n_rec * gf_tc_chunks(nt_gf) * ((n_src + kTcM - 1) / kTcM) * 4 * kTcTile;
 }
 int gf_tc_sources_per_tile() { return kTcM; }
 
