@@ -29,15 +29,17 @@
 // one bulk copy (cp.async.bulk, completing on an mbarrier, no multicast)
 // stages a chunk's A operands where the MMAs read them, and a second one on
 // the same mbarrier brings the chunk's rows of the input history; four chunks
-// are staged, the next two in flight while two are in use.  The CTA's 256
-// threads build the history window operand (double-buffered), one thread
-// issues the 12 MMAs of the chunk, commits them to the slot's mbarrier and
-// refills the slot of the chunk two back, warps 0-3 (the owners of the 128
-// tensor-memory lanes) drain the accumulators.  One CTA (256 threads, 204 KB
-// of shared memory, 128 tensor-memory columns) per SM and (source tile,
-// receiver split); every wait is bounded and a wait that gives up sets the
-// solve's error word (ADF_E_TIMEOUT), lets the copies and products in flight
-// land, frees the tensor memory and leaves the partials unwritten.
+// are staged, the next two in flight while two are in use.  Warps are
+// specialised and hand work over on mbarriers, with no CTA barrier inside
+// the loop: warps 0-3 (the owners of the 128 tensor-memory lanes) build each
+// chunk's history operand (double-buffered) and drain the accumulators; one
+// thread of warp 4 waits for a chunk's tile and operand, issues its 12 MMAs,
+// commits them to the slot's mbarrier and refills the slot of the chunk two
+// back.  One CTA (160 threads, 204 KB of shared memory, 128 tensor-memory
+// columns) per SM and (source tile, receiver split); every wait is bounded
+// and a wait that gives up sets the solve's error word (ADF_E_TIMEOUT), ends
+// every role's loop, lets the copies and products in flight land, frees the
+// tensor memory and leaves the partials unwritten.
 #include "adf_internal.h"
 #include "ptx_util.h"
 
@@ -49,7 +51,8 @@ constexpr int kTcN = kGfBlock;         // steps of a block (MMA N)
 constexpr int kTcStages = 4;           // staged map tiles in flight
 constexpr int kTcTile = kTcL * kTcM;   // floats of one tensor's tile (8 KB)
 constexpr int kTcBTile = kTcN * kTcL;  // floats of one history window operand (2 KB)
-constexpr int kTcThreads = 256;        // 8 warps share the operand work; warps 0-3 own the lanes
+constexpr int kTcThreads = 160;        // warps 0-3: history operand, drains; warp 4: MMAs, copies
+constexpr int kTcIssuer = 128;         // the thread that issues the MMAs and the bulk copies
 constexpr int kTcWinD = 64;            // doubles per staged history window (50 at most used)
 // shared memory (bytes): staged operand tiles [kTcStages][tensor][hi, lo]
 // [kTcTile] f32 (read by the MMAs where they land), history windows
@@ -186,12 +189,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
   double* sums = reinterpret_cast<double*>(base + kTcSumOff);
   __shared__ __align__(8) uint64_t full[kTcStages];  // staged tile and window landed
   __shared__ __align__(8) uint64_t mmad[kTcStages];  // products of a staged chunk done
+  __shared__ __align__(8) uint64_t bready[2];        // history operand of a buffer built
+  __shared__ __align__(8) uint64_t drained[2];       // accumulator set added into the sums
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   for (int i = tid; i < 2 * kTcN * kTcM; i += kTcThreads) sums[i] = 0.0;
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&full[s]), 1);
     for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&mmad[s]), 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(smem_u32(&bready[s]), 4);   // one arrival per builder warp
+      mbar_init(smem_u32(&drained[s]), 4);
+    }
     fence_mbar_init();
     s_abort = 0;
   }
@@ -227,7 +236,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
     gs = (g0 + lo) & ~1LL;
     cnt = (int)((g0 + hi - gs + 2) & ~1LL);
   };
-  // thread 0: the next chunk to stage, as (receiver offset, chunk)
+  // issuer: the next chunk to stage, as (receiver offset, chunk)
   int staged = 0, srr = 0, sc = 0;
   auto stage_next = [&]() {
     const int s = staged % kTcStages;
@@ -248,12 +257,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
       ++srr;
     }
   };
-  if (tid == 0)
+  if (tid == kTcIssuer)
     while (staged < min(Q, kTcStages)) stage_next();
   auto bounded = [&](uint64_t* bar, int phase) {
     if (!mbar_wait(smem_u32(bar), (uint32_t)phase & 1u, kTcWaitLimit)) {
       atomicOr(gerr, 4);  // reported as ADF_E_TIMEOUT
-      s_abort = 1;         // read by every thread after the next barrier
+      s_abort = 1;         // every role leaves its loop
     }
   };
   // warps 0-3: adds accumulator set `set` of this warp's lanes into the
@@ -276,48 +285,68 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
   const uint64_t descA = umma_desc(smem_u32(stg), kTcALbo, kTcSbo);
   const uint64_t descB = umma_desc(smem_u32(opB), kTcBLbo, kTcSbo);
 
-  int q = 0, rr = 0, c = 0;  // chunk q = chunk c of receiver r0 + rr
-  bool aborted = false;
-  for (; q < Q; ++q, c = (c + 1 == nch ? 0 : c + 1), rr += (c == 0)) {
-    const int s = q % kTcStages, buf = q & 1, r = r0 + rr;
-    if (c == 0 && q > 0 && warp < 4) {  // the previous receiver's products into Float64
-      bounded(&mmad[(q - 1) % kTcStages], (q - 1) / kTcStages);
-      tc_fence_after();
-      drain((rr - 1) & 1);
-    }
-    if (q >= 2) bounded(&mmad[(q - 2) % kTcStages], (q - 2) / kTcStages);  // B buffer of q-2
-    bounded(&full[s], q / kTcStages);
-    // the block's far-lag window of receiver r's input history: thread ->
-    // step b = tid/8, lags 2(tid%8), +1 of the chunk (half a core-matrix row)
-    {
-      long long gs;
-      int cnt;
-      win_of(rr, c, gs, cnt);
-      const double* w = win + s * kTcWinD;
-      const long long row0 = (long long)r * nt - gs;  // window index of history row 0
-      const int b = tid >> 3, pr = tid & 7;
-      const int lim = min(it0 + b, ngf);
-      float hv[2], lv[2];
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int lag = kTcL * c + 1 + 2 * pr + j;
-        const double h = (lag > b && lag < lim) ? w[row0 + it0 - 1 + b - lag] : 0.0;
-        hv[j] = tf32_hi((float)h);
-        lv[j] = (float)(h - (double)hv[j]);
+  // Warps 0-3 build each chunk's history operand and hand it over on
+  // bready; the issuer waits for the staged tile and the operand, issues the
+  // chunk's products and commits them to mmad; no CTA barrier inside the
+  // loop, so building, issuing and the tensor cores overlap across chunks.
+  const int lane = tid & 31;
+  auto abort_seen = [&]() { return *reinterpret_cast<volatile int*>(&s_abort) != 0; };
+  int q = 0;  // the chunk this thread's role stopped at
+  if (warp < 4) {
+    int rr = 0, c = 0;  // chunk q = chunk c of receiver r0 + rr
+    for (; q < Q; ++q, c = (c + 1 == nch ? 0 : c + 1), rr += (c == 0)) {
+      const int s = q % kTcStages, buf = q & 1, r = r0 + rr;
+      if (c == 0 && q > 0) {  // the previous receiver's products into Float64
+        bounded(&mmad[(q - 1) % kTcStages], (q - 1) / kTcStages);
+        tc_fence_after();
+        drain((rr - 1) & 1);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&drained[(rr - 1) & 1]));
       }
-      float* B = opB + buf * 2 * kTcBTile;
-      const int off = ((pr >> 1) * (kTcN / 8) + (b >> 3)) * 32 + (b & 7) * 4 + (pr & 1) * 2;
-      *reinterpret_cast<float2*>(B + off) = make_float2(hv[0], hv[1]);
-      *reinterpret_cast<float2*>(B + kTcBTile + off) = make_float2(lv[0], lv[1]);
+      if (q >= 2) bounded(&mmad[(q - 2) % kTcStages], (q - 2) / kTcStages);  // B buffer of q-2
+      bounded(&full[s], q / kTcStages);
+      // the block's far-lag window of receiver r's input history: thread ->
+      // step b = tid/4, lags 4(tid%4) .. +3 of the chunk (one core-matrix row)
+      {
+        long long gs;
+        int cnt;
+        win_of(rr, c, gs, cnt);
+        const double* w = win + s * kTcWinD;
+        const long long row0 = (long long)r * nt - gs;  // window index of history row 0
+        const int b = tid >> 2, kb = tid & 3;
+        const int lim = min(it0 + b, ngf);
+        float hv[4], lv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int lag = kTcL * c + 1 + 4 * kb + j;
+          const double h = (lag > b && lag < lim) ? w[row0 + it0 - 1 + b - lag] : 0.0;
+          hv[j] = tf32_hi((float)h);
+          lv[j] = (float)(h - (double)hv[j]);
+        }
+        float* B = opB + buf * 2 * kTcBTile;
+        const int off = (kb * (kTcN / 8) + (b >> 3)) * 32 + (b & 7) * 4;
+        *reinterpret_cast<float4*>(B + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<float4*>(B + kTcBTile + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+      }
+      fence_proxy_async_smem();  // the B operand is read by the tensor cores (async proxy)
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bready[buf]));
+      if (abort_seen()) break;
     }
-    fence_proxy_async_smem();  // the B operand is read by the tensor cores (async proxy)
-    tc_fence_before();
-    __syncthreads();
-    if (s_abort) {
-      aborted = true;
-      break;
+    if (q == Q && !abort_seen()) {  // the last receiver's products
+      bounded(&mmad[(Q - 1) % kTcStages], (Q - 1) / kTcStages);
+      tc_fence_after();
+      drain(((Q - 1) / nch) & 1);
     }
-    if (tid == 0) {
+  } else if (tid == kTcIssuer) {
+    int rr = 0, c = 0;
+    for (; q < Q; ++q, c = (c + 1 == nch ? 0 : c + 1), rr += (c == 0)) {
+      const int s = q % kTcStages, buf = q & 1;
+      bounded(&full[s], q / kTcStages);
+      bounded(&bready[buf], q >> 1);
+      if (c == 0 && rr >= 2) bounded(&drained[rr & 1], (rr - 2) >> 1);  // set of receiver rr-2
+      if (abort_seen()) break;
       tc_fence_after();
       const uint32_t set = (uint32_t)((rr & 1) * 2 * kTcN);
       const uint64_t a0 = descA + (uint64_t)((s * 4 * kTcTile * 4) >> 4);
@@ -344,17 +373,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
       }
     }
   }
-  if (!aborted && warp < 4) {  // the last receiver's products
-    bounded(&mmad[(Q - 1) % kTcStages], (Q - 1) / kTcStages);
-    tc_fence_after();
-    drain(((Q - 1) / nch) & 1);
-  }
   tc_fence_before();
   __syncthreads();
-  if (aborted || s_abort) {
+  if (s_abort) {
     // let the copies and products in flight land before the CTA exits
     // (bounded again); no partial is written, the host reports the error
-    if (tid == 0) {
+    if (tid == kTcIssuer) {
       for (int k = q; k < staged; ++k)
         mbar_wait(smem_u32(&full[k % kTcStages]), (uint32_t)(k / kTcStages) & 1u, kTcWaitLimit);
       if (q > 0)
