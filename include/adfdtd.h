@@ -193,7 +193,8 @@ typedef struct {
                       current 32-step block on the tensor cores (TF32 split
                       into three products, FP32 per receiver, Float64 over
                       receivers), within about 1e-6 of the Float64 sums; the
-                      map is kept a second time, packed as operand tiles  */
+                      map is kept again as packed operand tiles of twice
+                      its size (TF32 parts and remainders)               */
 } adf_gfmap;
 #define ADF_GF_CONTRACT_FP64 0
 #define ADF_GF_CONTRACT_TF32X3 1
