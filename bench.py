@@ -121,6 +121,11 @@ def parse():
                     help="run only the KH section and print it (profiling runs)")
     ap.add_argument("--gf-only", action="store_true",
                     help="run only the in-loop GF section and print it (profiling runs)")
+    ap.add_argument("--gf-tc-only", action="store_true",
+                    help="run only the tensor-core GF section once, no warm-up (profiling runs)")
+    ap.add_argument("--gf-tc-io", type=int, default=1024, help="sources = receivers of that map")
+    ap.add_argument("--gf-tc-lags", type=int, default=512, help="lags of that map")
+    ap.add_argument("--gf-tc-nt", type=int, default=700, help="steps of that run")
     return ap.parse_args()
 
 
@@ -1030,6 +1035,14 @@ def main():
         return kh_only(args)
     if args.gf_only:
         return gf_only(args)
+    if args.gf_tc_only:
+        import acoustic_disguising_b200 as A
+
+        ctx = A.Context(0)
+        out = gf_tc_section(A, ctx, nt=args.gf_tc_nt, nt_gf=args.gf_tc_lags, n_io=args.gf_tc_io)
+        print(json.dumps({"gf_map_tensor_core": out}), flush=True)
+        ctx.close()
+        return 0
     if args.hologram_only:
         return hologram_only(args)
     if args.serving_only:
