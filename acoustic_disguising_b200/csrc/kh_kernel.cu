@@ -498,6 +498,7 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   const int taps = (int)std::floor(2.0 * hw) + 1;
   int lm = 0;
   if (taps <= 16) lm = 16;
+  else if (taps <= 24) lm = 24;  // e.g. +-6 sigma at 20 kHz and dt = 2.1 us: 19 taps
   else if (taps <= 32) lm = 32;
   else
     return fail(ADF_E_ARG, "adf_kh_pressure: the +-" + std::to_string(ws) +
@@ -645,12 +646,16 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
 
   // the instantiation for (taps, kind, samples per lane)
   using KhFn = void (*)(KhParams);
-  static const KhFn kfn[2][2][2] = {
+  // (taps past the window are zero, so a wider instantiation gives the same
+  // sums with more FMAs: the narrowest that holds the window is taken)
+  static const KhFn kfn[3][2][2] = {
       {{adf_kh_pressure_kernel<16, 0, KH_T_SHORT>, adf_kh_pressure_kernel<16, 0, KH_T_LONG>},
        {adf_kh_pressure_kernel<16, 1, KH_T_SHORT>, adf_kh_pressure_kernel<16, 1, KH_T_LONG>}},
+      {{adf_kh_pressure_kernel<24, 0, KH_T_SHORT>, adf_kh_pressure_kernel<24, 0, KH_T_LONG>},
+       {adf_kh_pressure_kernel<24, 1, KH_T_SHORT>, adf_kh_pressure_kernel<24, 1, KH_T_LONG>}},
       {{adf_kh_pressure_kernel<32, 0, KH_T_SHORT>, adf_kh_pressure_kernel<32, 0, KH_T_LONG>},
        {adf_kh_pressure_kernel<32, 1, KH_T_SHORT>, adf_kh_pressure_kernel<32, 1, KH_T_LONG>}}};
-  const KhFn fn = kfn[lm == 16 ? 0 : 1][kind ? 1 : 0][T == KH_T_LONG ? 1 : 0];
+  const KhFn fn = kfn[lm == 16 ? 0 : (lm == 24 ? 1 : 2)][kind ? 1 : 0][T == KH_T_LONG ? 1 : 0];
   e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, std::string("kh smem: ") + cudaGetErrorString(e));
   const dim3 grid((unsigned)ntiles, (unsigned)((nt + TB - 1) / TB));

@@ -62,6 +62,7 @@ def run_pair(adf, oracle, c, window_sigmas=6.0):
     (256, 96, 1024, 5e-6, 0.25, 1.0),     # far field, 16-tap window
     (45, 50, 1001, 5e-6, 0.25, 0.8),      # ragged: ns, nr, nt off every block size
     (128, 64, 900, 5e-6, 0.25, 0.30),     # targets just outside the surface (wide delay spread)
+    (80, 48, 1200, 3.5e-6, 0.25, 0.7),    # 23-tap window (the 24-tap instantiation)
     (64, 40, 1500, 2.5e-6, 0.25, 0.6),    # 32-tap window
 ])
 def test_kh_matches_fp64_oracle(adf, oracle, ctx, ns, nr, nt, dt, r_surf, r_tgt):
@@ -143,6 +144,7 @@ def run_velocity(adf, oracle, c, seed=9):
     (256, 96, 1024, 5e-6, 0.25, 1.0),     # far field
     (128, 64, 900, 5e-6, 0.25, 0.30),     # near field: the 1/r^3 pedestal of v_v is large
     (45, 50, 1001, 5e-6, 0.25, 0.8),      # ragged sizes
+    (80, 48, 1200, 3.5e-6, 0.25, 0.7),    # 23-tap window
     (64, 40, 1500, 2.5e-6, 0.25, 0.6),    # 32-tap window
 ])
 def test_kh_velocity_matches_fp64_oracle(adf, oracle, ctx, ns, nr, nt, dt, r_surf, r_tgt):
