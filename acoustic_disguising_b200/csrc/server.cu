@@ -250,9 +250,24 @@ class Engine {
     for (GfJob* j : resident_)
       max_rem = std::max(max_rem, j->solve->dev.it_stop - j->solve->dev.it_base + 1);
     const int n = std::min(chunk_, max_rem);
-    int rc = batch_.run_chunk(ctx_, n, chunk_);
-    if (rc) return rc;
-    for (GfJob* j : resident_) j->solve->dev.it_base += n;
+    // Requests still queued after admit() cannot join before a resident
+    // solve finishes (memory, work cap or slots are exhausted): replay full
+    // chunks back to back up to the first such retirement and synchronise
+    // once, instead of returning to the host after every chunk.  With the
+    // queue empty, one chunk per tick keeps new arrivals' admission prompt.
+    int reps = 1;
+    if (!pending_.empty() && n == chunk_ && !ctx_->kernel_timing) {
+      int min_rem = max_rem;
+      for (GfJob* j : resident_)
+        min_rem = std::min(min_rem, j->solve->dev.it_stop - j->solve->dev.it_base + 1);
+      reps = std::max(1, (min_rem + chunk_ - 1) / chunk_);
+    }
+    int rc = ADF_OK;
+    for (int r = 0; r < reps; ++r) {
+      rc = batch_.run_chunk(ctx_, n, chunk_);
+      if (rc) return rc;
+      for (GfJob* j : resident_) j->solve->dev.it_base += n;
+    }
     rc = batch_.check_error(ctx_);  // synchronises the stream
     if (rc) return rc;
     batch_.collect_kernel_times(ctx_, n);
