@@ -40,10 +40,14 @@
 // and a wait that gives up sets the solve's error word (ADF_E_TIMEOUT), ends
 // every role's loop, lets the copies and products in flight land, frees the
 // tensor memory and leaves the partials unwritten.
+#include <atomic>
+
 #include "adf_internal.h"
 #include "ptx_util.h"
 
 namespace adf {
+
+constexpr int kMaxDevices = 64;  // devices a process can launch this kernel on
 
 constexpr int kTcM = 128;              // sources per CTA = tensor-memory lanes
 constexpr int kTcL = 16;               // lags per chunk (two MMA k-steps of 8)
@@ -415,13 +419,18 @@ cudaError_t launch_gf_tc_pack(const SolveDev& d, float* out, cudaStream_t s) {
 }
 
 cudaError_t launch_gf_far_tc(const EpiParams& p, int max_blocks, cudaStream_t s) {
-  static bool attr = false;  // the first launch of the process raises the shared-memory limit
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute((const void*)adf_gf_far_tc_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kTcDynSmem);
+  // the first launch on each device raises the kernel's shared-memory limit
+  // there (contexts on several devices or threads may launch concurrently)
+  static std::atomic<bool> attr_set[kMaxDevices];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!attr_set[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute((const void*)adf_gf_far_tc_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcDynSmem);
     if (e != cudaSuccess) return e;
-    attr = true;
+    attr_set[dev].store(true, std::memory_order_release);
   }
   adf_gf_far_tc_kernel<<<dim3(max_blocks > 0 ? max_blocks : 1, p.n_solves), kTcThreads, kTcDynSmem,
                          s>>>(p);
