@@ -27,6 +27,41 @@ def test_library_exports_every_declared_symbol(adf):
     assert set(names) <= bound
 
 
+def test_ctypes_structures_match_the_c_header(adf, tmp_path):
+    """Every structure the binding passes through the C ABI has the size and
+    field offsets that include/adfdtd.h gives it (gcc on the header), so a
+    field added on one side only is caught without a GPU."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    from acoustic_disguising_b200 import _lib as L
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc is not available")
+    pairs = [(L.Domain, "adf_domain"), (L.TxGridC, "adf_txgrid"), (L.CpmlC, "adf_cpml"),
+             (L.GfRequestC, "adf_gf_request"), (L.KhDescC, "adf_kh_desc"),
+             (L.GfMapC, "adf_gfmap")]
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "adfdtd.h"', "int main(void) {"]
+    want = []
+    for cls, cname in pairs:
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {name}));')
+            want.append(getattr(cls, name).offset)
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    include = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([gcc, "-I", include, "-o", str(exe), str(src)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got == want
+
+
 def test_no_cpu_fallback_without_gpu(adf):
     import torch
     if torch.cuda.is_available():
