@@ -1019,10 +1019,7 @@ def gf_only(args):
         A.build()
     ctx = A.Context(0)
     gf_section(A, ctx, nt=40)
-    out = {"gf_map": gf_section(A, ctx)}
-    gf_tc_section(A, ctx, nt=80, nt_gf=64, n_io=256)
-    out["gf_map_tensor_core"] = gf_tc_section(A, ctx)
-    print(json.dumps(out), flush=True)
+    print(json.dumps({"gf_map": gf_section(A, ctx)}), flush=True)
     ctx.close()
     return 0
 
