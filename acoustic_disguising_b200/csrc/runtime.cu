@@ -704,32 +704,33 @@ static cudaError_t upload_traces(Solve& s, const adf_txgrid* txs, cudaStream_t s
   return e;
 }
 
-static int download_traces(Solve& s, adf_txgrid* txs) {
+// Device (step-major) traces -> the caller's Julia (nt, ntx) arrays.  Stops at
+// the first failed copy and returns its error; nothing is transposed from it.
+static cudaError_t download_trace(Solve& s, std::vector<float>& tmp, const float* src, float* jl) {
+  const cudaError_t e = cudaMemcpy(tmp.data(), src, tmp.size() * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) transpose_to_julia(tmp.data(), jl, s.dev.nt, s.dev.ntx);
+  return e;
+}
+
+static cudaError_t download_traces(Solve& s, adf_txgrid* txs) {
   SolveDev& d = s.dev;
-  const int64_t nt = d.nt, ntx = d.ntx;
-  std::vector<float> tmp((size_t)(nt * ntx));
-  auto down = [&](const float* src, float* jl) {
-    cudaMemcpy(tmp.data(), src, tmp.size() * 4, cudaMemcpyDeviceToHost);
-    transpose_to_julia(tmp.data(), jl, nt, ntx);
-  };
-  for (int c = 0; c < 4; ++c) {
-    down(d.rec[c], txs->rec[c]);
-    if (c > 0) down(d.src[c], txs->src[c]);
+  std::vector<float> tmp((size_t)(d.nt * d.ntx));
+  cudaError_t e = cudaSuccess;
+  for (int c = 0; c < 4 && e == cudaSuccess; ++c) {
+    e = download_trace(s, tmp, d.rec[c], txs->rec[c]);
+    if (c > 0 && e == cudaSuccess) e = download_trace(s, tmp, d.src[c], txs->src[c]);
   }
-  down(d.vn_rec, txs->vn_rec);
-  return ADF_OK;
+  if (e == cudaSuccess) e = download_trace(s, tmp, d.vn_rec, txs->vn_rec);
+  return e;
 }
 
 // the GF extrapolation writes p_src and vn_src rows: both come back too
-static int download_gf_sources(Solve& s, adf_txgrid* txs) {
+static cudaError_t download_gf_sources(Solve& s, adf_txgrid* txs) {
   SolveDev& d = s.dev;
-  const int64_t nt = d.nt, ntx = d.ntx;
-  std::vector<float> tmp((size_t)(nt * ntx));
-  cudaMemcpy(tmp.data(), d.src[0], tmp.size() * 4, cudaMemcpyDeviceToHost);
-  transpose_to_julia(tmp.data(), txs->src[0], nt, ntx);
-  cudaMemcpy(tmp.data(), d.vn_src, tmp.size() * 4, cudaMemcpyDeviceToHost);
-  transpose_to_julia(tmp.data(), txs->vn_src, nt, ntx);
-  return ADF_OK;
+  std::vector<float> tmp((size_t)(d.nt * d.ntx));
+  cudaError_t e = download_trace(s, tmp, d.src[0], txs->src[0]);
+  if (e == cudaSuccess) e = download_trace(s, tmp, d.vn_src, txs->vn_src);
+  return e;
 }
 
 // psi: Julia (npml,ny,nz,2) / (nx,npml,nz,2) / (nx,ny,npml,2) <-> device.
@@ -1270,19 +1271,21 @@ static int run_fdtd_impl(adf_ctx* ctx, const adf_domain* d, float* field, adf_tx
   }
   // output buffer of the last executed step
   const int fb = (int)((stop_step - start_step + 1) & 1);
-  cudaMemcpy2D(field, (size_t)d->nx * 4, sd.field + (size_t)fb * sd.buf_stride,
-               (size_t)sd.nxp * 4, (size_t)d->nx * 4, (size_t)d->ny * d->nz * 4,
-               cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy2D(field, (size_t)d->nx * 4, sd.field + (size_t)fb * sd.buf_stride,
+                               (size_t)sd.nxp * 4, (size_t)d->nx * 4,
+                               (size_t)d->ny * d->nz * 4, cudaMemcpyDeviceToHost);
   if (npml > 0)
-    for (int a = 0; a < 3; ++a) {
-      if (cpml->mv[a]) psi_copy(*s, a, false, cpml->mv[a], false, fb, st);
-      if (cpml->mp[a]) psi_copy(*s, a, true, cpml->mp[a], false, fb, st);
+    for (int a = 0; a < 3 && e == cudaSuccess; ++a) {
+      if (cpml->mv[a]) e = psi_copy(*s, a, false, cpml->mv[a], false, fb, st);
+      if (cpml->mp[a] && e == cudaSuccess) e = psi_copy(*s, a, true, cpml->mp[a], false, fb, st);
     }
-  download_traces(*s, txs);
-  if (use_gf) download_gf_sources(*s, txs);
-  cudaError_t e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) e = cudaGetLastError();  // a failed download
-  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  if (e == cudaSuccess) e = download_traces(*s, txs);
+  if (use_gf && e == cudaSuccess) e = download_gf_sources(*s, txs);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("download: ") + cudaGetErrorString(e));
+  }
   return ADF_OK;
 }
 
