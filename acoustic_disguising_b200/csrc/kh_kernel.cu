@@ -668,6 +668,7 @@ static int kh_run(adf_ctx* ctx, const adf_kh_desc* d, const float* in_q, const f
   cudaMemcpyAsync(out, dout.p, (size_t)4 * nt * nr, cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost, st);
   e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaGetLastError();  // a download refused when it was enqueued
   if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);

@@ -470,11 +470,15 @@ int Batch::setup(adf_ctx* ctx, const std::vector<Solve*>& list) {
       return fail(ADF_E_NOMEM, "batch descriptor allocation failed");
     }
   }
-  host_solves = sd;
   cudaStream_t st = ctx->stream;
   cudaMemcpyAsync(d_solves, sd.data(), sizeof(SolveDev) * ns, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_items, items.data(), sizeof(int4) * n_items, cudaMemcpyHostToDevice, st);
-  cudaStreamSynchronize(st);
+  {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();  // a copy refused when it was enqueued
+    if (e != cudaSuccess)
+      return fail(ADF_E_DEVICE, std::string("batch descriptor upload: ") + cudaGetErrorString(e));
+  }
   // step + epilogue; GF solves add the extrapolation and its reduction when
   // a source's receivers are split
   per_step = max_gf_nsrc > 0 ? (gf_reduce ? 4 : 3) : 2;
@@ -647,13 +651,6 @@ int Batch::check_error(adf_ctx* ctx) {
     if (w & 4) return fail(ADF_E_TIMEOUT, "step kernel: a bounded wait for a staged plane gave up");
     if (w) return fail(ADF_E_STATE, "step kernel error word " + std::to_string(w));
   }
-  return ADF_OK;
-}
-
-int Batch::upload_descriptors(adf_ctx* ctx) {
-  for (size_t i = 0; i < solves.size(); ++i) host_solves[i] = solves[i]->dev;
-  cudaMemcpyAsync(d_solves, host_solves.data(), sizeof(SolveDev) * solves.size(),
-                  cudaMemcpyHostToDevice, ctx->stream);
   return ADF_OK;
 }
 

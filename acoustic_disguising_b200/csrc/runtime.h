@@ -89,7 +89,6 @@ struct Solve {
 
 struct Batch {
   std::vector<Solve*> solves;
-  std::vector<SolveDev> host_solves;
   SolveDev* d_solves = nullptr;
   int4* d_items = nullptr;
   int cap_solves = 0, cap_items = 0;
@@ -111,7 +110,6 @@ struct Batch {
   ~Batch();
   void release();
   int setup(adf_ctx* ctx, const std::vector<Solve*>& list);
-  int upload_descriptors(adf_ctx* ctx);
   int launch_step(adf_ctx* ctx, int step);
   int run(adf_ctx* ctx, int nsteps, bool use_graph, int chunk);
   int run_chunk(adf_ctx* ctx, int n, int chunk);
