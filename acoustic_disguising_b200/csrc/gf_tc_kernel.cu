@@ -263,8 +263,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
   };
   if (tid == kTcIssuer)
     while (staged < min(Q, kTcStages)) stage_next();
+  auto abort_seen = [&]() { return *reinterpret_cast<volatile int*>(&s_abort) != 0; };
+  // once any wait has given up, no later wait of the loops blocks again: a
+  // wait that does not complete on its first try returns when the abort flag
+  // is set, and each role leaves its loop at its next abort check
   auto bounded = [&](uint64_t* bar, int phase) {
-    if (!mbar_wait(smem_u32(bar), (uint32_t)phase & 1u, kTcWaitLimit)) {
+    const uint32_t a = smem_u32(bar), par = (uint32_t)phase & 1u;
+    if (mbar_try_wait(a, par) || abort_seen()) return;
+    if (!mbar_wait(a, par, kTcWaitLimit)) {
       atomicOr(gerr, 4);  // reported as ADF_E_TIMEOUT
       s_abort = 1;         // every role leaves its loop
     }
@@ -294,7 +300,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
   // chunk's products and commits them to mmad; no CTA barrier inside the
   // loop, so building, issuing and the tensor cores overlap across chunks.
   const int lane = tid & 31;
-  auto abort_seen = [&]() { return *reinterpret_cast<volatile int*>(&s_abort) != 0; };
   int q = 0;  // the chunk this thread's role stopped at
   if (warp < 4) {
     int rr = 0, c = 0;  // chunk q = chunk c of receiver r0 + rr
@@ -371,8 +376,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) adf_gf_far_tc_kernel(const EpiP
       }
       tc_commit(smem_u32(&mmad[s]));
       // the slot of chunk q-2 is free once its products are done: chunk q+2
+      // (never staged over products that are not known to be done)
       if (q >= 2 && staged < Q) {
         bounded(&mmad[(q - 2) % kTcStages], (q - 2) / kTcStages);
+        if (abort_seen()) {
+          ++q;  // chunk q's products were issued: the clean-up waits for them
+          break;
+        }
         stage_next();
       }
     }
