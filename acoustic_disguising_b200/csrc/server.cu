@@ -211,15 +211,24 @@ static int gf_extract(adf_ctx* ctx, GfJob& j) {
   const int n = d.ntx - 1;
   const size_t nt = (size_t)d.nt;
   cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaSuccess;
   if (n > 0) {
-    launch_extract(d.rec[0], d.nt, d.ntx, 1, s.stage, st);
-    launch_extract(d.vn_rec, d.nt, d.ntx, 1, s.stage + nt * n, st);
-    cudaMemcpyAsync(j.req.out_p, s.stage, nt * n * 4, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(j.req.out_vn, s.stage + nt * n, nt * n * 4, cudaMemcpyDeviceToHost, st);
+    e = launch_extract(d.rec[0], d.nt, d.ntx, 1, s.stage, st);
+    if (e == cudaSuccess) e = launch_extract(d.vn_rec, d.nt, d.ntx, 1, s.stage + nt * n, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(j.req.out_p, s.stage, nt * n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(j.req.out_vn, s.stage + nt * n, nt * n * 4, cudaMemcpyDeviceToHost, st);
     ctx->d2h_bytes += (int64_t)(2 * nt * n * 4);
   }
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return fail(ADF_E_DEVICE, cudaGetErrorString(e));
+  // the stream is synchronised even after a failed enqueue: the host
+  // buffers may still be targets of copies already issued
+  const cudaError_t es = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = es;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADF_E_DEVICE, std::string("GF output download: ") + cudaGetErrorString(e));
+  }
   return ADF_OK;
 }
 
