@@ -13,11 +13,13 @@
 // product runs on tcgen05.mma with FP32 accumulation in tensor memory.  Every
 // Float32 map entry and Float64 history sample is split into a TF32 part
 // (rounded to nearest, ties away) and the remainder, and hi*hi + hi*lo +
-// lo*hi is accumulated (the dropped lo*lo term is below 2^-22 of the
-// product).  After the last chunk of a receiver its accumulator is added
-// into Float64 sums in shared memory (two accumulator sets in tensor memory
-// alternate, so one is drained while the next receiver's products run), so
-// the sum over receivers stays in Float64.  The result agrees with the
+// lo*hi is accumulated: the dropped lo*lo term is below 2^-22 of the
+// product and each remainder, read by the tensor cores at TF32 width, loses
+// below 2^-21, so a product is within 5 * 2^-22 of g*h (the products of
+// TF32 parts are exact in FP32).  After the last chunk of a receiver its
+// accumulator is added into Float64 sums in shared memory (two accumulator
+// sets in tensor memory alternate, so one is drained while the next
+// receiver's products run), so the sum over receivers stays in Float64.  The result agrees with the
 // Float64 sum to about 1e-6 relative, Float32 level: an opt-in contraction
 // (ADF_GF_CONTRACT_TF32X3); the default path keeps the Float64 FMAs of the
 // reference's accumulation.

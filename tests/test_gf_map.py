@@ -160,6 +160,64 @@ def test_gf_map_unknown_contraction(adf):
         adf.GfMap("PVFromPin", tuple(ts), isr, irc, False, "bf16")._c(1.0)
 
 
+def _tf32_round(x32):
+    """Float32 -> TF32 as csrc/gf_tc_kernel.cu splits it (tf32_hi): half a
+    TF32 unit added to the bit pattern, the low 13 mantissa bits cleared
+    (nearest, ties away from zero)."""
+    b = np.ascontiguousarray(x32, dtype=np.float32).view(np.uint32)
+    return ((b + np.uint32(0x1000)) & np.uint32(0xFFFFE000)).view(np.float32)
+
+
+def _tf32_trunc(x32):
+    b = np.ascontiguousarray(x32, dtype=np.float32).view(np.uint32)
+    return (b & np.uint32(0xFFFFE000)).view(np.float32)
+
+
+def _split_inputs(n, seed):
+    """Float32 map entries and Float64 history samples over 60 binades, a
+    third of the map entries with the mantissa's low 13 bits forced to the
+    rounding tie (0x1000) or all ones (0x1FFF, where rounding carries into
+    the exponent)."""
+    rng = np.random.default_rng(seed)
+    g = (rng.standard_normal(n) * np.exp2(rng.integers(-30, 30, n))).astype(np.float32)
+    gb = g.view(np.uint32)
+    k = n // 3
+    gb[:k] = (gb[:k] & np.uint32(0xFFFFE000)) | np.uint32(0x1000)
+    gb[k:2 * k] |= np.uint32(0x1FFF)
+    h = rng.standard_normal(n) * np.exp2(rng.integers(-30, 30, n).astype(np.float64))
+    return gb.view(np.float32), h
+
+
+@pytest.mark.parametrize("tf32_read,bound", [("truncated", 5), ("rounded", 3)])
+def test_tf32x3_split_product_error_bound(tf32_read, bound):
+    """Precision of the tensor-core contraction per product (no GPU): a
+    Float32 map entry g and a Float64 history sample h are split as the
+    kernel splits them (gh = TF32 of g, gl = g - gh in Float32; hh = TF32 of
+    (float)h, hl = (float)(h - hh)), and gh*hh + gh*hl + gl*hh stands for
+    g*h.  gl is exact, gh and hh are TF32 values, and whether the tensor
+    cores read the remainders truncated or rounded to TF32 width, the error
+    stays below bound * 2^-22 of |g*h|: the dropped gl*hl is below 2^-22,
+    each remainder read at TF32 width loses below 2^-21 truncated or 2^-22
+    rounded (a factor 1 + 2^-9 covers the parts' own 1 + 2^-11 growth).
+    The products of TF32 values are exact in Float64 here and in the tensor
+    cores' FP32 products."""
+    g, h = _split_inputs(1 << 20, 11)
+    gh = _tf32_round(g)
+    gl = (g - gh).astype(np.float32)
+    assert np.array_equal(gl.astype(np.float64), g.astype(np.float64) - gh.astype(np.float64))
+    assert not np.any(gh.view(np.uint32) & np.uint32(0x1FFF))
+    hh = _tf32_round(h.astype(np.float32))
+    hl = (h - hh.astype(np.float64)).astype(np.float32)
+    read = _tf32_trunc if tf32_read == "truncated" else _tf32_round
+    f = lambda v: v.astype(np.float64)  # noqa: E731
+    approx = f(gh) * f(hh) + f(gh) * f(read(hl)) + f(read(gl)) * f(hh)
+    exact = g.astype(np.float64) * h
+    rel = np.abs(approx - exact) / np.abs(exact)
+    assert rel.max() < bound * 2.0 ** -22 * (1 + 2.0 ** -9)
+    # the split is needed: one TF32 product alone is about 2^-11 off
+    assert (np.abs(f(gh) * f(hh) - exact) / np.abs(exact)).max() > 2.0 ** -12
+
+
 @pytest.mark.gpu
 def test_gf_map_tensor_core_contraction_rejects_pvfrompv(adf, oracle, ctx):
     """The tensor-core contraction covers the input-history kinds only."""
