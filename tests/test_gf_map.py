@@ -218,6 +218,61 @@ def test_tf32x3_split_product_error_bound(tf32_read, bound):
     assert (np.abs(f(gh) * f(hh) - exact) / np.abs(exact)).max() > 2.0 ** -12
 
 
+def test_gf_tc_history_window_indexes():
+    """Index arithmetic of the tensor-core far-lag kernel (csrc/gf_tc_kernel.cu,
+    win_of and the B-operand build), restated and checked on the CPU over
+    every block start, map length and chunk: each history row a far lag of
+    the block reads lies in the chunk's staged window, the window is an even
+    run of at most kTcWinD = 64 doubles starting on an even element (16-B
+    aligned bulk copy) inside the receiver's row of the history, the chunks
+    cover exactly the far lags (lag > step of the block, lag < min(it0 +
+    step, ngf)), and far plus near lags (the
+    per-step kernel's lag <= step) give the full causal sum."""
+    L, N, WIN = 16, 32, 64
+    rng = np.random.default_rng(3)
+    for nt in (40, 97, 700):
+        for ngf in (2, 17, 20, 33, 100, 512):
+            for r in (0, 1, 5):  # receiver rows start at r * nt (odd nt: odd starts)
+                g0 = r * nt
+                for it0 in range(1, nt, N):
+                    lag_hi = min(it0 + N - 1, ngf) - 1
+                    nch = (lag_hi + L - 1) // L if lag_hi >= 1 else 0
+                    covered = set()
+                    for c in range(nch):
+                        lo = max(0, it0 - 1 - L * (c + 1))
+                        hi = min(it0 - 2, it0 + N - 3 - L * c)
+                        if hi < lo:
+                            gs, cnt = 0, 0
+                        else:
+                            gs = (g0 + lo) & ~1
+                            cnt = (g0 + hi - gs + 2) & ~1
+                            assert gs % 2 == 0 and cnt % 2 == 0 and 0 < cnt <= WIN
+                            # the copy stays in this receiver's row of the history
+                            assert g0 - 1 <= gs and gs + cnt <= (r + 1) * nt
+                        for b in range(N):
+                            lim = min(it0 + b, ngf)
+                            for k in range(L):
+                                lag = L * c + 1 + k
+                                if not (b < lag < lim):
+                                    continue
+                                row = it0 - 1 + b - lag
+                                assert 0 <= row < nt
+                                w = (g0 - gs) + row
+                                assert 0 <= w < cnt, (nt, ngf, it0, c, b, lag)
+                                covered.add((b, lag))
+                    far = {(b, lag) for b in range(N) for lag in range(b + 1, min(it0 + b, ngf))}
+                    assert covered == far, (nt, ngf, it0)
+    # far + near = the full causal sum, one receiver, one block
+    ngf, it0, nt = 100, 65, 200
+    G = rng.standard_normal(ngf)
+    pin = rng.standard_normal(nt)
+    for b in range(N):
+        full = sum(G[lag] * pin[it0 - 1 + b - lag] for lag in range(min(it0 + b, ngf)))
+        near = sum(G[lag] * pin[it0 - 1 + b - lag] for lag in range(min(b + 1, it0 + b, ngf)))
+        far = sum(G[lag] * pin[it0 - 1 + b - lag] for lag in range(b + 1, min(it0 + b, ngf)))
+        assert abs(full - (near + far)) <= 1e-12 * (1 + abs(full))
+
+
 @pytest.mark.gpu
 def test_gf_map_tensor_core_contraction_rejects_pvfrompv(adf, oracle, ctx):
     """The tensor-core contraction covers the input-history kinds only."""
