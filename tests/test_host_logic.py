@@ -27,6 +27,58 @@ def test_library_exports_every_declared_symbol(adf):
     assert set(names) <= bound
 
 
+def _c_declarations():
+    """{name: [parameter type]} of every entry point in include/adfdtd.h."""
+    txt = open(os.path.join(ROOT, "include", "adfdtd.h")).read()
+    txt = re.sub(r"/\*.*?\*/", " ", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^int\s+(adf_\w+)\s*\(([^;]*?)\)\s*;", txt, flags=re.M | re.S):
+        params = " ".join(m.group(2).split())
+        types = []
+        if params != "void":
+            for p in params.split(","):
+                p = p.strip()
+                name = re.search(r"(\**)\s*(\w+)$", p)
+                types.append((p[:name.start()] + name.group(1)).replace("const", "").replace(" ", ""))
+        out[m.group(1)] = types
+    return out
+
+
+def test_ctypes_signatures_match_the_c_header(adf):
+    """Every argument the binding declares has the C type include/adfdtd.h
+    gives it: scalars by width and signedness, pointers as pointers, and a
+    typed pointer to the same structure or scalar (c_void_p stands for any
+    pointer)."""
+    from acoustic_disguising_b200 import _lib as L
+
+    scalars = {"int": C.c_int, "uint32_t": C.c_uint32, "int64_t": C.c_int64,
+               "size_t": C.c_size_t, "double": C.c_double}
+    structs = {"adf_domain": L.Domain, "adf_txgrid": L.TxGridC, "adf_cpml": L.CpmlC,
+               "adf_gfmap": L.GfMapC, "adf_gf_request": L.GfRequestC,
+               "adf_kh_desc": L.KhDescC}
+    decl = _c_declarations()
+    bound = {name: (res, args) for name, res, args in L.SIGNATURES}
+    assert set(decl) == set(bound)
+    for name, ctypes_ in decl.items():
+        res, args = bound[name]
+        assert res is C.c_int, name
+        assert len(args) == len(ctypes_), name
+        for i, (ct, a) in enumerate(zip(ctypes_, args)):
+            where = f"{name} argument {i} ({ct})"
+            if ct == "adf_step_cb":
+                assert a is L.STEP_CB, where
+            elif not ct.endswith("*"):
+                assert a is scalars[ct], where
+            elif a in (C.c_void_p, C.c_char_p):
+                assert ct != "char*" or a is C.c_char_p, where
+            else:
+                assert hasattr(a, "_type_") and issubclass(a, C._Pointer), where
+                base = ct[:-1]
+                want = structs.get(base) or scalars.get(base) or (
+                    C.c_void_p if base in ("adf_ctx*", "adf_server*") else None)
+                assert a._type_ is want, where
+
+
 def test_ctypes_structures_match_the_c_header(adf, tmp_path):
     """Every structure the binding passes through the C ABI has the size and
     field offsets that include/adfdtd.h gives it (gcc on the header), so a
