@@ -633,6 +633,8 @@ void Batch::collect_kernel_times(adf_ctx* ctx, int n) {
     if (cudaEventElapsedTime(&ms, ctx->kev[2 * s], ctx->kev[2 * s + 1]) == cudaSuccess) {
       ctx->kernel_ms += ms;
       ++ctx->kernel_launches;
+    } else {
+      cudaGetLastError();  // a missing sample is not a device error of the next call
     }
   }
 }
